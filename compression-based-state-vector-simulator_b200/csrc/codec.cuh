@@ -1,0 +1,187 @@
+// Error-bounded quantiser of the block codec (host and device).
+//
+// Replaces the reference's log compander + nvCOMP Bitcomp lossy FP64 stage
+// (src/cppsim/compand_kernel.cuh:5-30, compand_bitcomp_pipeline.cuh:14-62).
+// That pipeline bounds every real component by |xhat - x| <= (eps_rel|x| +
+// eps_abs)/2 (a round-to-nearest step of log1p(eps_rel) in the log domain,
+// offset tau' = (1-2 eps_rel) eps_abs/eps_rel).  This quantiser meets the same
+// pointwise bound with integer and exact floating-point operations only:
+//
+//   |x| <  2^e0 : c = rint(|x| * 2^L)                (2^-L <= eps_abs)
+//   |x| >= 2^e0 : c = 2^m + (bits(|x|) rounded to m mantissa bits) - bits(2^e0)
+//                                                     (2^-m <= eps_rel)
+//   e0 = m - L, q = sign ? -c : c
+//
+// Both steps coincide in the binade [2^e0, 2^(e0+1)), so c is continuous and
+// monotone in |x|.  The CPU oracle (oracle/codec_oracle.c) states the same map;
+// the integer codes agree bit for bit.
+//
+// Chunk payload layout (32-lane vertical frame of reference): the 2^(C+1)
+// components of a chunk (interleaved re, im) are split into 32 streams,
+// stream l = components l, l+32, ...; u = q - base (base = chunk minimum) is
+// packed LSB first in `width` bits per component into rows of 32-bit words,
+// word r of stream l at index r*32 + l.  rows = ceil(per_lane*width/32),
+// payload bytes = 128*rows.
+#pragma once
+
+#include <cstdint>
+#include <cstring>
+#include <cmath>
+
+#include "internal.h"
+
+namespace qs {
+
+constexpr int64_t kCodeLimit = 0x3fffffff;
+
+__host__ __device__ inline uint64_t payload_rows(int C, uint32_t width) {
+    const uint64_t per_lane = (uint64_t(2) << C) / 32;
+    return (per_lane * width + 31) / 32;
+}
+
+__host__ __device__ inline uint64_t payload_bytes(int C, uint32_t width) {
+    return payload_rows(C, width) * 128;
+}
+
+__host__ __device__ inline uint32_t bit_length(uint32_t v) {
+#ifdef __CUDA_ARCH__
+    return 32u - __clz(v);
+#else
+    return v ? 32u - (uint32_t)__builtin_clz(v) : 0u;
+#endif
+}
+
+// ---------------------------------------------------------------- float
+__host__ __device__ inline int32_t quantize(float x, CodecParams p) {
+    uint32_t bits;
+#ifdef __CUDA_ARCH__
+    bits = __float_as_uint(x);
+#else
+    std::memcpy(&bits, &x, 4);
+#endif
+    const uint32_t abits = bits & 0x7fffffffu;
+    const bool neg = (bits >> 31) != 0;
+    const int e0 = p.m - p.L;
+    const uint32_t thr = uint32_t(e0 + 127) << 23;
+    int64_t c;
+    if (abits < thr) {
+        float a;
+#ifdef __CUDA_ARCH__
+        a = __uint_as_float(abits);
+        const float scale = __uint_as_float(uint32_t(p.L + 127) << 23);  // 2^L exactly
+        c = (int64_t)__float2ll_rn(__fmul_rn(a, scale));
+#else
+        std::memcpy(&a, &abits, 4);
+        c = (int64_t)std::nearbyint(a * std::ldexp(1.0f, p.L));
+#endif
+    } else {
+        const int sh = 23 - p.m;
+        const uint64_t half = sh > 0 ? (uint64_t(1) << (sh - 1)) : 0;
+        c = (int64_t)((uint64_t(abits) + half) >> sh) - (int64_t(e0 + 127) << p.m) + (int64_t(1) << p.m);
+    }
+    if (c > kCodeLimit) c = kCodeLimit;
+    return (int32_t)(neg ? -c : c);
+}
+
+__host__ __device__ inline float dequantize_f32(int32_t q, CodecParams p) {
+    const bool neg = q < 0;
+    const int64_t c = neg ? -(int64_t)q : (int64_t)q;
+    float a;
+    if (c <= (int64_t(1) << p.m)) {
+#ifdef __CUDA_ARCH__
+        const float iscale = __uint_as_float(uint32_t(127 - p.L) << 23);  // 2^-L exactly
+        a = __fmul_rn((float)c, iscale);
+#else
+        a = (float)c * std::ldexp(1.0f, -p.L);
+#endif
+    } else {
+        const int e0 = p.m - p.L;
+        const int sh = 23 - p.m;
+        const uint32_t bits =
+            (uint32_t)((uint64_t)(c - (int64_t(1) << p.m) + (int64_t(e0 + 127) << p.m)) << sh);
+#ifdef __CUDA_ARCH__
+        a = __uint_as_float(bits);
+#else
+        std::memcpy(&a, &bits, 4);
+#endif
+    }
+    return neg ? -a : a;
+}
+
+// ---------------------------------------------------------------- double
+__host__ __device__ inline int32_t quantize(double x, CodecParams p) {
+    uint64_t bits;
+#ifdef __CUDA_ARCH__
+    bits = (uint64_t)__double_as_longlong(x);
+#else
+    std::memcpy(&bits, &x, 8);
+#endif
+    const uint64_t abits = bits & 0x7fffffffffffffffull;
+    const bool neg = (bits >> 63) != 0;
+    const int e0 = p.m - p.L;
+    const uint64_t thr = uint64_t(e0 + 1023) << 52;
+    int64_t c;
+    if (abits < thr) {
+        double a;
+#ifdef __CUDA_ARCH__
+        a = __longlong_as_double((long long)abits);
+        const double scale = __longlong_as_double((long long)(uint64_t(p.L + 1023) << 52));
+        c = (int64_t)__double2ll_rn(__dmul_rn(a, scale));
+#else
+        std::memcpy(&a, &abits, 8);
+        c = (int64_t)std::nearbyint(a * std::ldexp(1.0, p.L));
+#endif
+    } else {
+        const int sh = 52 - p.m;
+        const uint64_t half = uint64_t(1) << (sh - 1);
+        c = (int64_t)((abits + half) >> sh) - (int64_t(e0 + 1023) << p.m) + (int64_t(1) << p.m);
+    }
+    if (c > kCodeLimit) c = kCodeLimit;
+    return (int32_t)(neg ? -c : c);
+}
+
+__host__ __device__ inline double dequantize_f64(int32_t q, CodecParams p) {
+    const bool neg = q < 0;
+    const int64_t c = neg ? -(int64_t)q : (int64_t)q;
+    double a;
+    if (c <= (int64_t(1) << p.m)) {
+#ifdef __CUDA_ARCH__
+        const double iscale = __longlong_as_double((long long)(uint64_t(1023 - p.L) << 52));
+        a = __dmul_rn((double)c, iscale);
+#else
+        a = (double)c * std::ldexp(1.0, -p.L);
+#endif
+    } else {
+        const int e0 = p.m - p.L;
+        const int sh = 52 - p.m;
+        const uint64_t bits = (uint64_t)(c - (int64_t(1) << p.m) + (int64_t(e0 + 1023) << p.m)) << sh;
+#ifdef __CUDA_ARCH__
+        a = __longlong_as_double((long long)bits);
+#else
+        std::memcpy(&a, &bits, 8);
+#endif
+    }
+    return neg ? -a : a;
+}
+
+__host__ __device__ inline float dequantize(int32_t q, CodecParams p, float) { return dequantize_f32(q, p); }
+__host__ __device__ inline double dequantize(int32_t q, CodecParams p, double) { return dequantize_f64(q, p); }
+
+// Quantiser parameters from the error bounds; false when eps_rel is out of
+// range.  L is clamped so that 2^L, 2^-L and 2^e0 are normal numbers.
+inline bool codec_params(bool f64, double eps_rel, double eps_abs, CodecParams *out) {
+    if (!(eps_rel > 0.0) || !(eps_rel < 1.0)) return false;
+    int m = (int)std::ceil(-std::log2(eps_rel));
+    if (m < 1) m = 1;
+    if (m > 24) return false;
+    if (!f64 && m > 23) m = 23;
+    const int bias = f64 ? 1023 : 127;
+    int L = eps_abs > 0.0 ? (int)std::ceil(-std::log2(eps_abs)) : bias - 1;
+    if (L > bias - 1) L = bias - 1;
+    if (L < m - (bias - 2)) L = m - (bias - 2);
+    out->m = m;
+    out->L = L;
+    return true;
+}
+
+}  // namespace qs

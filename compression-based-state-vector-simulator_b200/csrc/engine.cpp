@@ -1,0 +1,1252 @@
+// Host engine of the compressed state-vector path and the C ABI (qompsim.h).
+//
+// Restates the host logic of CompressedQuantumState
+// (src/cppsim/compressed_state.hpp): block geometry and initial state
+// (:87-239, :327-352), the stage partitioner partition_circuit (:509-583),
+// make_block_groups (:585-671), partition_and_register_circuit (:673-726),
+// register_circuit_stages (:464-507), the active-group rule of
+// build_stage_group_execution_plan (:791-837), apply_circuit (:840-937),
+// append_total_SV_bytes / get_max_SV_bytes (:374-445) and
+// get_decompressed_state_vector (:1683-1707).
+//
+// What differs by design: the compressed store stays in device memory; a
+// stage runs as one or more fused device passes (kernels.cu) instead of a
+// host loop over groups with per-gate launches; the active-group test and
+// the zero-mask update run on the device, so apply_circuit enqueues the
+// whole circuit without a host synchronisation.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <set>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/qompsim.h"
+#include "codec.cuh"
+#include "internal.h"
+
+using cplx = std::complex<double>;
+
+namespace {
+
+std::string g_last_error = "no error";
+
+const char *kTimerKeys[10] = {"decomp", "gate", "comp", "fused_swap", "allgather",
+                              "hmalloc", "dmalloc", "h2d", "d2h", "dfree"};
+
+// --------------------------------------------------------------- gates
+struct CGate {
+    int nq = 0;
+    int q[2] = {0, 0};
+    cplx m[16];
+    bool mix[2] = {false, false};
+    bool diag = false;
+};
+
+// Express a matrix whose index bit i belongs to order[i] in ascending
+// qubit order.
+void reorder_ascending(int k, const int *order, const cplx *in, int *qout, cplx *out) {
+    int idx[2] = {0, 1};
+    if (k == 2 && order[0] > order[1]) std::swap(idx[0], idx[1]);
+    for (int i = 0; i < k; ++i) qout[i] = order[idx[i]];
+    const int dim = 1 << k;
+    auto map = [&](int x) {  // new index -> old index
+        int r = 0;
+        for (int i = 0; i < k; ++i)
+            if ((x >> i) & 1) r |= 1 << idx[i];
+        return r;
+    };
+    for (int r = 0; r < dim; ++r)
+        for (int c = 0; c < dim; ++c) out[r * dim + c] = in[map(r) * dim + map(c)];
+}
+
+bool canonicalize(const qs_gate &g, bool ref_controls, uint32_t n, CGate *cg, std::string *err) {
+    const std::string name(g.name, strnlen(g.name, sizeof(g.name)));
+    if (name == "FusedSWAP") {
+        *err = "FusedSWAP gates exchange qubits between MPI ranks; this engine has one GPU and no ranks";
+        return false;
+    }
+    if (g.ntargets < 1 || g.ntargets > 2 || g.ncontrols > 2) {
+        *err = "Error: only single- or two-qubit gates are implemented";
+        return false;
+    }
+    for (uint32_t i = 0; i < g.ntargets; ++i)
+        if (g.targets[i] >= n) { *err = "gate target index out of range"; return false; }
+    for (uint32_t i = 0; i < g.ncontrols; ++i)
+        if (g.controls[i] >= n) { *err = "gate control index out of range"; return false; }
+    const int nt = (int)g.ntargets;
+    const int dimt = 1 << nt;
+    cplx M[16];
+    for (int k = 0; k < dimt * dimt; ++k) M[k] = cplx(g.matrix[2 * k], g.matrix[2 * k + 1]);
+    const bool use_controls = !ref_controls || name == "CNOT";
+    if (use_controls && g.ncontrols > 0) {
+        const int k = nt + (int)g.ncontrols;
+        if (k > 2) {
+            *err = "Error: only single- or two-qubit gates are implemented (targets + controls > 2)";
+            return false;
+        }
+        int order[2];
+        for (int i = 0; i < nt; ++i) order[i] = (int)g.targets[i];
+        for (int i = 0; i < (int)g.ncontrols; ++i) order[nt + i] = (int)g.controls[i];
+        if (order[0] == order[1]) { *err = "duplicated qubit index in gate"; return false; }
+        cplx F[16];
+        const int dim = 1 << k;
+        for (int r = 0; r < dim; ++r)
+            for (int c = 0; c < dim; ++c) F[r * dim + c] = r == c ? 1.0 : 0.0;
+        int cm = 0;
+        for (int i = 0; i < (int)g.ncontrols; ++i)
+            if (g.control_values[i]) cm |= 1 << i;
+        const int base = cm << nt;
+        for (int r = 0; r < dimt; ++r)
+            for (int c = 0; c < dimt; ++c) F[(base + r) * dim + base + c] = M[r * dimt + c];
+        cg->nq = k;
+        reorder_ascending(k, order, F, cg->q, cg->m);
+    } else if (nt == 1) {
+        cg->nq = 1;
+        cg->q[0] = (int)g.targets[0];
+        for (int k2 = 0; k2 < 4; ++k2) cg->m[k2] = M[k2];
+    } else {
+        if (g.targets[0] == g.targets[1]) { *err = "duplicated qubit index in gate"; return false; }
+        cg->nq = 2;
+        if (ref_controls) {
+            // The reference's two-qubit kernels pair matrix bit 0 with the lower
+            // target whatever the target order (compressed_state_cuda.cu:632-642).
+            cg->q[0] = (int)std::min(g.targets[0], g.targets[1]);
+            cg->q[1] = (int)std::max(g.targets[0], g.targets[1]);
+            for (int k2 = 0; k2 < 16; ++k2) cg->m[k2] = M[k2];
+        } else {
+            int order[2] = {(int)g.targets[0], (int)g.targets[1]};
+            reorder_ascending(2, order, M, cg->q, cg->m);
+        }
+    }
+    const int dim = 1 << cg->nq;
+    for (int b = 0; b < cg->nq; ++b) {
+        bool mx = false;
+        for (int r = 0; r < dim; ++r)
+            for (int c = 0; c < dim; ++c)
+                if ((((r ^ c) >> b) & 1) && cg->m[r * dim + c] != cplx(0.0, 0.0)) mx = true;
+        cg->mix[b] = mx;
+    }
+    cg->diag = !cg->mix[0] && !(cg->nq == 2 && cg->mix[1]);
+    return true;
+}
+
+qs::KGate to_kgate(const CGate &cg, const std::vector<int> &tile_qubits, int C) {
+    qs::KGate k;
+    std::memset(&k, 0, sizeof(k));
+    k.nq = cg.nq;
+    k.diag = cg.diag ? 1 : 0;
+    for (int i = 0; i < cg.nq; ++i) {
+        k.q[i] = cg.q[i];
+        if (cg.q[i] < C) {
+            k.tpos[i] = cg.q[i];
+        } else {
+            auto it = std::find(tile_qubits.begin(), tile_qubits.end(), cg.q[i]);
+            k.tpos[i] = it == tile_qubits.end() ? -1 : C + (int)(it - tile_qubits.begin());
+        }
+    }
+    const int dim = 1 << cg.nq;
+    for (int r = 0; r < dim * dim; ++r) {
+        k.m[2 * r] = cg.m[r].real();
+        k.m[2 * r + 1] = cg.m[r].imag();
+    }
+    return k;
+}
+
+struct PassPlan {
+    std::vector<int> tile;        // tile qubits >= C, ascending
+    std::vector<uint32_t> gates;  // indices into the gate list
+};
+
+// Split a gate sequence into passes: a pass's tile holds the chunk qubits
+// [0, C) plus at most jmax other qubits, which must include every qubit on
+// which a gate of the pass mixes amplitudes.  Tiles are padded to jmin
+// qubits with in-block qubits so that a tile has several chunks.
+std::vector<PassPlan> plan_passes(const std::vector<uint32_t> &gate_ids, const std::vector<CGate> &cg, int C,
+                                  int jmax, int jmin, int pad_lo, int pad_hi) {
+    std::vector<PassPlan> out;
+    std::set<int> cur;
+    PassPlan p;
+    for (uint32_t gi : gate_ids) {
+        std::set<int> need = cur;
+        for (int b = 0; b < cg[gi].nq; ++b)
+            if (cg[gi].mix[b] && cg[gi].q[b] >= C) need.insert(cg[gi].q[b]);
+        if ((int)need.size() > jmax) {
+            p.tile.assign(cur.begin(), cur.end());
+            out.push_back(p);
+            p = PassPlan();
+            cur.clear();
+            for (int b = 0; b < cg[gi].nq; ++b)
+                if (cg[gi].mix[b] && cg[gi].q[b] >= C) cur.insert(cg[gi].q[b]);
+        } else {
+            cur = need;
+        }
+        p.gates.push_back(gi);
+    }
+    p.tile.assign(cur.begin(), cur.end());
+    out.push_back(p);
+    for (auto &pp : out) {
+        std::set<int> s(pp.tile.begin(), pp.tile.end());
+        for (int q = pad_lo; q < pad_hi && (int)s.size() < jmin; ++q) s.insert(q);
+        pp.tile.assign(s.begin(), s.end());
+    }
+    return out;
+}
+
+std::string format_size(unsigned long long size) {
+    char buf[64];
+    if (size > (1ULL << 30)) snprintf(buf, sizeof(buf), "%.3f GiB", (double)size / (1ULL << 30));
+    else if (size > (1ULL << 20)) snprintf(buf, sizeof(buf), "%.3f MiB", (double)size / (1ULL << 20));
+    else if (size > (1ULL << 10)) snprintf(buf, sizeof(buf), "%.3f KiB", (double)size / (1ULL << 10));
+    else snprintf(buf, sizeof(buf), "%llu bytes", size);
+    return buf;
+}
+
+int env_int(const char *name, int dflt) {
+    const char *v = std::getenv(name);
+    return v ? std::atoi(v) : dflt;
+}
+
+}  // namespace
+
+#define CUDA_TRY(h, expr)                                                               \
+    do {                                                                                \
+        cudaError_t e__ = (expr);                                                       \
+        if (e__ != cudaSuccess) {                                                       \
+            (h)->err = std::string(#expr) + ": " + cudaGetErrorString(e__);             \
+            return QS_ERR_CUDA;                                                         \
+        }                                                                               \
+    } while (0)
+
+// =====================================================================
+// compressed state
+// =====================================================================
+struct qs_state {
+    uint32_t n = 0, B = 0, C = 0, nb = 0;
+    uint64_t nchunks = 0;
+    bool f64 = true;
+    double eps_rel = 0, eps_abs = 0;
+    qs::CodecParams codec{};
+    uint32_t flags = 0;
+    int tile_log2 = 13;
+    cudaStream_t stream = nullptr;
+    std::string err = "no error";
+
+    std::vector<qs_gate> gates;
+    std::vector<CGate> cgates;
+    std::vector<std::vector<uint32_t>> stages;
+    std::vector<std::vector<uint32_t>> b2g;
+    std::vector<uint32_t> num_groups;
+    bool planned = false;
+
+    struct DevPass {
+        uint32_t stage;
+        int j;
+        int32_t tq[qs::kMaxTileQubits];
+        uint32_t gate_off, ngates;
+        bool first, final;
+    };
+    std::vector<DevPass> passes;
+    std::vector<uint64_t> stage_amps;   // amplitudes in active groups (for stats), filled on demand
+
+    qs::ChunkMeta *meta[2] = {nullptr, nullptr};
+    uint32_t *arena[2] = {nullptr, nullptr};
+    uint64_t capacity = 0;
+    unsigned long long *counters = nullptr;  // [0..1] bump, [2..4] stats, [5] init scratch
+    uint8_t *mask = nullptr;
+    uint32_t *block_nz = nullptr;
+    unsigned long long *block_bytes = nullptr, *block_acc = nullptr;
+    uint8_t *group_active = nullptr;
+    uint32_t *b2g_dev = nullptr;
+    qs::KGate *kgates = nullptr;
+    unsigned long long *history_dev = nullptr;  // [0..ns] totals, [ns+1..2ns] active blocks per stage
+    size_t history_cap = 0;
+    std::vector<cudaEvent_t> pass_ev;           // QS_FLAG_PROFILE: two events per pass
+    int32_t *error_dev = nullptr;
+    double *dscratch = nullptr;
+    int cur = 0;
+    uint64_t arena_used = 0;
+
+    std::vector<uint64_t> history;
+    double times[10] = {0};
+    qs_stats st{};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+
+    ~qs_state() {
+        for (int i = 0; i < 2; ++i) {
+            if (meta[i]) cudaFree(meta[i]);
+            if (arena[i]) cudaFree(arena[i]);
+            if (ev[i]) cudaEventDestroy(ev[i]);
+        }
+        if (counters) cudaFree(counters);
+        if (mask) cudaFree(mask);
+        if (block_nz) cudaFree(block_nz);
+        if (block_bytes) cudaFree(block_bytes);
+        if (block_acc) cudaFree(block_acc);
+        if (group_active) cudaFree(group_active);
+        if (b2g_dev) cudaFree(b2g_dev);
+        if (kgates) cudaFree(kgates);
+        if (history_dev) cudaFree(history_dev);
+        for (auto e : pass_ev) cudaEventDestroy(e);
+        if (error_dev) cudaFree(error_dev);
+        if (dscratch) cudaFree(dscratch);
+    }
+
+    bool quiet() const { return (flags & QS_FLAG_QUIET) != 0; }
+    bool ref_controls() const { return (flags & QS_FLAG_REFERENCE_CONTROLS) != 0; }
+    uint64_t chunks_per_block() const { return uint64_t(1) << (B - C); }
+
+    // Encode |basis> into the current store: only the block holding `basis`
+    // is stored, every chunk of it is zero except the one holding `basis`.
+    qs_status init_basis(uint64_t basis) {
+        const uint64_t blk = basis >> B;
+        const uint64_t chunk = basis >> C;
+        CUDA_TRY(this, cudaMemsetAsync(mask, 0, nb, stream));
+        CUDA_TRY(this, cudaMemsetAsync(block_bytes, 0, nb * sizeof(unsigned long long), stream));
+        CUDA_TRY(this, cudaMemsetAsync(meta[cur] + blk * chunks_per_block(), 0,
+                                       chunks_per_block() * sizeof(qs::ChunkMeta), stream));
+        const int comp = (int)(2 * (basis & ((uint64_t(1) << C) - 1)));
+        const int32_t q1 = f64 ? qs::quantize(1.0, codec) : qs::quantize(1.0f, codec);
+        const uint32_t w = qs::bit_length((uint32_t)q1);
+        std::vector<uint32_t> words(qs::payload_rows(C, w) * 32, 0u);
+        const int lane = comp % 32, i = comp / 32;
+        const uint64_t bitpos = (uint64_t)i * w;
+        const uint64_t r = bitpos >> 5, s = bitpos & 31;
+        words[r * 32 + lane] |= (uint32_t)((uint64_t)q1 << s);
+        if (s + w > 32) words[(r + 1) * 32 + lane] |= (uint32_t)((uint64_t)q1 >> (32 - s));
+        qs::ChunkMeta md{0, 0, w};
+        CUDA_TRY(this, cudaMemcpyAsync(arena[cur], words.data(), words.size() * 4, cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(this, cudaMemcpyAsync(meta[cur] + chunk, &md, sizeof(md), cudaMemcpyHostToDevice, stream));
+        const uint8_t one = 1;
+        CUDA_TRY(this, cudaMemcpyAsync(mask + blk, &one, 1, cudaMemcpyHostToDevice, stream));
+        const unsigned long long bytes = words.size() * 4 + chunks_per_block() * sizeof(qs::ChunkMeta);
+        CUDA_TRY(this, cudaMemcpyAsync(block_bytes + blk, &bytes, sizeof(bytes), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(this, cudaStreamSynchronize(stream));
+        arena_used = words.size() * 4;
+        history.assign(1, bytes);
+        return QS_OK;
+    }
+};
+
+static qs_status fail(qs_state *h, qs_status s, const std::string &msg) {
+    if (h) h->err = msg;
+    else g_last_error = msg;
+    return s;
+}
+
+extern "C" {
+
+const char *qs_last_error(const qs_state *h) { return h ? h->err.c_str() : g_last_error.c_str(); }
+
+qs_status qs_codec_params(qs_dtype dtype, double eps_rel, double eps_abs, int32_t *m, int32_t *L) {
+    qs::CodecParams p;
+    if (!qs::codec_params(dtype == QS_COMPLEX128, eps_rel, eps_abs, &p)) {
+        g_last_error = "eps_rel must lie in [2^-24, 1)";
+        return QS_ERR_ARG;
+    }
+    if (m) *m = p.m;
+    if (L) *L = p.L;
+    return QS_OK;
+}
+
+qs_status qs_create(qs_state **out, uint32_t n, uint32_t block_size, qs_dtype dtype, double eps_rel,
+                    double eps_abs, uint32_t flags) {
+    if (!out) return fail(nullptr, QS_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (dtype != QS_COMPLEX128 && dtype != QS_COMPLEX64) return fail(nullptr, QS_ERR_ARG, "unknown dtype");
+    if (n > 40 || block_size > n || block_size < 4)
+        return fail(nullptr, QS_ERR_ARG, "need 4 <= block_size <= n <= 40");
+    qs::CodecParams cp;
+    if (!qs::codec_params(dtype == QS_COMPLEX128, eps_rel, eps_abs, &cp))
+        return fail(nullptr, QS_ERR_ARG, "eps_rel must lie in [2^-24, 1) (BITCOMP_REL_EB)");
+    if (n - block_size > 30) return fail(nullptr, QS_ERR_ARG, "at most 2^30 blocks");
+    auto *h = new (std::nothrow) qs_state();
+    if (!h) return fail(nullptr, QS_ERR_NOMEM, "host allocation failed");
+    h->n = n;
+    h->B = block_size;
+    h->C = std::min<uint32_t>(block_size, (uint32_t)env_int("QOMPSIM_CHUNK_LOG2", qs::kMaxChunkLog2));
+    if (h->C < (uint32_t)qs::kMinChunkLog2 || h->C > (uint32_t)qs::kMaxChunkLog2) {
+        delete h;
+        return fail(nullptr, QS_ERR_ARG, "QOMPSIM_CHUNK_LOG2 must lie in [4, 8]");
+    }
+    h->nb = 1u << (n - block_size);
+    h->nchunks = uint64_t(1) << (n - h->C);
+    h->f64 = dtype == QS_COMPLEX128;
+    h->eps_rel = eps_rel;
+    h->eps_abs = eps_abs;
+    h->codec = cp;
+    h->flags = flags;
+    h->tile_log2 = env_int("QOMPSIM_TILE_LOG2", h->f64 ? 12 : 13);
+    h->tile_log2 = std::max<int>(h->tile_log2, (int)h->C + 2);
+    h->tile_log2 = std::min<int>(h->tile_log2, std::min<int>(qs::kMaxTileLog2, (int)h->C + qs::kMaxTileQubits));
+
+    auto cleanup = [&](qs_status s) { std::string m = h->err; delete h; g_last_error = m; return s; };
+#define CREATE_TRY(expr)                                                         \
+    do {                                                                         \
+        cudaError_t e__ = (expr);                                                \
+        if (e__ != cudaSuccess) {                                                \
+            h->err = std::string(#expr) + ": " + cudaGetErrorString(e__);        \
+            return cleanup(e__ == cudaErrorMemoryAllocation ? QS_ERR_CAPACITY : QS_ERR_CUDA); \
+        }                                                                        \
+    } while (0)
+
+    size_t free_b = 0, total_b = 0;
+    CREATE_TRY(cudaMemGetInfo(&free_b, &total_b));
+    const uint64_t meta_bytes = h->nchunks * sizeof(qs::ChunkMeta);
+    const uint64_t worst = h->nchunks * qs::payload_bytes((int)h->C, 32);
+    const uint64_t reserve = (uint64_t)1 << 30;
+    uint64_t avail = free_b > 2 * meta_bytes + reserve ? free_b - 2 * meta_bytes - reserve : 0;
+    const char *cap_env = std::getenv("QOMPSIM_ARENA_BYTES");
+    h->capacity = cap_env ? (uint64_t)std::strtoull(cap_env, nullptr, 10) : std::min<uint64_t>(worst, avail / 2);
+    h->capacity = (h->capacity + 127) / 128 * 128;
+    if (h->capacity < 4096) {
+        h->err = "not enough device memory for the compressed store";
+        return cleanup(QS_ERR_CAPACITY);
+    }
+    for (int i = 0; i < 2; ++i) {
+        CREATE_TRY(cudaMalloc(&h->meta[i], meta_bytes));
+        CREATE_TRY(cudaMalloc(&h->arena[i], h->capacity));
+        CREATE_TRY(cudaMemset(h->meta[i], 0, meta_bytes));
+        CREATE_TRY(cudaEventCreate(&h->ev[i]));
+    }
+    CREATE_TRY(cudaMalloc(&h->counters, 8 * sizeof(unsigned long long)));
+    CREATE_TRY(cudaMalloc(&h->mask, h->nb));
+    CREATE_TRY(cudaMalloc(&h->block_nz, h->nb * sizeof(uint32_t)));
+    CREATE_TRY(cudaMalloc(&h->block_bytes, h->nb * sizeof(unsigned long long)));
+    CREATE_TRY(cudaMalloc(&h->block_acc, h->nb * sizeof(unsigned long long)));
+    CREATE_TRY(cudaMalloc(&h->group_active, h->nb));
+    CREATE_TRY(cudaMalloc(&h->error_dev, sizeof(int32_t)));
+    CREATE_TRY(cudaMalloc(&h->dscratch, 4 * sizeof(double)));
+    CREATE_TRY(cudaMemset(h->error_dev, 0, sizeof(int32_t)));
+#undef CREATE_TRY
+    qs_status s = h->init_basis(0);
+    if (s != QS_OK) return cleanup(s);
+    if (!h->quiet()) {
+        printf("B200 fused stage pipeline, error-bounded block codec (%s)\n", h->f64 ? "complex128" : "complex64");
+        printf("  relative error bound: %g\n", eps_rel);
+        printf("  absolute error bound: %g\n", eps_abs);
+        fflush(stdout);
+    }
+    *out = h;
+    return QS_OK;
+}
+
+qs_status qs_destroy(qs_state *h) {
+    delete h;
+    return QS_OK;
+}
+
+qs_status qs_set_stream(qs_state *h, void *stream) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    h->stream = (cudaStream_t)stream;
+    return QS_OK;
+}
+
+qs_status qs_register_gates(qs_state *h, const qs_gate *gates, size_t count) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (count && !gates) return fail(h, QS_ERR_ARG, "gates is NULL");
+    std::vector<CGate> cg(count);
+    for (size_t i = 0; i < count; ++i) {
+        std::string e;
+        if (!canonicalize(gates[i], h->ref_controls(), h->n, &cg[i], &e))
+            return fail(h, strnlen(gates[i].name, 24) && std::string(gates[i].name) == "FusedSWAP"
+                               ? QS_ERR_UNSUPPORTED_GATE
+                               : (e.find("index") != std::string::npos || e.find("duplicated") != std::string::npos
+                                      ? QS_ERR_ARG
+                                      : QS_ERR_UNSUPPORTED_GATE),
+                        "gate " + std::to_string(i) + ": " + e);
+    }
+    h->gates.assign(gates, gates + count);
+    h->cgates.swap(cg);
+    h->planned = false;
+    h->stages.clear();
+    return QS_OK;
+}
+
+// partition_circuit (compressed_state.hpp:509-583).
+static std::vector<std::vector<uint32_t>> partition_circuit(const qs_state *h, uint32_t inner_size) {
+    std::vector<std::vector<uint32_t>> stages;
+    std::vector<uint32_t> cur, global_indices, global_targets;
+    const uint32_t threshold = std::max<uint32_t>(inner_size, 2u);
+    for (uint32_t i = 0; i < h->gates.size(); ++i) {
+        const qs_gate &g = h->gates[i];
+        for (uint32_t k = 0; k < g.ntargets; ++k)
+            if (g.targets[k] >= h->B) global_targets.push_back(g.targets[k]);
+        for (uint32_t k = 0; k < g.ncontrols; ++k)
+            if (g.controls[k] >= h->B) global_targets.push_back(g.controls[k]);
+        std::vector<uint32_t> tmp = global_indices;
+        for (uint32_t gt : global_targets)
+            if (std::find(tmp.begin(), tmp.end(), gt) == tmp.end()) tmp.push_back(gt);
+        if (tmp.size() > threshold) {
+            stages.push_back(cur);
+            cur.clear();
+            tmp = global_targets;
+            global_indices.clear();
+            global_targets.clear();
+        }
+        global_indices = tmp;
+        global_targets.clear();
+        cur.push_back(i);
+    }
+    if (!cur.empty()) stages.push_back(cur);
+    return stages;
+}
+
+// make_block_groups (compressed_state.hpp:585-671).
+static void make_block_groups(qs_state *h) {
+    h->b2g.assign(h->stages.size(), std::vector<uint32_t>(h->nb, 0));
+    h->num_groups.assign(h->stages.size(), 1);
+    for (size_t s = 0; s < h->stages.size(); ++s) {
+        std::vector<bool> inner(h->n, false);
+        for (uint32_t q = 0; q < h->B; ++q) inner[q] = true;
+        for (uint32_t gi : h->stages[s]) {
+            const qs_gate &g = h->gates[gi];
+            for (uint32_t k = 0; k < g.ntargets; ++k)
+                if (g.targets[k] >= h->B) inner[g.targets[k]] = true;
+            for (uint32_t k = 0; k < g.ncontrols; ++k)
+                if (g.controls[k] >= h->B) inner[g.controls[k]] = true;
+        }
+        std::vector<uint32_t> outer;
+        for (uint32_t q = 0; q < h->n; ++q)
+            if (!inner[q]) outer.push_back(q);
+        for (uint32_t b = 0; b < h->nb; ++b) {
+            uint32_t gid = 0;
+            for (size_t i = 0; i < outer.size(); ++i) gid |= ((b >> (outer[i] - h->B)) & 1u) << i;
+            h->b2g[s][b] = gid;
+        }
+        h->num_groups[s] = 1u << outer.size();
+    }
+}
+
+// Device-side plan: passes of every stage, gates with tile positions, maps.
+static qs_status build_device_plan(qs_state *h) {
+    const int C = (int)h->C;
+    const int jmax = std::min(h->tile_log2 - C, qs::kMaxTileQubits);
+    const int jmin = std::min(3, jmax);
+    std::vector<qs::KGate> kg;
+    h->passes.clear();
+    for (uint32_t s = 0; s < h->stages.size(); ++s) {
+        for (uint32_t gi : h->stages[s])
+            if (gi >= h->cgates.size()) return fail(h, QS_ERR_ARG, "stage refers to a gate index out of range");
+        auto pl = plan_passes(h->stages[s], h->cgates, C, jmax, jmin, C, (int)h->B);
+        for (size_t p = 0; p < pl.size(); ++p) {
+            qs_state::DevPass dp{};
+            dp.stage = s;
+            dp.j = (int)pl[p].tile.size();
+            if (dp.j > qs::kMaxTileQubits) return fail(h, QS_ERR_ARG, "tile plan exceeds the tile size");
+            for (int k = 0; k < dp.j; ++k) dp.tq[k] = pl[p].tile[k] - C;
+            dp.gate_off = (uint32_t)kg.size();
+            dp.ngates = (uint32_t)pl[p].gates.size();
+            dp.first = p == 0;
+            dp.final = p + 1 == pl.size();
+            for (uint32_t gi : pl[p].gates) kg.push_back(to_kgate(h->cgates[gi], pl[p].tile, C));
+            h->passes.push_back(dp);
+        }
+    }
+    if (h->kgates) { cudaFree(h->kgates); h->kgates = nullptr; }
+    if (h->b2g_dev) { cudaFree(h->b2g_dev); h->b2g_dev = nullptr; }
+    if (h->history_dev) { cudaFree(h->history_dev); h->history_dev = nullptr; }
+    if (!kg.empty()) {
+        CUDA_TRY(h, cudaMalloc(&h->kgates, kg.size() * sizeof(qs::KGate)));
+        CUDA_TRY(h, cudaMemcpy(h->kgates, kg.data(), kg.size() * sizeof(qs::KGate), cudaMemcpyHostToDevice));
+    }
+    const size_t ns = h->stages.size();
+    if (ns) {
+        CUDA_TRY(h, cudaMalloc(&h->b2g_dev, ns * h->nb * sizeof(uint32_t)));
+        for (size_t s = 0; s < ns; ++s)
+            CUDA_TRY(h, cudaMemcpy(h->b2g_dev + s * h->nb, h->b2g[s].data(), h->nb * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice));
+        uint32_t gmax = *std::max_element(h->num_groups.begin(), h->num_groups.end());
+        if (gmax > h->nb) return fail(h, QS_ERR_ARG, "num_groups larger than the number of blocks");
+    }
+    h->history_cap = 2 * ns + 1;
+    CUDA_TRY(h, cudaMalloc(&h->history_dev, h->history_cap * sizeof(unsigned long long)));
+    for (auto e : h->pass_ev) cudaEventDestroy(e);
+    h->pass_ev.clear();
+    if (h->flags & QS_FLAG_PROFILE) {
+        h->pass_ev.resize(2 * h->passes.size());
+        for (auto &e : h->pass_ev) CUDA_TRY(h, cudaEventCreate(&e));
+    }
+    h->planned = true;
+    return QS_OK;
+}
+
+qs_status qs_partition(qs_state *h, uint32_t inner_size, int verbose) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    for (const auto &g : h->gates)
+        if (std::string(g.name, strnlen(g.name, 24)) == "FusedSWAP")
+            return fail(h, QS_ERR_UNSUPPORTED_GATE, "FusedSWAP needs MPI ranks");
+    h->stages = partition_circuit(h, inner_size);
+    make_block_groups(h);
+    qs_status s = build_device_plan(h);
+    if (s != QS_OK) return s;
+    if (verbose > 0) {
+        printf("Circuit Stages: [");
+        for (size_t i = 0; i < h->stages.size(); ++i)
+            printf("%zu%s", h->stages[i].size(), i + 1 == h->stages.size() ? "" : ", ");
+        printf("]\n");
+    }
+    if (verbose > 1) {
+        printf("\n=== Block Groups ===\n");
+        for (size_t s2 = 0; s2 < h->stages.size(); ++s2) {
+            printf("Stage %zu block groups:\n", s2);
+            std::vector<std::vector<uint32_t>> groups(h->num_groups[s2]);
+            for (uint32_t b = 0; b < h->nb; ++b) groups[h->b2g[s2][b]].push_back(b);
+            for (size_t g = 0; g < groups.size(); ++g) {
+                printf("  Group %zu: [", g);
+                for (size_t i = 0; i < groups[g].size(); ++i)
+                    printf("%u%s", groups[g][i], i + 1 == groups[g].size() ? "" : ", ");
+                printf("]\n");
+            }
+        }
+    }
+    fflush(stdout);
+    return QS_OK;
+}
+
+qs_status qs_register_stages(qs_state *h, const uint32_t *stage_sizes, size_t nstages, const uint32_t *ids,
+                             const uint32_t *block_to_group, const uint32_t *num_groups) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (nstages && (!stage_sizes || !block_to_group || !num_groups)) return fail(h, QS_ERR_ARG, "NULL argument");
+    h->stages.assign(nstages, {});
+    size_t off = 0;
+    for (size_t s = 0; s < nstages; ++s) {
+        if (stage_sizes[s] && !ids) return fail(h, QS_ERR_ARG, "stage_gate_ids is NULL");
+        h->stages[s].assign(ids + off, ids + off + stage_sizes[s]);
+        off += stage_sizes[s];
+    }
+    h->b2g.assign(nstages, std::vector<uint32_t>(h->nb));
+    h->num_groups.assign(num_groups, num_groups + nstages);
+    for (size_t s = 0; s < nstages; ++s) {
+        for (uint32_t b = 0; b < h->nb; ++b) {
+            const uint32_t g = block_to_group[s * h->nb + b];
+            if (g >= h->num_groups[s]) return fail(h, QS_ERR_ARG, "group id out of range");
+            h->b2g[s][b] = g;
+        }
+    }
+    return build_device_plan(h);
+}
+
+qs_status qs_plan_stages(const qs_gate *gates, size_t count, uint32_t n, uint32_t block_size, uint32_t inner_size,
+                         size_t *nstages, uint32_t *stage_sizes, uint32_t *stage_gate_ids, uint32_t *block_to_group,
+                         uint32_t *num_groups) {
+    if (!nstages || (count && !gates)) return fail(nullptr, QS_ERR_ARG, "NULL argument");
+    if (n > 40 || block_size > n || n - block_size > 30) return fail(nullptr, QS_ERR_ARG, "bad geometry");
+    qs_state tmp;  // host-only: no device allocation happens for a default state
+    tmp.n = n;
+    tmp.B = block_size;
+    tmp.nb = 1u << (n - block_size);
+    tmp.gates.assign(gates, gates + count);
+    for (size_t i = 0; i < count; ++i) {
+        for (uint32_t k = 0; k < gates[i].ntargets && k < 2; ++k)
+            if (gates[i].targets[k] >= n) return fail(nullptr, QS_ERR_ARG, "gate target index out of range");
+        for (uint32_t k = 0; k < gates[i].ncontrols && k < 2; ++k)
+            if (gates[i].controls[k] >= n) return fail(nullptr, QS_ERR_ARG, "gate control index out of range");
+    }
+    tmp.stages = partition_circuit(&tmp, inner_size);
+    make_block_groups(&tmp);
+    *nstages = tmp.stages.size();
+    size_t off = 0;
+    for (size_t s = 0; s < tmp.stages.size(); ++s) {
+        if (stage_sizes) stage_sizes[s] = (uint32_t)tmp.stages[s].size();
+        if (stage_gate_ids)
+            for (uint32_t g : tmp.stages[s]) stage_gate_ids[off++] = g;
+        if (block_to_group) std::memcpy(block_to_group + s * tmp.nb, tmp.b2g[s].data(), tmp.nb * sizeof(uint32_t));
+        if (num_groups) num_groups[s] = tmp.num_groups[s];
+    }
+    return QS_OK;
+}
+
+qs_status qs_get_plan_info(qs_state *h, uint32_t *nstages, uint32_t *nblocks) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (nstages) *nstages = (uint32_t)h->stages.size();
+    if (nblocks) *nblocks = h->nb;
+    return QS_OK;
+}
+
+qs_status qs_get_stage(qs_state *h, uint32_t stage, uint32_t *gate_ids, uint32_t cap, uint32_t *count,
+                       uint32_t *block_to_group, uint32_t *num_groups) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (stage >= h->stages.size()) return fail(h, QS_ERR_ARG, "stage out of range");
+    const auto &st = h->stages[stage];
+    if (count) *count = (uint32_t)st.size();
+    if (gate_ids)
+        for (uint32_t i = 0; i < std::min<uint32_t>(cap, (uint32_t)st.size()); ++i) gate_ids[i] = st[i];
+    if (block_to_group) std::memcpy(block_to_group, h->b2g[stage].data(), h->nb * sizeof(uint32_t));
+    if (num_groups) *num_groups = h->num_groups[stage];
+    return QS_OK;
+}
+
+qs_status qs_apply_circuit(qs_state *h) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (!h->planned) return fail(h, QS_ERR_STATE, "no registered circuit: call qs_partition or qs_register_stages");
+    cudaStream_t s = h->stream;
+    const int C = (int)h->C;
+    if (!h->quiet()) {
+        printf("# of PUs per rank: 1\n# of streams per PU: 1\n");
+        fflush(stdout);
+    }
+    CUDA_TRY(h, cudaMemsetAsync(h->counters, 0, 8 * sizeof(unsigned long long), s));
+    CUDA_TRY(h, cudaMemsetAsync(h->history_dev, 0, h->history_cap * sizeof(unsigned long long), s));
+    CUDA_TRY(h, cudaMemsetAsync(h->error_dev, 0, sizeof(int32_t), s));
+    CUDA_TRY(h, qs::launch_sum_mask_bytes(h->mask, h->block_bytes, h->nb, h->history_dev, s));
+    CUDA_TRY(h, cudaEventRecord(h->ev[0], s));
+    size_t pi = 0;
+    for (uint32_t st = 0; st < h->stages.size(); ++st) {
+        const uint32_t *b2g = h->b2g_dev + (size_t)st * h->nb;
+        CUDA_TRY(h, qs::launch_stage_begin(b2g, h->mask, h->nb, h->group_active, h->num_groups[st], h->block_nz,
+                                           h->block_acc, h->history_dev + h->stages.size() + 1 + st, s));
+        for (; pi < h->passes.size() && h->passes[pi].stage == st; ++pi) {
+            const auto &dp = h->passes[pi];
+            const int out = h->cur ^ 1;
+            CUDA_TRY(h, cudaMemsetAsync(h->counters + out, 0, sizeof(unsigned long long), s));
+            qs::PassArgs a{};
+            a.n = (int)h->n;
+            a.B = (int)h->B;
+            a.C = C;
+            a.j = dp.j;
+            for (int k = 0; k < dp.j; ++k) a.tq[k] = dp.tq[k];
+            a.n_tiles = uint64_t(1) << (h->n - C - dp.j);
+            a.gates = h->kgates + dp.gate_off;
+            a.ngates = (int)dp.ngates;
+            a.codec = h->codec;
+            a.meta_in = h->meta[h->cur];
+            a.arena_in = h->arena[h->cur];
+            a.meta_out = h->meta[out];
+            a.arena_out = h->arena[out];
+            a.bump = h->counters + out;
+            a.capacity = h->capacity;
+            a.block_to_group = b2g;
+            a.group_active = h->group_active;
+            a.mask = h->mask;
+            a.first_pass = dp.first;
+            a.final_pass = dp.final;
+            a.exact_zero = (h->flags & QS_FLAG_CODE_ZERO_TEST) ? 0 : 1;
+            a.block_nz = h->block_nz;
+            a.block_bytes = h->block_acc;
+            a.error = h->error_dev;
+            a.stats = h->counters + 2;
+            if (!h->pass_ev.empty()) CUDA_TRY(h, cudaEventRecord(h->pass_ev[2 * pi], s));
+            CUDA_TRY(h, qs::launch_pass(h->f64, a, h->tile_log2, s));
+            if (!h->pass_ev.empty()) CUDA_TRY(h, cudaEventRecord(h->pass_ev[2 * pi + 1], s));
+            h->cur = out;
+        }
+        CUDA_TRY(h, qs::launch_stage_end(b2g, h->group_active, h->nb, h->block_nz, h->block_acc, h->mask,
+                                         h->block_bytes, h->history_dev + st + 1, s));
+    }
+    CUDA_TRY(h, cudaEventRecord(h->ev[1], s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
+    int32_t errflag = 0;
+    unsigned long long ctr[8];
+    CUDA_TRY(h, cudaMemcpy(&errflag, h->error_dev, sizeof(errflag), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(ctr, h->counters, sizeof(ctr), cudaMemcpyDeviceToHost));
+    std::vector<unsigned long long> hist(h->history_cap);
+    CUDA_TRY(h, cudaMemcpy(hist.data(), h->history_dev, hist.size() * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost));
+    float ms = 0;
+    CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
+    if (errflag)
+        return fail(h, QS_ERR_CAPACITY,
+                    "compressed store overflowed its arena (" + std::to_string(h->capacity) +
+                        " bytes); the state is invalid.  Set QOMPSIM_ARENA_BYTES larger.");
+    if (!h->passes.empty()) h->arena_used = ctr[h->cur];
+    const size_t ns = h->stages.size();
+    h->history.assign(hist.begin(), hist.begin() + ns + 1);
+    uint64_t updates = 0;
+    for (size_t st = 0; st < ns; ++st) updates += (uint64_t)h->stages[st].size() * hist[ns + 1 + st] << h->B;
+    double pass_ms = 0;
+    for (size_t p = 0; p < h->pass_ev.size() / 2; ++p) {
+        float t = 0;
+        CUDA_TRY(h, cudaEventElapsedTime(&t, h->pass_ev[2 * p], h->pass_ev[2 * p + 1]));
+        pass_ms += t;
+    }
+    h->times[1] += ms / 1000.0;
+    h->st.stages = h->stages.size();
+    h->st.passes = h->passes.size();
+    h->st.bytes_read = ctr[2];
+    h->st.bytes_written = ctr[3];
+    h->st.tiles = ctr[4];
+    h->st.amp_gate_updates = updates;
+    h->st.kernel_ms = h->pass_ev.empty() ? ms : pass_ms;
+    h->st.apply_ms = ms;
+    h->st.mantissa_bits = h->codec.m;
+    h->st.linear_exp = h->codec.L;
+    h->st.chunk_log2 = (int32_t)h->C;
+    h->st.tile_log2 = h->tile_log2;
+    if (!h->quiet()) {
+        printf("Total SV bytes: %s\n", format_size(hist[0]).c_str());
+        for (size_t st = 0; st < ns; ++st)
+            printf("[Stage %zu/%zu] Total SV bytes: %s\n", st, h->stages.size() - 1, format_size(hist[st + 1]).c_str());
+        fflush(stdout);
+    }
+    return QS_OK;
+}
+
+qs_status qs_norm_squared(qs_state *h, double *out) {
+    if (!h || !out) return fail(h, QS_ERR_ARG, "NULL argument");
+    CUDA_TRY(h, cudaMemsetAsync(h->dscratch, 0, sizeof(double), h->stream));
+    CUDA_TRY(h, qs::launch_norm(h->f64, h->meta[h->cur], h->arena[h->cur], h->mask, (int)h->B, (int)h->C, h->codec,
+                                h->nchunks, h->dscratch, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(out, h->dscratch, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return QS_OK;
+}
+
+qs_status qs_get_vector(qs_state *h, double *out, int renormalize) {
+    if (!h || !out) return fail(h, QS_ERR_ARG, "NULL argument");
+    double scale = 1.0;
+    if (renormalize) {
+        double nrm = 0;
+        qs_status s = qs_norm_squared(h, &nrm);
+        if (s != QS_OK) return s;
+        if (nrm > 0) scale = 1.0 / std::sqrt(nrm);
+    }
+    const uint64_t chunk_amps = uint64_t(1) << h->C;
+    const uint64_t slab_chunks = std::max<uint64_t>(1, (uint64_t(1) << 24) / chunk_amps);
+    double *dbuf = nullptr;
+    const uint64_t nslab = std::min<uint64_t>(slab_chunks, h->nchunks);
+    CUDA_TRY(h, cudaMalloc(&dbuf, nslab * chunk_amps * 2 * sizeof(double)));
+    qs_status rs = QS_OK;
+    for (uint64_t c0 = 0; c0 < h->nchunks; c0 += nslab) {
+        const uint64_t cnt = std::min<uint64_t>(nslab, h->nchunks - c0);
+        cudaError_t e = qs::launch_readout(h->f64, h->meta[h->cur], h->arena[h->cur], h->mask, (int)h->B, (int)h->C,
+                                           h->codec, c0, cnt, dbuf, scale, h->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(out + c0 * chunk_amps * 2, dbuf, cnt * chunk_amps * 2 * sizeof(double),
+                                cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) {
+            h->err = std::string("readout: ") + cudaGetErrorString(e);
+            rs = QS_ERR_CUDA;
+            break;
+        }
+    }
+    cudaFree(dbuf);
+    return rs;
+}
+
+qs_status qs_get_zero_mask(qs_state *h, uint8_t *out) {
+    if (!h || !out) return fail(h, QS_ERR_ARG, "NULL argument");
+    CUDA_TRY(h, cudaMemcpyAsync(out, h->mask, h->nb, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return QS_OK;
+}
+
+qs_status qs_get_block_bytes(qs_state *h, uint64_t *out) {
+    if (!h || !out) return fail(h, QS_ERR_ARG, "NULL argument");
+    CUDA_TRY(h, cudaMemcpyAsync(out, h->block_bytes, h->nb * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return QS_OK;
+}
+
+qs_status qs_get_max_sv_bytes(qs_state *h, uint64_t *out) {
+    if (!h || !out) return fail(h, QS_ERR_ARG, "NULL argument");
+    uint64_t m = 0;
+    for (uint64_t v : h->history) m = std::max(m, v);
+    *out = m;
+    return QS_OK;
+}
+
+qs_status qs_get_sv_bytes_history(qs_state *h, uint64_t *out, size_t cap, size_t *count) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (count) *count = h->history.size();
+    if (out)
+        for (size_t i = 0; i < std::min(cap, h->history.size()); ++i) out[i] = h->history[i];
+    return QS_OK;
+}
+
+qs_status qs_get_total_times(qs_state *h, double out[10]) {
+    if (!h || !out) return fail(h, QS_ERR_ARG, "NULL argument");
+    for (int i = 0; i < 10; ++i) out[i] = h->times[i];
+    (void)kTimerKeys;
+    return QS_OK;
+}
+
+qs_status qs_get_stats(qs_state *h, qs_stats *out) {
+    if (!h || !out) return fail(h, QS_ERR_ARG, "NULL argument");
+    *out = h->st;
+    return QS_OK;
+}
+
+qs_status qs_set_basis_state(qs_state *h, uint64_t basis) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (basis >> h->n) return fail(h, QS_ERR_ARG, "basis index out of range");
+    return h->init_basis(basis);
+}
+
+qs_status qs_load_vector(qs_state *h, const double *vec) {
+    if (!h || !vec) return fail(h, QS_ERR_ARG, "NULL argument");
+    cudaStream_t s = h->stream;
+    const uint64_t chunk_amps = uint64_t(1) << h->C;
+    const uint64_t nslab = std::min<uint64_t>(std::max<uint64_t>(1, (uint64_t(1) << 24) / chunk_amps), h->nchunks);
+    double *dbuf = nullptr;
+    CUDA_TRY(h, cudaMalloc(&dbuf, nslab * chunk_amps * 2 * sizeof(double)));
+    auto done = [&](qs_status st) { cudaFree(dbuf); return st; };
+    if (cudaMemsetAsync(h->counters + h->cur, 0, sizeof(unsigned long long), s) != cudaSuccess ||
+        cudaMemsetAsync(h->block_nz, 0, h->nb * sizeof(uint32_t), s) != cudaSuccess ||
+        cudaMemsetAsync(h->block_acc, 0, h->nb * sizeof(unsigned long long), s) != cudaSuccess ||
+        cudaMemsetAsync(h->error_dev, 0, sizeof(int32_t), s) != cudaSuccess)
+        return done(fail(h, QS_ERR_CUDA, "memset failed"));
+    for (uint64_t c0 = 0; c0 < h->nchunks; c0 += nslab) {
+        const uint64_t cnt = std::min<uint64_t>(nslab, h->nchunks - c0);
+        cudaError_t e = cudaMemcpyAsync(dbuf, vec + c0 * chunk_amps * 2, cnt * chunk_amps * 2 * sizeof(double),
+                                        cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+            e = qs::launch_encode(h->f64, dbuf, (int)h->B, (int)h->C, h->codec, c0, cnt, h->meta[h->cur],
+                                  h->arena[h->cur], h->counters + h->cur, h->capacity, h->block_nz, h->block_acc,
+                                  h->error_dev, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return done(fail(h, QS_ERR_CUDA, std::string("load: ") + cudaGetErrorString(e)));
+    }
+    // mask = any non-zero in block; block bytes of zero blocks = 0
+    std::vector<uint32_t> nz(h->nb);
+    std::vector<unsigned long long> acc(h->nb);
+    int32_t errflag = 0;
+    unsigned long long used = 0;
+    if (cudaMemcpy(nz.data(), h->block_nz, h->nb * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(acc.data(), h->block_acc, h->nb * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(&errflag, h->error_dev, 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(&used, h->counters + h->cur, 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return done(fail(h, QS_ERR_CUDA, "load readback failed"));
+    if (errflag) return done(fail(h, QS_ERR_CAPACITY, "vector does not fit the arena"));
+    std::vector<uint8_t> mk(h->nb);
+    unsigned long long total = 0;
+    for (uint32_t b = 0; b < h->nb; ++b) {
+        mk[b] = nz[b] ? 1 : 0;
+        if (!mk[b]) acc[b] = 0;
+        total += acc[b];
+    }
+    if (cudaMemcpy(h->mask, mk.data(), h->nb, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->block_bytes, acc.data(), h->nb * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+        return done(fail(h, QS_ERR_CUDA, "load upload failed"));
+    h->arena_used = used;
+    h->history.assign(1, total);
+    return done(QS_OK);
+}
+
+// ---- store serialisation
+struct StoreHeader {
+    char magic[8];
+    uint32_t n, B, C, f64;
+    int32_t m, L;
+    uint64_t nb, nchunks, arena_bytes;
+};
+
+qs_status qs_export_store(qs_state *h, void *buf, uint64_t cap, uint64_t *size) {
+    if (!h || !size) return fail(h, QS_ERR_ARG, "NULL argument");
+    const uint64_t nbpad = (h->nb + 7) / 8 * 8;
+    const uint64_t need = sizeof(StoreHeader) + nbpad + h->nb * 8 + h->nchunks * sizeof(qs::ChunkMeta) + h->arena_used;
+    *size = need;
+    if (!buf) return QS_OK;
+    if (cap < need) return fail(h, QS_ERR_ARG, "export buffer too small");
+    StoreHeader hd{};
+    std::memcpy(hd.magic, "QSSTORE1", 8);
+    hd.n = h->n; hd.B = h->B; hd.C = h->C; hd.f64 = h->f64;
+    hd.m = h->codec.m; hd.L = h->codec.L;
+    hd.nb = h->nb; hd.nchunks = h->nchunks; hd.arena_bytes = h->arena_used;
+    char *p = (char *)buf;
+    std::memcpy(p, &hd, sizeof(hd));
+    p += sizeof(hd);
+    cudaStream_t s = h->stream;
+    CUDA_TRY(h, cudaMemcpyAsync(p, h->mask, h->nb, cudaMemcpyDeviceToHost, s));
+    p += nbpad;
+    CUDA_TRY(h, cudaMemcpyAsync(p, h->block_bytes, h->nb * 8, cudaMemcpyDeviceToHost, s));
+    p += h->nb * 8;
+    CUDA_TRY(h, cudaMemcpyAsync(p, h->meta[h->cur], h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyDeviceToHost, s));
+    p += h->nchunks * sizeof(qs::ChunkMeta);
+    if (h->arena_used) CUDA_TRY(h, cudaMemcpyAsync(p, h->arena[h->cur], h->arena_used, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
+    h->times[8] += 0;  // d2h time is measured by callers with their own events
+    return QS_OK;
+}
+
+qs_status qs_import_store(qs_state *h, const void *buf, uint64_t size) {
+    if (!h || !buf) return fail(h, QS_ERR_ARG, "NULL argument");
+    if (size < sizeof(StoreHeader)) return fail(h, QS_ERR_CORRUPT, "store shorter than its header");
+    StoreHeader hd;
+    std::memcpy(&hd, buf, sizeof(hd));
+    if (std::memcmp(hd.magic, "QSSTORE1", 8) != 0 || hd.n != h->n || hd.B != h->B || hd.C != h->C ||
+        hd.f64 != (uint32_t)h->f64 || hd.m != h->codec.m || hd.L != h->codec.L || hd.nb != h->nb ||
+        hd.nchunks != h->nchunks)
+        return fail(h, QS_ERR_CORRUPT, "store header does not match this state's geometry or codec");
+    const uint64_t nbpad = (h->nb + 7) / 8 * 8;
+    const uint64_t need = sizeof(StoreHeader) + nbpad + h->nb * 8 + h->nchunks * sizeof(qs::ChunkMeta) + hd.arena_bytes;
+    if (size != need) return fail(h, QS_ERR_CORRUPT, "store length does not match its header");
+    if (hd.arena_bytes > h->capacity) return fail(h, QS_ERR_CAPACITY, "store larger than the arena");
+    const char *p = (const char *)buf + sizeof(hd);
+    cudaStream_t s = h->stream;
+    CUDA_TRY(h, cudaMemcpyAsync(h->mask, p, h->nb, cudaMemcpyHostToDevice, s));
+    p += nbpad;
+    CUDA_TRY(h, cudaMemcpyAsync(h->block_bytes, p, h->nb * 8, cudaMemcpyHostToDevice, s));
+    std::vector<uint64_t> bb(h->nb);
+    std::memcpy(bb.data(), p, h->nb * 8);
+    p += h->nb * 8;
+    CUDA_TRY(h, cudaMemcpyAsync(h->meta[h->cur], p, h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyHostToDevice, s));
+    p += h->nchunks * sizeof(qs::ChunkMeta);
+    if (hd.arena_bytes) CUDA_TRY(h, cudaMemcpyAsync(h->arena[h->cur], p, hd.arena_bytes, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
+    h->arena_used = hd.arena_bytes;
+    uint64_t total = 0;
+    for (uint64_t v : bb) total += v;
+    h->history.assign(1, total);
+    return QS_OK;
+}
+
+}  // extern "C"
+
+// =====================================================================
+// dense state
+// =====================================================================
+struct qs_dense {
+    uint32_t n = 0;
+    bool f64 = true;
+    void *state = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err = "no error";
+    qs::KGate *kg = nullptr;
+    size_t kg_cap = 0;
+    double *dscratch = nullptr;
+    ~qs_dense() {
+        if (state) cudaFree(state);
+        if (kg) cudaFree(kg);
+        if (dscratch) cudaFree(dscratch);
+    }
+    uint64_t dim() const { return uint64_t(1) << n; }
+    size_t amp_bytes() const { return f64 ? 16 : 8; }
+};
+
+static qs_status dfail(qs_dense *h, qs_status s, const std::string &m) {
+    if (h) h->err = m;
+    else g_last_error = m;
+    return s;
+}
+
+static qs_status dense_upload_gates(qs_dense *h, const std::vector<qs::KGate> &kg) {
+    if (kg.size() > h->kg_cap) {
+        if (h->kg) cudaFree(h->kg);
+        h->kg = nullptr;
+        h->kg_cap = 0;
+        CUDA_TRY(h, cudaMalloc(&h->kg, kg.size() * sizeof(qs::KGate)));
+        h->kg_cap = kg.size();
+    }
+    if (!kg.empty())
+        CUDA_TRY(h, cudaMemcpyAsync(h->kg, kg.data(), kg.size() * sizeof(qs::KGate), cudaMemcpyHostToDevice, h->stream));
+    return QS_OK;
+}
+
+extern "C" {
+
+const char *qs_dense_last_error(const qs_dense *h) { return h ? h->err.c_str() : g_last_error.c_str(); }
+
+qs_status qs_dense_create(qs_dense **out, uint32_t n, qs_dtype dtype) {
+    if (!out) return dfail(nullptr, QS_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (n < 1 || n > 36) return dfail(nullptr, QS_ERR_ARG, "need 1 <= n <= 36");
+    if (dtype != QS_COMPLEX128 && dtype != QS_COMPLEX64) return dfail(nullptr, QS_ERR_ARG, "unknown dtype");
+    auto *h = new (std::nothrow) qs_dense();
+    if (!h) return dfail(nullptr, QS_ERR_NOMEM, "host allocation failed");
+    h->n = n;
+    h->f64 = dtype == QS_COMPLEX128;
+    cudaError_t e = cudaMalloc(&h->state, h->dim() * h->amp_bytes());
+    if (e == cudaSuccess) e = cudaMalloc(&h->dscratch, 4 * sizeof(double));
+    if (e != cudaSuccess) {
+        std::string m = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        delete h;
+        return dfail(nullptr, e == cudaErrorMemoryAllocation ? QS_ERR_CAPACITY : QS_ERR_CUDA, m);
+    }
+    qs_status s = qs_dense_set_basis_state(h, 0);
+    if (s != QS_OK) {
+        std::string m = h->err;
+        delete h;
+        return dfail(nullptr, s, m);
+    }
+    *out = h;
+    return QS_OK;
+}
+
+qs_status qs_dense_destroy(qs_dense *h) {
+    delete h;
+    return QS_OK;
+}
+
+qs_status qs_dense_set_stream(qs_dense *h, void *stream) {
+    if (!h) return dfail(nullptr, QS_ERR_ARG, "NULL handle");
+    h->stream = (cudaStream_t)stream;
+    return QS_OK;
+}
+
+qs_status qs_dense_set_basis_state(qs_dense *h, uint64_t basis) {
+    if (!h) return dfail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (basis >> h->n) return dfail(h, QS_ERR_ARG, "basis index out of range");
+    CUDA_TRY(h, cudaMemsetAsync(h->state, 0, h->dim() * h->amp_bytes(), h->stream));
+    if (h->f64) {
+        const double one[2] = {1.0, 0.0};
+        CUDA_TRY(h, cudaMemcpyAsync((char *)h->state + basis * 16, one, 16, cudaMemcpyHostToDevice, h->stream));
+    } else {
+        const float one[2] = {1.0f, 0.0f};
+        CUDA_TRY(h, cudaMemcpyAsync((char *)h->state + basis * 8, one, 8, cudaMemcpyHostToDevice, h->stream));
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return QS_OK;
+}
+
+static qs_status dense_canon(qs_dense *h, const qs_gate *gates, size_t count, std::vector<CGate> *cg) {
+    cg->resize(count);
+    for (size_t i = 0; i < count; ++i) {
+        std::string e;
+        if (!canonicalize(gates[i], false, h->n, &(*cg)[i], &e))
+            return dfail(h, e.find("index") != std::string::npos ? QS_ERR_ARG : QS_ERR_UNSUPPORTED_GATE,
+                         "gate " + std::to_string(i) + ": " + e);
+    }
+    return QS_OK;
+}
+
+qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) {
+    if (!h) return dfail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (count && !gates) return dfail(h, QS_ERR_ARG, "gates is NULL");
+    if (!count) return QS_OK;
+    std::vector<CGate> cg;
+    qs_status s = dense_canon(h, gates, count, &cg);
+    if (s != QS_OK) return s;
+    const int C = (int)std::min<uint32_t>(h->n, (uint32_t)env_int("QOMPSIM_DENSE_CHUNK_LOG2", 5));
+    const int tl = env_int("QOMPSIM_DENSE_TILE_LOG2", h->f64 ? 12 : 13);
+    const int tile_log2 = std::min<int>((int)h->n, std::min<int>(tl, C + qs::kMaxTileQubits));
+    const int jmax = tile_log2 - C;
+    std::vector<uint32_t> ids(count);
+    for (size_t i = 0; i < count; ++i) ids[i] = (uint32_t)i;
+    auto pl = plan_passes(ids, cg, C, jmax, std::min(jmax, 3), C, (int)h->n);
+    std::vector<qs::KGate> kg;
+    for (auto &p : pl)
+        for (uint32_t gi : p.gates) kg.push_back(to_kgate(cg[gi], p.tile, C));
+    s = dense_upload_gates(h, kg);
+    if (s != QS_OK) return s;
+    size_t off = 0;
+    for (auto &p : pl) {
+        qs::DensePassArgs a{};
+        a.n = (int)h->n;
+        a.C = C;
+        a.j = (int)p.tile.size();
+        for (int k = 0; k < a.j; ++k) a.tq[k] = p.tile[k] - C;
+        a.n_tiles = uint64_t(1) << (h->n - C - a.j);
+        a.gates = h->kg + off;
+        a.ngates = (int)p.gates.size();
+        a.state = h->state;
+        off += p.gates.size();
+        CUDA_TRY(h, qs::launch_dense_pass(h->f64, a, tile_log2, h->stream));
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return QS_OK;
+}
+
+qs_status qs_dense_apply_gates_pergate(qs_dense *h, const qs_gate *gates, size_t count) {
+    if (!h) return dfail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (count && !gates) return dfail(h, QS_ERR_ARG, "gates is NULL");
+    if (!count) return QS_OK;
+    std::vector<CGate> cg;
+    qs_status s = dense_canon(h, gates, count, &cg);
+    if (s != QS_OK) return s;
+    if (h->n < 2) {
+        for (auto &g : cg)
+            if (g.nq == 2) return dfail(h, QS_ERR_ARG, "two-qubit gate on a one-qubit state");
+    }
+    std::vector<qs::KGate> kg;
+    for (auto &g : cg) kg.push_back(to_kgate(g, {}, 64));
+    s = dense_upload_gates(h, kg);
+    if (s != QS_OK) return s;
+    for (size_t i = 0; i < kg.size(); ++i) CUDA_TRY(h, qs::launch_pergate(h->f64, h->state, (int)h->n, h->kg + i, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return QS_OK;
+}
+
+qs_status qs_dense_get_vector(qs_dense *h, double *out) {
+    if (!h || !out) return dfail(h, QS_ERR_ARG, "NULL argument");
+    if (h->f64) {
+        CUDA_TRY(h, cudaMemcpyAsync(out, h->state, h->dim() * 16, cudaMemcpyDeviceToHost, h->stream));
+    } else {
+        double *tmp = nullptr;
+        CUDA_TRY(h, cudaMalloc(&tmp, h->dim() * 16));
+        cudaError_t e = qs::launch_dense_to_c128(false, h->state, h->dim(), tmp, h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, h->dim() * 16, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        cudaFree(tmp);
+        if (e != cudaSuccess) return dfail(h, QS_ERR_CUDA, std::string("get_vector: ") + cudaGetErrorString(e));
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return QS_OK;
+}
+
+qs_status qs_dense_set_vector(qs_dense *h, const double *in) {
+    if (!h || !in) return dfail(h, QS_ERR_ARG, "NULL argument");
+    if (h->f64) {
+        CUDA_TRY(h, cudaMemcpyAsync(h->state, in, h->dim() * 16, cudaMemcpyHostToDevice, h->stream));
+    } else {
+        double *tmp = nullptr;
+        CUDA_TRY(h, cudaMalloc(&tmp, h->dim() * 16));
+        cudaError_t e = cudaMemcpyAsync(tmp, in, h->dim() * 16, cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess) e = qs::launch_c128_to_dense(false, tmp, h->dim(), h->state, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        cudaFree(tmp);
+        if (e != cudaSuccess) return dfail(h, QS_ERR_CUDA, std::string("set_vector: ") + cudaGetErrorString(e));
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return QS_OK;
+}
+
+qs_status qs_dense_norm_squared(qs_dense *h, double *out) {
+    if (!h || !out) return dfail(h, QS_ERR_ARG, "NULL argument");
+    CUDA_TRY(h, cudaMemsetAsync(h->dscratch, 0, sizeof(double), h->stream));
+    CUDA_TRY(h, qs::launch_dense_norm(h->f64, h->state, h->dim(), h->dscratch, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(out, h->dscratch, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return QS_OK;
+}
+
+qs_status qs_dense_device_ptr(qs_dense *h, void **out) {
+    if (!h || !out) return dfail(h, QS_ERR_ARG, "NULL argument");
+    *out = h->state;
+    return QS_OK;
+}
+
+// Device codec round trip used by the CPU/GPU bit-identity tests.
+qs_status qs_codec_test(qs_dtype dtype, double eps_rel, double eps_abs, uint32_t chunk_log2, const void *vals,
+                        uint64_t nchunks, uint32_t *words, int32_t *bases, uint32_t *widths, void *decoded) {
+    qs::CodecParams p;
+    const bool f64 = dtype == QS_COMPLEX128;
+    if (!qs::codec_params(f64, eps_rel, eps_abs, &p)) return dfail(nullptr, QS_ERR_ARG, "bad error bounds");
+    if (chunk_log2 < (uint32_t)qs::kMinChunkLog2 || chunk_log2 > (uint32_t)qs::kMaxChunkLog2 || !vals || !words ||
+        !bases || !widths || !decoded)
+        return dfail(nullptr, QS_ERR_ARG, "bad argument");
+    const uint64_t ncomp = (uint64_t(2) << chunk_log2) * nchunks;
+    const size_t rsz = f64 ? 8 : 4;
+    const uint64_t max_words = (uint64_t(2) << chunk_log2) * nchunks;  // width 32 -> one word per component
+    void *dv = nullptr, *dd = nullptr;
+    uint32_t *dw = nullptr;
+    int32_t *db = nullptr;
+    uint32_t *dwi = nullptr;
+    cudaError_t e = cudaMalloc(&dv, ncomp * rsz);
+    if (e == cudaSuccess) e = cudaMalloc(&dd, ncomp * rsz);
+    if (e == cudaSuccess) e = cudaMalloc(&dw, max_words * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&db, nchunks * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&dwi, nchunks * 4);
+    if (e == cudaSuccess) e = cudaMemset(dw, 0, max_words * 4);
+    if (e == cudaSuccess) e = cudaMemcpy(dv, vals, ncomp * rsz, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = qs::launch_codec_test(f64, dv, (int)chunk_log2, p, nchunks, dw, db, dwi, dd, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(words, dw, max_words * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(bases, db, nchunks * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(widths, dwi, nchunks * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(decoded, dd, ncomp * rsz, cudaMemcpyDeviceToHost);
+    cudaFree(dv);
+    cudaFree(dd);
+    cudaFree(dw);
+    cudaFree(db);
+    cudaFree(dwi);
+    if (e != cudaSuccess) return dfail(nullptr, QS_ERR_CUDA, std::string("codec test: ") + cudaGetErrorString(e));
+    return QS_OK;
+}
+
+}  // extern "C"

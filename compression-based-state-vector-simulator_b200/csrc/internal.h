@@ -1,0 +1,125 @@
+// Internal interface between the host engine (engine.cpp) and the device code
+// (kernels.cu).  Not part of the C ABI.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace qs {
+
+// Largest chunk: 2^8 amplitudes = 512 real components = 16 per lane.
+constexpr int kMaxChunkLog2 = 8;
+constexpr int kMinChunkLog2 = 4;
+constexpr int kMaxPerLane = (2 << kMaxChunkLog2) / 32;
+// Largest tile: 2^14 amplitudes; at most kMaxTileQubits qubits above the chunk.
+constexpr int kMaxTileLog2 = 14;
+constexpr int kMaxTileQubits = 10;
+constexpr int kPassThreads = 256;
+
+// Header of one encoded chunk (16 bytes).  offset is a byte offset into the
+// payload arena; the payload is 128 * rows bytes (see codec.cuh).
+struct ChunkMeta {
+    uint64_t offset;
+    int32_t base;
+    uint32_t width;
+};
+static_assert(sizeof(ChunkMeta) == 16, "chunk header is 16 bytes");
+
+// A gate as the device applies it: nq (1 or 2) qubits in ascending order,
+// matrix index bit i <-> q[i], complex128 row-major interleaved.  tpos[i] is
+// the qubit's bit position inside the tile, or -1 when the qubit is outside
+// the tile (then the gate is diagonal in that qubit and the tile's fixed bit
+// selects the sub-matrix).  diag != 0: the matrix is diagonal.
+struct KGate {
+    int32_t nq;
+    int32_t q[2];
+    int32_t tpos[2];
+    int32_t diag;
+    int32_t pad[2];
+    double m[32];
+};
+static_assert(sizeof(KGate) == 288, "KGate layout");
+
+struct CodecParams {
+    int32_t m;      // mantissa bits kept (relative step 2^-m)
+    int32_t L;      // absolute step 2^-L in the linear region
+};
+
+// One fused pass over the compressed store.
+struct PassArgs {
+    int32_t n, B, C, j;                 // qubits, block log2, chunk log2, tile qubits above C
+    int32_t tq[kMaxTileQubits];         // tile qubits minus C (chunk-index bit), ascending
+    uint64_t n_tiles;                   // 2^(n - C - j)
+    const KGate *gates;
+    int32_t ngates;
+    CodecParams codec;
+    const ChunkMeta *meta_in;
+    const uint32_t *arena_in;
+    ChunkMeta *meta_out;
+    uint32_t *arena_out;
+    unsigned long long *bump;           // bytes used in arena_out
+    uint64_t capacity;                  // bytes of arena_out
+    const uint32_t *block_to_group;     // stage's map
+    const uint8_t *group_active;
+    const uint8_t *mask;                // zero-block mask at stage start
+    int32_t first_pass, final_pass, exact_zero;
+    uint32_t *block_nz;                 // final pass: any non-zero in block
+    unsigned long long *block_bytes;    // final pass: stored bytes of block
+    int32_t *error;                     // 1 = arena overflow
+    unsigned long long *stats;          // [0] bytes read [1] bytes written [2] tiles
+};
+
+// One fused pass over a dense state vector (in place).
+struct DensePassArgs {
+    int32_t n, C, j;
+    int32_t tq[kMaxTileQubits];
+    uint64_t n_tiles;
+    const KGate *gates;
+    int32_t ngates;
+    void *state;
+};
+
+// ---- launchers (kernels.cu); all asynchronous on `stream` ----
+cudaError_t launch_pass(bool f64, const PassArgs &a, int tile_log2, cudaStream_t stream);
+cudaError_t launch_dense_pass(bool f64, const DensePassArgs &a, int tile_log2, cudaStream_t stream);
+cudaError_t launch_pergate(bool f64, void *state, int n, const KGate *gate_dev, cudaStream_t stream);
+
+cudaError_t launch_stage_begin(const uint32_t *block_to_group, const uint8_t *mask, uint32_t nb,
+                               uint8_t *group_active, uint32_t num_groups, uint32_t *block_nz,
+                               unsigned long long *block_bytes, unsigned long long *active_blocks,
+                               cudaStream_t stream);
+cudaError_t launch_stage_end(const uint32_t *block_to_group, const uint8_t *group_active, uint32_t nb,
+                             const uint32_t *block_nz, const unsigned long long *block_bytes_acc,
+                             uint8_t *mask, unsigned long long *block_bytes,
+                             unsigned long long *history_slot, cudaStream_t stream);
+
+// Decode chunks [chunk0, chunk0 + nchunks) into complex128 (interleaved).
+cudaError_t launch_readout(bool f64, const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask,
+                           int B, int C, CodecParams codec, uint64_t chunk0, uint64_t nchunks,
+                           double *out, double scale, cudaStream_t stream);
+// sum |a|^2 over the stored blocks (FP64 accumulation); *out must be zeroed.
+cudaError_t launch_norm(bool f64, const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask,
+                        int B, int C, CodecParams codec, uint64_t nchunks, double *out,
+                        cudaStream_t stream);
+// Encode complex128 chunks (host layout interleaved, on device) into the
+// store: chunks [chunk0, chunk0 + nchunks) read from `vals`.
+cudaError_t launch_encode(bool f64, const double *vals, int B, int C, CodecParams codec,
+                          uint64_t chunk0, uint64_t nchunks, ChunkMeta *meta, uint32_t *arena,
+                          unsigned long long *bump, uint64_t capacity, uint32_t *block_nz,
+                          unsigned long long *block_bytes, int32_t *error, cudaStream_t stream);
+cudaError_t launch_dense_norm(bool f64, const void *state, uint64_t dim, double *out, cudaStream_t stream);
+cudaError_t launch_dense_to_c128(bool f64, const void *state, uint64_t dim, double *out, cudaStream_t stream);
+cudaError_t launch_c128_to_dense(bool f64, const double *in, uint64_t dim, void *state, cudaStream_t stream);
+cudaError_t launch_sum_mask_bytes(const uint8_t *mask, const unsigned long long *block_bytes, uint32_t nb,
+                                  unsigned long long *out, cudaStream_t stream);
+
+// Device codec round trip of whole chunks (tests of CPU/GPU bit identity).
+cudaError_t launch_codec_test(bool f64, const void *vals, int C, CodecParams codec, uint64_t nchunks,
+                              uint32_t *words, int32_t *bases, uint32_t *widths, void *decoded,
+                              cudaStream_t stream);
+
+int sm_count();
+
+}  // namespace qs

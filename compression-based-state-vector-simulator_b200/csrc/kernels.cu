@@ -1,0 +1,854 @@
+// Device code of the compressed state-vector engine (sm_100a).
+//
+// The hot path is pass_kernel: one fused pass of a circuit stage over the
+// HBM-resident compressed store.  It replaces, for every active group of the
+// stage, the reference's chain H2D -> Bitcomp decode + inverse compander ->
+// one kernel per gate per block pair -> zero check -> compander + Bitcomp
+// encode -> D2H (src/cppsim/compressed_state_cuda.cu:143-381, kernels
+// :392-811, compand_kernel.cuh:5-30, cuda_complex_helper.cuh:96-106).
+//
+// Work unit: a tile = 2^j chunks (2^C amplitudes each) whose chunk indices
+// differ exactly in the pass's tile qubits, so every gate of the pass that
+// mixes amplitudes acts inside one tile.  A CTA decodes the tile's chunks
+// into shared memory (one warp per chunk, coalesced 128-byte payload rows),
+// applies the pass's gates in shared memory, re-quantises, reserves output
+// space for the whole tile with one atomicAdd on the arena's bump counter
+// and writes the packed chunks back with coalesced stores.
+#include <cstdio>
+#include <climits>
+
+#include "codec.cuh"
+#include "internal.h"
+
+namespace qs {
+
+namespace {
+
+template <typename R> struct Cplx;
+template <> struct Cplx<float> { using T = float2; };
+template <> struct Cplx<double> { using T = double2; };
+
+template <typename T>
+__device__ __forceinline__ T cmul(T a, T b) {
+    T r;
+    r.x = a.x * b.x - a.y * b.y;
+    r.y = a.x * b.y + a.y * b.x;
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T cfma(T a, T b, T c) {  // a*b + c
+    T r;
+    r.x = fma(a.x, b.x, fma(-a.y, b.y, c.x));
+    r.y = fma(a.x, b.y, fma(a.y, b.x, c.y));
+    return r;
+}
+
+template <typename T, typename R>
+__device__ __forceinline__ T make_c(double re, double im) {
+    T r;
+    r.x = (R)re;
+    r.y = (R)im;
+    return r;
+}
+
+__device__ __forceinline__ uint64_t insert_zero_bits(uint64_t x, const int32_t *pos, int cnt) {
+    for (int s = 0; s < cnt; ++s) {
+        const int t = pos[s];
+        const uint64_t lo = x & ((uint64_t(1) << t) - 1);
+        x = ((x >> t) << (t + 1)) | lo;
+    }
+    return x;
+}
+
+__device__ __forceinline__ uint64_t deposit_bits(uint32_t c, const int32_t *pos, int cnt) {
+    uint64_t r = 0;
+    for (int s = 0; s < cnt; ++s) r |= uint64_t((c >> s) & 1u) << pos[s];
+    return r;
+}
+
+// ------------------------------------------------------------ tile gates
+// All routines run on every thread of the CTA over a tile of 2^nb elements.
+
+template <typename T>
+__device__ void tile_2x2(T *t, int nb, int p, T e0, T e1, T e2, T e3) {
+    const int half = 1 << (nb - 1);
+    const int lowmask = (1 << p) - 1;
+    for (int i = threadIdx.x; i < half; i += blockDim.x) {
+        const int i0 = ((i & ~lowmask) << 1) | (i & lowmask);
+        const int i1 = i0 | (1 << p);
+        const T a = t[i0], b = t[i1];
+        t[i0] = cfma(e0, a, cmul(e1, b));
+        t[i1] = cfma(e2, a, cmul(e3, b));
+    }
+}
+
+template <typename T>
+__device__ void tile_diag2(T *t, int nb, int p, T d0, T d1) {
+    const int size = 1 << nb;
+    for (int i = threadIdx.x; i < size; i += blockDim.x) {
+        t[i] = cmul(((i >> p) & 1) ? d1 : d0, t[i]);
+    }
+}
+
+template <typename T>
+__device__ void tile_4x4(T *t, int nb, int pa, int pb, const T *m) {
+    const int quarter = 1 << (nb - 2);
+    const int lo = pa < pb ? pa : pb, hi = pa < pb ? pb : pa;
+    const int mlo = (1 << lo) - 1, mhi = (1 << hi) - 1;
+    for (int i = threadIdx.x; i < quarter; i += blockDim.x) {
+        // insert zeros at lo, then at hi
+        int b = ((i & ~mlo) << 1) | (i & mlo);
+        b = ((b & ~mhi) << 1) | (b & mhi);
+        const int ia = 1 << pa, ib = 1 << pb;
+        const T v0 = t[b], v1 = t[b | ia], v2 = t[b | ib], v3 = t[b | ia | ib];
+        T o[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            T acc = cmul(m[4 * r + 0], v0);
+            acc = cfma(m[4 * r + 1], v1, acc);
+            acc = cfma(m[4 * r + 2], v2, acc);
+            acc = cfma(m[4 * r + 3], v3, acc);
+            o[r] = acc;
+        }
+        t[b] = o[0];
+        t[b | ia] = o[1];
+        t[b | ib] = o[2];
+        t[b | ia | ib] = o[3];
+    }
+}
+
+template <typename T>
+__device__ void tile_diag4(T *t, int nb, int pa, int pb, T d0, T d1, T d2, T d3) {
+    const int size = 1 << nb;
+    for (int i = threadIdx.x; i < size; i += blockDim.x) {
+        const int k = ((i >> pa) & 1) | (((i >> pb) & 1) << 1);
+        const T d = k == 0 ? d0 : (k == 1 ? d1 : (k == 2 ? d2 : d3));
+        t[i] = cmul(d, t[i]);
+    }
+}
+
+template <typename T>
+__device__ void tile_scale(T *t, int nb, T s) {
+    if (s.x == 1 && s.y == 0) return;
+    const int size = 1 << nb;
+    for (int i = threadIdx.x; i < size; i += blockDim.x) t[i] = cmul(s, t[i]);
+}
+
+// Apply one gate to the tile whose element 0 is global amplitude base_amp
+// (all tile bits zero there, so qubits outside the tile read their fixed
+// value from base_amp).
+template <typename R>
+__device__ void tile_apply_gate(typename Cplx<R>::T *t, int nb, const KGate &g, uint64_t base_amp) {
+    using T = typename Cplx<R>::T;
+    const double *m = g.m;
+    auto M = [&](int r, int c) -> T {
+        const int k = 2 * (r * (g.nq == 1 ? 2 : 4) + c);
+        return make_c<T, R>(m[k], m[k + 1]);
+    };
+    if (g.nq == 1) {
+        const int p = g.tpos[0];
+        if (p >= 0) {
+            if (g.diag) tile_diag2(t, nb, p, M(0, 0), M(1, 1));
+            else tile_2x2(t, nb, p, M(0, 0), M(0, 1), M(1, 0), M(1, 1));
+        } else {
+            const int v = (int)((base_amp >> g.q[0]) & 1);
+            tile_scale(t, nb, M(v, v));
+        }
+        return;
+    }
+    const bool in0 = g.tpos[0] >= 0, in1 = g.tpos[1] >= 0;
+    if (in0 && in1) {
+        if (g.diag) {
+            tile_diag4(t, nb, g.tpos[0], g.tpos[1], M(0, 0), M(1, 1), M(2, 2), M(3, 3));
+        } else {
+            T mm[16];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) mm[4 * r + c] = M(r, c);
+            tile_4x4(t, nb, g.tpos[0], g.tpos[1], mm);
+        }
+    } else if (in0 || in1) {
+        const int b = in0 ? 0 : 1;             // matrix bit that varies in the tile
+        const int p = in0 ? g.tpos[0] : g.tpos[1];
+        const int v = (int)((base_amp >> g.q[1 - b]) & 1);
+        auto idx = [&](int x) { return b == 0 ? (x | (v << 1)) : (v | (x << 1)); };
+        if (g.diag) tile_diag2(t, nb, p, M(idx(0), idx(0)), M(idx(1), idx(1)));
+        else tile_2x2(t, nb, p, M(idx(0), idx(0)), M(idx(0), idx(1)), M(idx(1), idx(0)), M(idx(1), idx(1)));
+    } else {
+        const int v0 = (int)((base_amp >> g.q[0]) & 1), v1 = (int)((base_amp >> g.q[1]) & 1);
+        const int k = v0 | (v1 << 1);
+        tile_scale(t, nb, M(k, k));
+    }
+}
+
+// ------------------------------------------------------------ chunk codec
+// Per-warp decode of one chunk into comp[lane + 32 i] (i < per_lane).
+template <typename R>
+__device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena, const ChunkMeta md,
+                                             int per_lane, CodecParams p, R *comp, uint32_t *wstage,
+                                             int lane) {
+    const uint32_t w = md.width;
+    if (w == 0) {
+        const R v = dequantize(md.base, p, R());
+        for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = v;
+        return;
+    }
+    const uint32_t rows = (uint32_t)(((uint32_t)per_lane * w + 31) >> 5);
+    const uint32_t *src = arena + (md.offset >> 2);
+    uint32_t tmp[kMaxPerLane];
+#pragma unroll
+    for (int r = 0; r < kMaxPerLane; ++r)
+        if (r < (int)rows) tmp[r] = __ldcs(src + r * 32 + lane);
+#pragma unroll
+    for (int r = 0; r < kMaxPerLane; ++r)
+        if (r < (int)rows) wstage[r * 32 + lane] = tmp[r];
+    uint64_t buf = 0;
+    uint32_t nbits = 0, r = 0;
+    const uint64_t mask = (w == 32) ? 0xffffffffull : ((1ull << w) - 1);
+    for (int i = 0; i < per_lane; ++i) {
+        if (nbits < w) {
+            buf |= (uint64_t)wstage[r * 32 + lane] << nbits;
+            ++r;
+            nbits += 32;
+        }
+        const uint32_t u = (uint32_t)(buf & mask);
+        buf >>= w;
+        nbits -= w;
+        comp[lane + 32 * i] = dequantize((int32_t)((uint32_t)md.base + u), p, R());
+    }
+}
+
+// Per-warp quantisation of one chunk held in comp[]: codes overwrite the
+// chunk's own shared memory as int32 (all values are read first).  Returns
+// base/width/non-zero flag (valid in every lane).
+template <typename R>
+__device__ __forceinline__ void quantize_chunk(R *comp, int per_lane, CodecParams p, bool exact_zero,
+                                               int lane, int32_t *base_out, uint32_t *width_out,
+                                               bool *nz_out) {
+    R v[kMaxPerLane];
+#pragma unroll
+    for (int i = 0; i < kMaxPerLane; ++i)
+        if (i < per_lane) v[i] = comp[lane + 32 * i];
+    __syncwarp();
+    int32_t *codes = reinterpret_cast<int32_t *>(comp);
+    int32_t lo = INT_MAX, hi = INT_MIN;
+    bool nz = false;
+#pragma unroll
+    for (int i = 0; i < kMaxPerLane; ++i) {
+        if (i < per_lane) {
+            const int32_t q = quantize(v[i], p);
+            codes[lane + 32 * i] = q;
+            lo = min(lo, q);
+            hi = max(hi, q);
+            nz |= exact_zero ? (v[i] != R(0)) : (q != 0);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    nz = __any_sync(0xffffffffu, nz);
+    __syncwarp();
+    *base_out = lo;
+    *width_out = bit_length((uint32_t)((int64_t)hi - (int64_t)lo));
+    *nz_out = nz;
+}
+
+// Per-warp packing of int32 codes[lane + 32 i] to dst (layout in codec.cuh).
+__device__ __forceinline__ void pack_chunk(const int32_t *codes, int per_lane, int32_t base, uint32_t w,
+                                           uint32_t *__restrict__ dst, int lane) {
+    if (w == 0) return;
+    uint64_t buf = 0;
+    uint32_t nbits = 0, r = 0;
+    for (int i = 0; i < per_lane; ++i) {
+        const uint32_t u = (uint32_t)(codes[lane + 32 * i] - base);
+        buf |= (uint64_t)u << nbits;
+        nbits += w;
+        if (nbits >= 32) {
+            __stcs(dst + r * 32 + lane, (uint32_t)buf);
+            ++r;
+            buf >>= 32;
+            nbits -= 32;
+        }
+    }
+    if (nbits > 0) __stcs(dst + r * 32 + lane, (uint32_t)buf);
+}
+
+__device__ __forceinline__ size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+size_t pass_smem_bytes(bool f64, int nb, int j) {
+    const size_t tile = (f64 ? 16 : 8) << nb;
+    const size_t stage = (size_t)(kPassThreads / 32) * kMaxPerLane * 32 * 4;
+    const size_t tables = ((size_t)3 * 4 << j) + 8;
+    const size_t offs = (size_t)8 << j;
+    return tile + stage + ((tables + 7) / 8) * 8 + offs;
+}
+
+// ------------------------------------------------------------ pass kernel
+template <typename R>
+__global__ void __launch_bounds__(kPassThreads) pass_kernel(const PassArgs a) {
+    using T = typename Cplx<R>::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ unsigned long long s_tile_off;
+    __shared__ int s_flag;
+
+    const int C = a.C, j = a.j, nb = C + j;
+    const int nchunks = 1 << j;
+    const int ncomp = 2 << C;
+    const int per_lane = ncomp >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int blk_shift = a.B - C;
+
+    T *tile = reinterpret_cast<T *>(smem);
+    uint32_t *stage_all = reinterpret_cast<uint32_t *>(smem + (sizeof(T) << nb));
+    uint32_t *wstage = stage_all + warp * (kMaxPerLane * 32);
+    int32_t *s_base = reinterpret_cast<int32_t *>(stage_all + nwarps * (kMaxPerLane * 32));
+    uint32_t *s_width = reinterpret_cast<uint32_t *>(s_base + nchunks);
+    uint32_t *s_nz = s_width + nchunks;
+    unsigned long long *s_off = reinterpret_cast<unsigned long long *>(
+        reinterpret_cast<unsigned char *>(s_base) + ((((size_t)3 * 4 << j) + 8 + 7) / 8) * 8);
+
+    unsigned long long rd = 0, wr = 0, ntiles = 0;
+
+    for (uint64_t tile_id = blockIdx.x; tile_id < a.n_tiles; tile_id += gridDim.x) {
+        const uint64_t chunk_base = insert_zero_bits(tile_id, a.tq, j);
+        const uint64_t block0 = chunk_base >> blk_shift;
+        if (!a.group_active[a.block_to_group[block0]]) continue;  // uniform in the CTA
+        if (threadIdx.x == 0) s_flag = *reinterpret_cast<volatile int32_t *>(a.error);
+        __syncthreads();
+        if (s_flag) break;
+        ++ntiles;
+
+        // ---- decode
+        for (int c = warp; c < nchunks; c += nwarps) {
+            const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, a.tq, j);
+            const uint64_t blk = chunk >> blk_shift;
+            R *comp = reinterpret_cast<R *>(tile) + (size_t)c * ncomp;
+            if (a.first_pass && !a.mask[blk]) {
+                for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = R(0);
+                continue;
+            }
+            const ChunkMeta md = a.meta_in[chunk];
+            decode_chunk<R>(a.arena_in, md, per_lane, a.codec, comp, wstage, lane);
+            if (lane == 0) rd += payload_bytes(C, md.width) + sizeof(ChunkMeta);
+        }
+        __syncthreads();
+
+        // ---- gates
+        const uint64_t base_amp = chunk_base << C;
+        for (int k = 0; k < a.ngates; ++k) {
+            tile_apply_gate<R>(tile, nb, a.gates[k], base_amp);
+            __syncthreads();
+        }
+
+        // ---- quantise (codes replace values in shared memory)
+        for (int c = warp; c < nchunks; c += nwarps) {
+            R *comp = reinterpret_cast<R *>(tile) + (size_t)c * ncomp;
+            int32_t base;
+            uint32_t width;
+            bool nz;
+            quantize_chunk<R>(comp, per_lane, a.codec, a.exact_zero != 0, lane, &base, &width, &nz);
+            if (lane == 0) {
+                s_base[c] = base;
+                s_width[c] = width;
+                s_nz[c] = nz ? 1u : 0u;
+            }
+        }
+        __syncthreads();
+
+        // ---- reserve the tile's output bytes with one atomic
+        if (threadIdx.x == 0) {
+            unsigned long long total = 0;
+            for (int c = 0; c < nchunks; ++c) {
+                s_off[c] = total;
+                total += payload_bytes(C, s_width[c]);
+            }
+            const unsigned long long off = atomicAdd(a.bump, total);
+            if (off + total > a.capacity) {
+                atomicExch(a.error, 1);
+                s_flag = 1;
+            } else {
+                s_flag = 0;
+            }
+            s_tile_off = off;
+            wr += total + (unsigned long long)nchunks * sizeof(ChunkMeta);
+        }
+        __syncthreads();
+        if (s_flag) break;
+
+        // ---- pack and store
+        for (int c = warp; c < nchunks; c += nwarps) {
+            const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, a.tq, j);
+            const int32_t *codes = reinterpret_cast<const int32_t *>(reinterpret_cast<R *>(tile) + (size_t)c * ncomp);
+            const unsigned long long off = s_tile_off + s_off[c];
+            const uint32_t w = s_width[c];
+            pack_chunk(codes, per_lane, s_base[c], w, a.arena_out + (off >> 2), lane);
+            if (lane == 0) {
+                ChunkMeta md;
+                md.offset = off;
+                md.base = s_base[c];
+                md.width = w;
+                a.meta_out[chunk] = md;
+                if (a.final_pass) {
+                    const uint64_t blk = chunk >> blk_shift;
+                    if (s_nz[c]) atomicOr(&a.block_nz[blk], 1u);
+                    atomicAdd(&a.block_bytes[blk], (unsigned long long)(payload_bytes(C, w) + sizeof(ChunkMeta)));
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (lane == 0 && rd) atomicAdd(&a.stats[0], rd);
+    if (threadIdx.x == 0) {
+        if (wr) atomicAdd(&a.stats[1], wr);
+        if (ntiles) atomicAdd(&a.stats[2], ntiles);
+    }
+}
+
+// ------------------------------------------------------------ dense pass
+template <typename R>
+__global__ void __launch_bounds__(kPassThreads) dense_pass_kernel(const DensePassArgs a) {
+    using T = typename Cplx<R>::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T *tile = reinterpret_cast<T *>(smem);
+    T *st = reinterpret_cast<T *>(a.state);
+    const int C = a.C, j = a.j, nb = C + j;
+    const int size = 1 << nb;
+    const int cmask = (1 << C) - 1;
+    for (uint64_t tile_id = blockIdx.x; tile_id < a.n_tiles; tile_id += gridDim.x) {
+        const uint64_t chunk_base = insert_zero_bits(tile_id, a.tq, j);
+        for (int e = threadIdx.x; e < size; e += blockDim.x) {
+            const uint64_t amp = ((chunk_base | deposit_bits((uint32_t)(e >> C), a.tq, j)) << C) | (uint64_t)(e & cmask);
+            tile[e] = st[amp];
+        }
+        __syncthreads();
+        const uint64_t base_amp = chunk_base << C;
+        for (int k = 0; k < a.ngates; ++k) {
+            tile_apply_gate<R>(tile, nb, a.gates[k], base_amp);
+            __syncthreads();
+        }
+        for (int e = threadIdx.x; e < size; e += blockDim.x) {
+            const uint64_t amp = ((chunk_base | deposit_bits((uint32_t)(e >> C), a.tq, j)) << C) | (uint64_t)(e & cmask);
+            st[amp] = tile[e];
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------ plain per-gate
+template <typename R>
+__global__ void pergate_kernel(typename Cplx<R>::T *st, int n, const KGate *__restrict__ gp) {
+    using T = typename Cplx<R>::T;
+    const KGate &g = *gp;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    if (g.nq == 1) {
+        const int p = g.q[0];
+        const T e0 = make_c<T, R>(g.m[0], g.m[1]), e1 = make_c<T, R>(g.m[2], g.m[3]);
+        const T e2 = make_c<T, R>(g.m[4], g.m[5]), e3 = make_c<T, R>(g.m[6], g.m[7]);
+        const uint64_t half = uint64_t(1) << (n - 1), low = (uint64_t(1) << p) - 1;
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half; i += stride) {
+            const uint64_t i0 = ((i & ~low) << 1) | (i & low), i1 = i0 | (uint64_t(1) << p);
+            const T a = st[i0], b = st[i1];
+            st[i0] = cfma(e0, a, cmul(e1, b));
+            st[i1] = cfma(e2, a, cmul(e3, b));
+        }
+    } else {
+        const int pa = g.q[0], pb = g.q[1];
+        T m[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) m[k] = make_c<T, R>(g.m[2 * k], g.m[2 * k + 1]);
+        const uint64_t quarter = uint64_t(1) << (n - 2);
+        const uint64_t mlo = (uint64_t(1) << pa) - 1, mhi = (uint64_t(1) << pb) - 1;
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < quarter; i += stride) {
+            uint64_t b = ((i & ~mlo) << 1) | (i & mlo);
+            b = ((b & ~mhi) << 1) | (b & mhi);
+            const uint64_t ia = uint64_t(1) << pa, ib = uint64_t(1) << pb;
+            const T v0 = st[b], v1 = st[b | ia], v2 = st[b | ib], v3 = st[b | ia | ib];
+            T o[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                T acc = cmul(m[4 * r], v0);
+                acc = cfma(m[4 * r + 1], v1, acc);
+                acc = cfma(m[4 * r + 2], v2, acc);
+                acc = cfma(m[4 * r + 3], v3, acc);
+                o[r] = acc;
+            }
+            st[b] = o[0];
+            st[b | ia] = o[1];
+            st[b | ib] = o[2];
+            st[b | ia | ib] = o[3];
+        }
+    }
+}
+
+// ------------------------------------------------------------ stage bookkeeping
+__global__ void stage_clear_kernel(uint8_t *group_active, uint32_t num_groups, uint32_t *block_nz,
+                                   unsigned long long *block_bytes, uint32_t nb) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < num_groups) group_active[i] = 0;
+    if (i < nb) {
+        block_nz[i] = 0;
+        block_bytes[i] = 0;
+    }
+}
+
+__global__ void stage_mark_kernel(const uint32_t *block_to_group, const uint8_t *mask, uint32_t nb,
+                                  uint8_t *group_active) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nb && mask[b]) group_active[block_to_group[b]] = 1;
+}
+
+// Blocks of active groups (all of them are processed, Q8): the stage's
+// amplitude count is this times 2^B.
+__global__ void stage_count_kernel(const uint32_t *block_to_group, const uint8_t *group_active, uint32_t nb,
+                                   unsigned long long *count) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long v = (b < nb && group_active[block_to_group[b]]) ? 1ull : 0ull;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(count, v);
+}
+
+// Zero-mask rule of the reference (compressed_state.hpp:1015-1026,
+// compressed_state_cuda.cu:282-305): only blocks that were zero before the
+// stage and belong to an active group are tested; a stored block stays
+// stored.
+__global__ void stage_end_kernel(const uint32_t *block_to_group, const uint8_t *group_active, uint32_t nb,
+                                 const uint32_t *block_nz, const unsigned long long *acc, uint8_t *mask,
+                                 unsigned long long *block_bytes, unsigned long long *history_slot) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long bytes = 0;
+    if (b < nb) {
+        uint8_t mk = mask[b];
+        if (group_active[block_to_group[b]]) {
+            if (!mk && block_nz[b]) mk = 1;
+            mask[b] = mk;
+            bytes = mk ? acc[b] : 0ull;
+        } else {
+            bytes = mk ? block_bytes[b] : 0ull;
+        }
+        block_bytes[b] = bytes;
+    }
+    for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+    if ((threadIdx.x & 31) == 0 && bytes) atomicAdd(history_slot, bytes);
+}
+
+__global__ void sum_mask_bytes_kernel(const uint8_t *mask, const unsigned long long *bb, uint32_t nb,
+                                      unsigned long long *out) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long v = (b < nb && mask[b]) ? bb[b] : 0ull;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(out, v);
+}
+
+// ------------------------------------------------------------ readout / norm
+template <typename R>
+__global__ void readout_kernel(const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B, int C,
+                               CodecParams p, uint64_t chunk0, uint64_t nchunks, double *out, double scale) {
+    __shared__ uint32_t stage[kPassThreads / 32][kMaxPerLane * 32];
+    __shared__ R vals[kPassThreads / 32][2 << kMaxChunkLog2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ncomp = 2 << C, per_lane = ncomp >> 5;
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t k = gw; k < nchunks; k += nw) {
+        const uint64_t chunk = chunk0 + k;
+        double *o = out + k * (uint64_t)ncomp;
+        if (!mask[chunk >> (B - C)]) {
+            for (int i = 0; i < per_lane; ++i) o[lane + 32 * i] = 0.0;
+            continue;
+        }
+        decode_chunk<R>(arena, meta[chunk], per_lane, p, vals[warp], stage[warp], lane);
+        for (int i = 0; i < per_lane; ++i) o[lane + 32 * i] = (double)vals[warp][lane + 32 * i] * scale;
+        __syncwarp();
+    }
+}
+
+template <typename R>
+__global__ void norm_kernel(const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B, int C,
+                            CodecParams p, uint64_t nchunks, double *out) {
+    __shared__ uint32_t stage[kPassThreads / 32][kMaxPerLane * 32];
+    __shared__ R vals[kPassThreads / 32][2 << kMaxChunkLog2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ncomp = 2 << C, per_lane = ncomp >> 5;
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    double acc = 0.0;
+    for (uint64_t chunk = gw; chunk < nchunks; chunk += nw) {
+        if (!mask[chunk >> (B - C)]) continue;
+        decode_chunk<R>(arena, meta[chunk], per_lane, p, vals[warp], stage[warp], lane);
+        for (int i = 0; i < per_lane; ++i) {
+            const double v = (double)vals[warp][lane + 32 * i];
+            acc = fma(v, v, acc);
+        }
+        __syncwarp();
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0 && acc != 0.0) atomicAdd(out, acc);
+}
+
+// Encode chunks from a device complex128 buffer into the store (load path).
+template <typename R>
+__global__ void encode_kernel(const double *vals, int B, int C, CodecParams p, uint64_t chunk0, uint64_t nchunks,
+                              ChunkMeta *meta, uint32_t *arena, unsigned long long *bump, uint64_t capacity,
+                              uint32_t *block_nz, unsigned long long *block_bytes, int32_t *error) {
+    __shared__ R buf[kPassThreads / 32][2 << kMaxChunkLog2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ncomp = 2 << C, per_lane = ncomp >> 5;
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t k = gw; k < nchunks; k += nw) {
+        const uint64_t chunk = chunk0 + k;
+        R *comp = buf[warp];
+        for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = (R)vals[k * (uint64_t)ncomp + lane + 32 * i];
+        __syncwarp();
+        int32_t base;
+        uint32_t width;
+        bool nz;
+        quantize_chunk<R>(comp, per_lane, p, true, lane, &base, &width, &nz);
+        const uint64_t bytes = payload_bytes(C, width);
+        unsigned long long off = 0;
+        if (lane == 0) off = atomicAdd(bump, (unsigned long long)bytes);
+        off = __shfl_sync(0xffffffffu, off, 0);
+        if (off + bytes > capacity) {
+            if (lane == 0) atomicExch(error, 1);
+            __syncwarp();
+            continue;
+        }
+        pack_chunk(reinterpret_cast<const int32_t *>(comp), per_lane, base, width, arena + (off >> 2), lane);
+        if (lane == 0) {
+            ChunkMeta md;
+            md.offset = off;
+            md.base = base;
+            md.width = width;
+            meta[chunk] = md;
+            const uint64_t blk = chunk >> (B - C);
+            if (nz) atomicOr(&block_nz[blk], 1u);
+            atomicAdd(&block_bytes[blk], (unsigned long long)(bytes + sizeof(ChunkMeta)));
+        }
+        __syncwarp();
+    }
+}
+
+template <typename R>
+__global__ void codec_test_kernel(const R *vals, int C, CodecParams p, uint64_t nchunks, uint32_t *words,
+                                  int32_t *bases, uint32_t *widths, R *decoded) {
+    __shared__ uint32_t stage[kPassThreads / 32][kMaxPerLane * 32];
+    __shared__ R buf[kPassThreads / 32][2 << kMaxChunkLog2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ncomp = 2 << C, per_lane = ncomp >> 5;
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint64_t max_words = (uint64_t)per_lane * 32;  // width 32
+    for (uint64_t k = gw; k < nchunks; k += nw) {
+        R *comp = buf[warp];
+        for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = vals[k * ncomp + lane + 32 * i];
+        __syncwarp();
+        int32_t base;
+        uint32_t width;
+        bool nz;
+        quantize_chunk<R>(comp, per_lane, p, true, lane, &base, &width, &nz);
+        uint32_t *dst = words + k * max_words;
+        pack_chunk(reinterpret_cast<const int32_t *>(comp), per_lane, base, width, dst, lane);
+        if (lane == 0) {
+            bases[k] = base;
+            widths[k] = width;
+        }
+        __syncwarp();
+        __threadfence_block();
+        ChunkMeta md;
+        md.offset = 0;
+        md.base = base;
+        md.width = width;
+        decode_chunk<R>(dst, md, per_lane, p, comp, stage[warp], lane);
+        __syncwarp();
+        for (int i = 0; i < per_lane; ++i) decoded[k * ncomp + lane + 32 * i] = comp[lane + 32 * i];
+        __syncwarp();
+    }
+}
+
+template <typename R>
+__global__ void dense_norm_kernel(const R *s, uint64_t ncomp, double *out) {
+    double acc = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < ncomp; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double v = (double)s[i];
+        acc = fma(v, v, acc);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0 && acc != 0.0) atomicAdd(out, acc);
+}
+
+template <typename R>
+__global__ void to_c128_kernel(const R *s, uint64_t ncomp, double *out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < ncomp; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = (double)s[i];
+}
+
+template <typename R>
+__global__ void from_c128_kernel(const double *in, uint64_t ncomp, R *s) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < ncomp; i += (uint64_t)gridDim.x * blockDim.x)
+        s[i] = (R)in[i];
+}
+
+int g_sm_count = 0;
+
+unsigned grid_for(uint64_t work, unsigned per_block, unsigned cap_per_sm = 8) {
+    const uint64_t need = (work + per_block - 1) / per_block;
+    const uint64_t cap = (uint64_t)sm_count() * cap_per_sm;
+    uint64_t g = need < cap ? need : cap;
+    return (unsigned)(g ? g : 1);
+}
+
+}  // namespace
+
+int sm_count() {
+    if (g_sm_count == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        g_sm_count = v;
+    }
+    return g_sm_count;
+}
+
+template <typename R>
+static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
+    const int nb = a.C + a.j;
+    const size_t smem = pass_smem_bytes(sizeof(R) == 8, nb, a.j);
+    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<R>, kPassThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    uint64_t grid = (uint64_t)per_sm * sm_count();
+    if (grid > a.n_tiles) grid = a.n_tiles;
+    if (grid == 0) grid = 1;
+    pass_kernel<R><<<(unsigned)grid, kPassThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pass(bool f64, const PassArgs &a, int, cudaStream_t s) {
+    return f64 ? launch_pass_t<double>(a, s) : launch_pass_t<float>(a, s);
+}
+
+template <typename R>
+static cudaError_t launch_dense_pass_t(const DensePassArgs &a, cudaStream_t s) {
+    const int nb = a.C + a.j;
+    const size_t smem = (size_t)(2 * sizeof(R)) << nb;
+    cudaError_t e = cudaFuncSetAttribute(dense_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense_pass_kernel<R>, kPassThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    uint64_t grid = (uint64_t)per_sm * sm_count();
+    if (grid > a.n_tiles) grid = a.n_tiles;
+    if (grid == 0) grid = 1;
+    dense_pass_kernel<R><<<(unsigned)grid, kPassThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dense_pass(bool f64, const DensePassArgs &a, int, cudaStream_t s) {
+    return f64 ? launch_dense_pass_t<double>(a, s) : launch_dense_pass_t<float>(a, s);
+}
+
+cudaError_t launch_pergate(bool f64, void *state, int n, const KGate *g, cudaStream_t s) {
+    const uint64_t work = uint64_t(1) << (n - 1);
+    const unsigned grid = grid_for(work, 256, 16);
+    if (f64) pergate_kernel<double><<<grid, 256, 0, s>>>((double2 *)state, n, g);
+    else pergate_kernel<float><<<grid, 256, 0, s>>>((float2 *)state, n, g);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stage_begin(const uint32_t *b2g, const uint8_t *mask, uint32_t nb, uint8_t *group_active,
+                               uint32_t num_groups, uint32_t *block_nz, unsigned long long *block_bytes,
+                               unsigned long long *active_blocks, cudaStream_t s) {
+    const uint32_t m = nb > num_groups ? nb : num_groups;
+    stage_clear_kernel<<<(m + 255) / 256, 256, 0, s>>>(group_active, num_groups, block_nz, block_bytes, nb);
+    stage_mark_kernel<<<(nb + 255) / 256, 256, 0, s>>>(b2g, mask, nb, group_active);
+    stage_count_kernel<<<(nb + 255) / 256, 256, 0, s>>>(b2g, group_active, nb, active_blocks);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stage_end(const uint32_t *b2g, const uint8_t *group_active, uint32_t nb, const uint32_t *block_nz,
+                             const unsigned long long *acc, uint8_t *mask, unsigned long long *block_bytes,
+                             unsigned long long *history_slot, cudaStream_t s) {
+    stage_end_kernel<<<(nb + 255) / 256, 256, 0, s>>>(b2g, group_active, nb, block_nz, acc, mask, block_bytes,
+                                                      history_slot);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sum_mask_bytes(const uint8_t *mask, const unsigned long long *bb, uint32_t nb,
+                                  unsigned long long *out, cudaStream_t s) {
+    sum_mask_bytes_kernel<<<(nb + 255) / 256, 256, 0, s>>>(mask, bb, nb, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_readout(bool f64, const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B, int C,
+                           CodecParams p, uint64_t chunk0, uint64_t nchunks, double *out, double scale,
+                           cudaStream_t s) {
+    const unsigned grid = grid_for(nchunks, kPassThreads / 32, 8);
+    if (f64) readout_kernel<double><<<grid, kPassThreads, 0, s>>>(meta, arena, mask, B, C, p, chunk0, nchunks, out, scale);
+    else readout_kernel<float><<<grid, kPassThreads, 0, s>>>(meta, arena, mask, B, C, p, chunk0, nchunks, out, scale);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_norm(bool f64, const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B, int C,
+                        CodecParams p, uint64_t nchunks, double *out, cudaStream_t s) {
+    const unsigned grid = grid_for(nchunks, kPassThreads / 32, 8);
+    if (f64) norm_kernel<double><<<grid, kPassThreads, 0, s>>>(meta, arena, mask, B, C, p, nchunks, out);
+    else norm_kernel<float><<<grid, kPassThreads, 0, s>>>(meta, arena, mask, B, C, p, nchunks, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_encode(bool f64, const double *vals, int B, int C, CodecParams p, uint64_t chunk0, uint64_t nchunks,
+                          ChunkMeta *meta, uint32_t *arena, unsigned long long *bump, uint64_t capacity,
+                          uint32_t *block_nz, unsigned long long *block_bytes, int32_t *error, cudaStream_t s) {
+    const unsigned grid = grid_for(nchunks, kPassThreads / 32, 8);
+    if (f64)
+        encode_kernel<double><<<grid, kPassThreads, 0, s>>>(vals, B, C, p, chunk0, nchunks, meta, arena, bump,
+                                                           capacity, block_nz, block_bytes, error);
+    else
+        encode_kernel<float><<<grid, kPassThreads, 0, s>>>(vals, B, C, p, chunk0, nchunks, meta, arena, bump, capacity,
+                                                          block_nz, block_bytes, error);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_codec_test(bool f64, const void *vals, int C, CodecParams p, uint64_t nchunks, uint32_t *words,
+                              int32_t *bases, uint32_t *widths, void *decoded, cudaStream_t s) {
+    const unsigned grid = grid_for(nchunks, kPassThreads / 32, 8);
+    if (f64)
+        codec_test_kernel<double><<<grid, kPassThreads, 0, s>>>((const double *)vals, C, p, nchunks, words, bases,
+                                                               widths, (double *)decoded);
+    else
+        codec_test_kernel<float><<<grid, kPassThreads, 0, s>>>((const float *)vals, C, p, nchunks, words, bases, widths,
+                                                              (float *)decoded);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dense_norm(bool f64, const void *state, uint64_t dim, double *out, cudaStream_t s) {
+    const unsigned grid = grid_for(2 * dim, 256, 8);
+    if (f64) dense_norm_kernel<double><<<grid, 256, 0, s>>>((const double *)state, 2 * dim, out);
+    else dense_norm_kernel<float><<<grid, 256, 0, s>>>((const float *)state, 2 * dim, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dense_to_c128(bool f64, const void *state, uint64_t dim, double *out, cudaStream_t s) {
+    const unsigned grid = grid_for(2 * dim, 256, 8);
+    if (f64) to_c128_kernel<double><<<grid, 256, 0, s>>>((const double *)state, 2 * dim, out);
+    else to_c128_kernel<float><<<grid, 256, 0, s>>>((const float *)state, 2 * dim, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_c128_to_dense(bool f64, const double *in, uint64_t dim, void *state, cudaStream_t s) {
+    const unsigned grid = grid_for(2 * dim, 256, 8);
+    if (f64) from_c128_kernel<double><<<grid, 256, 0, s>>>(in, 2 * dim, (double *)state);
+    else from_c128_kernel<float><<<grid, 256, 0, s>>>(in, 2 * dim, (float *)state);
+    return cudaGetLastError();
+}
+
+}  // namespace qs

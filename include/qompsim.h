@@ -1,0 +1,248 @@
+/*
+ * qompsim.h -- C ABI of the B200 compressed state-vector engine.
+ *
+ * Plain C: opaque handles, pointers and sizes, integer status codes.  No C++
+ * type and no exception crosses this boundary.  Each entry point names the
+ * reference interface it replaces (paths are relative to the reference
+ * project, FujitsuResearch/Compression-based-State-Vector-Simulator).
+ *
+ * Two handle types:
+ *   qs_state  -- the block-wise compressed state (CompressedQuantumState,
+ *                src/cppsim/compressed_state.hpp:9).  The compressed store
+ *                lives in device memory (HBM) for the whole life of the
+ *                handle; the reference kept it in host malloc buffers and
+ *                moved every group over PCIe each stage
+ *                (src/cppsim/compressed_state_cuda.cu:209-223, 343-370).
+ *   qs_dense  -- an uncompressed state vector in device memory (QuantumState,
+ *                src/cppsim/state.hpp:445-1045, updated gate by gate through
+ *                QuantumCircuit::update_quantum_state, src/cppsim/circuit.cpp:23-34).
+ *
+ * Threading: a handle is not re-entrant; use one handle per host thread.
+ * All device work of a handle is ordered on one CUDA stream (qs_set_stream,
+ * default: the legacy default stream).  Calls that return host data
+ * synchronise that stream.
+ */
+#ifndef QOMPSIM_H
+#define QOMPSIM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum qs_status {
+    QS_OK = 0,
+    QS_ERR_ARG = 1,              /* invalid argument (sizes, indices, bounds)          */
+    QS_ERR_CUDA = 2,             /* a CUDA runtime call failed                          */
+    QS_ERR_CAPACITY = 3,         /* compressed store does not fit the device memory     */
+    QS_ERR_UNSUPPORTED_GATE = 4, /* gate with >2 qubits, FusedSWAP (needs MPI ranks)    */
+    QS_ERR_TIMEOUT = 5,          /* reserved: a bounded device wait gave up             */
+    QS_ERR_CORRUPT = 6,          /* imported store failed its length/header checks      */
+    QS_ERR_STATE = 7,            /* call out of order (e.g. apply before registration)  */
+    QS_ERR_NOMEM = 8             /* host allocation failed                              */
+} qs_status;
+
+typedef enum qs_dtype {
+    QS_COMPLEX128 = 0,  /* amplitudes and gate arithmetic in FP64             */
+    QS_COMPLEX64 = 1    /* amplitudes and gate arithmetic in FP32; FP64 norms */
+} qs_dtype;
+
+/* Flags of qs_create. */
+#define QS_FLAG_CODE_ZERO_TEST 0x1u  /* a previously-zero block stays zero when all of its
+                                        quantised codes are 0, instead of the reference's
+                                        exact |a|^2 != 0 test (cuda_complex_helper.cuh:96-106) */
+#define QS_FLAG_REFERENCE_CONTROLS 0x2u /* reproduce the reference dispatch: controls are
+                                        honoured for "CNOT" only and 2x2 / 4x4 matrices are
+                                        applied uncontrolled, 4x4 bit0 on the lower target
+                                        (compressed_state.hpp:998-1008, compressed_state_cuda.cu:632-642) */
+#define QS_FLAG_QUIET 0x4u           /* no progress prints on stdout */
+#define QS_FLAG_PROFILE 0x8u         /* time every fused pass with CUDA events (qs_stats.kernel_ms) */
+
+/* One gate as the reference's partition_and_register_circuit binding hands
+ * it to the engine: to_matrix_gate(gate) with the original name kept
+ * (python/cppsim_wrapper.cpp:465-482). */
+typedef struct qs_gate {
+    char name[24];               /* "CNOT", "DenseMatrix", "H", ... ; "FusedSWAP" is rejected */
+    uint32_t ntargets;           /* 1 or 2                                                    */
+    uint32_t ncontrols;          /* 0..2 (targets + controls <= 2 unless REFERENCE_CONTROLS)   */
+    uint32_t targets[2];         /* matrix index bit i <-> targets[i]                          */
+    uint32_t controls[2];
+    uint32_t control_values[2];
+    double matrix[32];           /* row-major 2^ntargets x 2^ntargets, interleaved re, im      */
+} qs_gate;
+
+typedef struct qs_state qs_state;
+typedef struct qs_dense qs_dense;
+
+/* Codec / engine statistics of the last qs_apply_circuit. */
+typedef struct qs_stats {
+    uint64_t stages;             /* reference stages executed                          */
+    uint64_t passes;             /* fused device passes (a stage needs >= 1)           */
+    uint64_t tiles;              /* tiles processed (all passes)                       */
+    uint64_t bytes_read;         /* compressed payload + chunk headers read (all passes) */
+    uint64_t bytes_written;      /* compressed payload + chunk headers written          */
+    uint64_t amp_gate_updates;   /* sum over stages of gates(s) * amplitudes in active groups(s) */
+    double kernel_ms;            /* device time of the fused passes alone (QS_FLAG_PROFILE),
+                                    else equal to apply_ms                             */
+    double apply_ms;             /* device time of qs_apply_circuit end to end          */
+    int32_t mantissa_bits;       /* quantiser parameter m (relative step 2^-m)          */
+    int32_t linear_exp;          /* quantiser parameter L (absolute step 2^-L)          */
+    int32_t chunk_log2;          /* amplitudes per chunk = 2^chunk_log2                 */
+    int32_t tile_log2;           /* largest tile = 2^tile_log2 amplitudes               */
+} qs_stats;
+
+/* ---------------------------------------------------------------- errors */
+
+/* Text of the last error of `h`, or of the last failed qs_create /
+ * qs_dense_create when h is NULL.  Never NULL. */
+const char *qs_last_error(const qs_state *h);
+const char *qs_dense_last_error(const qs_dense *h);
+
+/* ------------------------------------------------------ compressed state */
+
+/* CompressedQuantumState(qubit_count, block_size) -- compressed_state.hpp:87-239
+ * and initialize_all_blocks (:327-352): block 0 holds |0...0>, all other
+ * blocks are zero (not stored).  eps_rel / eps_abs play the role of
+ * BITCOMP_REL_EB / BITCOMP_ABS_EB (:128-139); eps_rel must lie in
+ * [2^-24, 1).  Requires 4 <= block_size <= n <= 40. */
+qs_status qs_create(qs_state **out, uint32_t n, uint32_t block_size, qs_dtype dtype,
+                    double eps_rel, double eps_abs, uint32_t flags);
+
+/* ~CompressedQuantumState -- compressed_state.hpp:244-285. */
+qs_status qs_destroy(qs_state *h);
+
+/* Order all later device work of h on `cuda_stream` (a cudaStream_t). */
+qs_status qs_set_stream(qs_state *h, void *cuda_stream);
+
+/* Copy a gate list in (the gate_list argument of partition_and_register_circuit /
+ * register_circuit_stages, compressed_state.hpp:464-474, 673-682). */
+qs_status qs_register_gates(qs_state *h, const qs_gate *gates, size_t count);
+
+/* partition_and_register_circuit(gate_list, inner_size, verbose) --
+ * compressed_state.hpp:673-726: partition_circuit (:509-583) then
+ * make_block_groups (:585-671).  verbose > 0 prints "Circuit Stages: [...]",
+ * verbose > 1 also the block groups. */
+qs_status qs_partition(qs_state *h, uint32_t inner_size, int verbose);
+
+/* register_circuit_stages(gate_list, stages, block_to_group_list, stage_num_groups)
+ * -- compressed_state.hpp:464-474.  stage_gate_ids holds the gate indices of
+ * all stages back to back (stage_sizes[s] of them for stage s);
+ * block_to_group holds nstages * nblocks group ids. */
+qs_status qs_register_stages(qs_state *h, const uint32_t *stage_sizes, size_t nstages,
+                             const uint32_t *stage_gate_ids, const uint32_t *block_to_group,
+                             const uint32_t *num_groups);
+
+/* partition_circuit + make_block_groups on the host only (no device is
+ * touched): the stage plan qs_partition would build for `gates` on an
+ * n-qubit state with 2^block_size-amplitude blocks.  Call with NULL outputs
+ * to get *nstages; then stage_sizes (nstages), stage_gate_ids (count),
+ * block_to_group (nstages * 2^(n-block_size)) and num_groups (nstages),
+ * each may be NULL.  Restates compressed_state.hpp:509-671. */
+qs_status qs_plan_stages(const qs_gate *gates, size_t count, uint32_t n, uint32_t block_size,
+                         uint32_t inner_size, size_t *nstages, uint32_t *stage_sizes,
+                         uint32_t *stage_gate_ids, uint32_t *block_to_group, uint32_t *num_groups);
+
+/* Planner results: number of stages and blocks; one stage's gate ids,
+ * block->group map (nblocks entries, may be NULL) and group count. */
+qs_status qs_get_plan_info(qs_state *h, uint32_t *nstages, uint32_t *nblocks);
+qs_status qs_get_stage(qs_state *h, uint32_t stage, uint32_t *gate_ids, uint32_t cap,
+                       uint32_t *count, uint32_t *block_to_group, uint32_t *num_groups);
+
+/* apply_circuit() -- compressed_state.hpp:840-937 with process_SV_group_GPU
+ * (compressed_state_cuda.cu:143-381): every stage over its active groups,
+ * as fused device passes over the HBM-resident store. */
+qs_status qs_apply_circuit(qs_state *h);
+
+/* get_decompressed_state_vector() -- compressed_state.hpp:1683-1707: dense
+ * complex128 (interleaved re, im; 2*2^n doubles) into host memory.
+ * renormalize != 0 divides by the norm as the reference does. */
+qs_status qs_get_vector(qs_state *h, double *out, int renormalize);
+
+/* Squared norm of the compressed state, accumulated in FP64. */
+qs_status qs_norm_squared(qs_state *h, double *out);
+
+/* Zero-block mask: out[b] = 1 when block b is stored (the reference's
+ * block_pointers[b] != nullptr, compressed_state.hpp:18-19, 319-325). */
+qs_status qs_get_zero_mask(qs_state *h, uint8_t *out);
+
+/* blocks_bytes (compressed_state.hpp:19): stored bytes per block (0 for a
+ * zero block): chunk payloads plus their 16-byte chunk headers. */
+qs_status qs_get_block_bytes(qs_state *h, uint64_t *out);
+
+/* get_max_SV_bytes() -- compressed_state.hpp:439-445: the largest total
+ * over the initial state and every stage end. */
+qs_status qs_get_max_sv_bytes(qs_state *h, uint64_t *out);
+
+/* Totals after the initial state and after each stage ("Total SV bytes",
+ * compressed_state.hpp:374-437).  *count receives the number available. */
+qs_status qs_get_sv_bytes_history(qs_state *h, uint64_t *out, size_t cap, size_t *count);
+
+/* get_total_times() -- python/cppsim_wrapper.cpp:503-515, the same ten keys
+ * in this order: decomp, gate, comp, fused_swap, allgather, hmalloc, dmalloc,
+ * h2d, d2h, dfree (seconds).  "gate" holds the fused passes' device time,
+ * which also contains decoding and encoding; decomp/comp stay 0. */
+qs_status qs_get_total_times(qs_state *h, double out[10]);
+
+qs_status qs_get_stats(qs_state *h, qs_stats *out);
+
+/* Serialise the compressed store (zero mask, chunk headers and payloads) into
+ * host memory and back.  With buf == NULL, qs_export_store only reports the
+ * size.  These replace the host-resident block_pointers of the reference. */
+qs_status qs_export_store(qs_state *h, void *buf, uint64_t cap, uint64_t *size);
+qs_status qs_import_store(qs_state *h, const void *buf, uint64_t size);
+
+/* Reset to |basis> (basis < 2^n); the reference only has |0...0>. */
+qs_status qs_set_basis_state(qs_state *h, uint64_t basis);
+
+/* Load a dense complex128 vector (2*2^n doubles, host) into the compressed
+ * store, compressing it.  A block is stored when any amplitude is non-zero. */
+qs_status qs_load_vector(qs_state *h, const double *vec);
+
+/* ------------------------------------------------- uncompressed (dense) */
+
+/* QuantumState(qubit_count) on the device, initialised to |0...0>. */
+qs_status qs_dense_create(qs_dense **out, uint32_t n, qs_dtype dtype);
+qs_status qs_dense_destroy(qs_dense *h);
+qs_status qs_dense_set_stream(qs_dense *h, void *cuda_stream);
+
+/* QuantumCircuit::update_quantum_state(state) (src/cppsim/circuit.cpp:23-34):
+ * the gates are applied in order, grouped into fused tile passes. */
+qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count);
+
+/* The plain path: one full-vector kernel per gate, as the reference's
+ * gpusim kernels do (e.g. double_qubit_dense_matrix_gate_host,
+ * src/gpusim/update_ops_multi.cu:373).  Used as the per-gate baseline. */
+qs_status qs_dense_apply_gates_pergate(qs_dense *h, const qs_gate *gates, size_t count);
+
+/* QuantumState::get_vector / load (state.hpp:445-1045); 2*2^n doubles. */
+qs_status qs_dense_get_vector(qs_dense *h, double *out);
+qs_status qs_dense_set_vector(qs_dense *h, const double *in);
+qs_status qs_dense_set_basis_state(qs_dense *h, uint64_t basis);
+qs_status qs_dense_norm_squared(qs_dense *h, double *out);
+
+/* Device pointer of the amplitudes (interleaved re, im of the dtype). */
+qs_status qs_dense_device_ptr(qs_dense *h, void **out);
+
+/* ------------------------------------------------------------- codec */
+
+/* Quantiser parameters (m, L) the engine derives from eps_rel / eps_abs. */
+qs_status qs_codec_params(qs_dtype dtype, double eps_rel, double eps_abs,
+                          int32_t *m, int32_t *L);
+
+/* Encode nchunks chunks of 2^chunk_log2 amplitudes (vals: interleaved re, im
+ * of the dtype, host memory) on the device and decode them again.  words
+ * receives each chunk's payload at a stride of 2^(chunk_log2+1) words, bases
+ * and widths its frame of reference, decoded the round-tripped values.  It
+ * exists to check the device codec against its CPU statement bit for bit;
+ * the reference has no counterpart (Bitcomp is a closed library). */
+qs_status qs_codec_test(qs_dtype dtype, double eps_rel, double eps_abs, uint32_t chunk_log2,
+                        const void *vals, uint64_t nchunks, uint32_t *words, int32_t *bases,
+                        uint32_t *widths, void *decoded);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QOMPSIM_H */

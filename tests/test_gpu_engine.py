@@ -1,0 +1,303 @@
+"""GPU parity tests of the engine through its C ABI (run with -m gpu).
+
+Bars:
+* codec: device codes, packed words, frames and decoded values equal the
+  CPU statement (oracle/codec_oracle.c) bit for bit;
+* uncompressed path (QuantumState, fused tile passes and the plain per-gate
+  kernels): complex128 within 1e-12 per amplitude of the reference's csim
+  kernels; complex64 within 2e-6;
+* compressed path: zero-block masks and stage lists equal the oracle's
+  restatement of the reference planner/pipeline; amplitudes within the codec's
+  error budget of the FP64 csim result; fidelity |<psi_ref|psi>| >= 0.999 at
+  the reference's default bounds (BITCOMP_REL_EB 1e-3, BITCOMP_ABS_EB 1e-7).
+"""
+import math
+
+import numpy as np
+import pytest
+
+import helpers
+from oracle import codec as oc
+from oracle import csim_ref, pipeline, planner
+
+pytestmark = pytest.mark.gpu
+
+F64_TOL = 1e-12
+F32_TOL = 2e-6
+
+
+@pytest.fixture(scope="module")
+def qulacs_mod():
+    import qulacs
+    from qulacs import _native
+    _native.load_library()
+    return qulacs
+
+
+# ------------------------------------------------------------------ codec
+@pytest.mark.parametrize("f64", [True, False])
+@pytest.mark.parametrize("C", [4, 5, 7, 8])
+def test_device_codec_bit_identical(qulacs_mod, f64, C):
+    import ctypes as ct
+    from qulacs import _native
+    L = _native.lib()
+    rng = np.random.default_rng(100 + C)
+    nch = 64
+    n = 2 << C
+    vals = np.concatenate([
+        np.zeros(n), np.eye(1, n, 3).ravel(),
+        *[rng.normal(scale=10.0 ** -rng.uniform(0, 7), size=n) for _ in range(nch - 3)],
+        np.where(rng.random(n) < 0.1, rng.normal(size=n), 0.0),
+    ])
+    dt = np.float64 if f64 else np.float32
+    vals = np.ascontiguousarray(vals.astype(dt))
+    words = np.zeros(nch * n, dtype=np.uint32)
+    bases = np.zeros(nch, dtype=np.int32)
+    widths = np.zeros(nch, dtype=np.uint32)
+    dec = np.zeros_like(vals)
+    st = L.qs_codec_test(0 if f64 else 1, 1e-3, 1e-7, C, vals.ctypes.data, nch,
+                         words.ctypes.data_as(ct.POINTER(ct.c_uint32)), bases.ctypes.data_as(ct.POINTER(ct.c_int32)),
+                         widths.ctypes.data_as(ct.POINTER(ct.c_uint32)), dec.ctypes.data)
+    assert st == 0, L.qs_dense_last_error(None)
+    m, Lp = oc.params(f64, 1e-3, 1e-7)
+    for k in range(nch):
+        v = vals[k * n:(k + 1) * n]
+        w, b, wd = oc.encode_chunk(v, C, m, Lp)
+        assert (bases[k], widths[k]) == (b, wd)
+        assert np.array_equal(words[k * n:k * n + w.size], w)
+        assert np.array_equal(dec[k * n:(k + 1) * n], oc.decode_chunk(w, C, b, wd, m, Lp, f64))
+
+
+# ------------------------------------------------------------------ uncompressed
+def _dense_run(qulacs, c, dtype="complex128", pergate=False):
+    s = qulacs.QuantumState(c.get_qubit_count(), dtype=dtype)
+    s._apply_gates(c._gates, pergate=pergate)
+    return s.get_vector()
+
+
+@pytest.mark.parametrize("key", sorted(helpers.golden_circuits()))
+@pytest.mark.parametrize("pergate", [False, True])
+def test_dense_golden_complex128(qulacs_mod, key, pergate):
+    c = helpers.build_circuit(key)
+    v = _dense_run(qulacs_mod, c, pergate=pergate)
+    assert np.abs(v - helpers.golden_states()[key]).max() < F64_TOL
+
+
+@pytest.mark.parametrize("n,seed", [(6, 1), (9, 2), (12, 3), (14, 4), (16, 5)])
+def test_dense_random_complex128(qulacs_mod, n, seed):
+    c = helpers.random_circuit(n, 120, seed)
+    ref = csim_ref.run_circuit(n, c._gates)
+    for pergate in (False, True):
+        v = _dense_run(qulacs_mod, c, pergate=pergate)
+        assert np.abs(v - ref).max() < F64_TOL, pergate
+
+
+@pytest.mark.parametrize("n,seed", [(10, 7), (15, 8)])
+def test_dense_random_complex64(qulacs_mod, n, seed):
+    c = helpers.random_circuit(n, 80, seed)
+    ref = csim_ref.run_circuit(n, c._gates)
+    v = _dense_run(qulacs_mod, c, dtype="complex64")
+    assert np.abs(v - ref).max() < F32_TOL * 10
+
+
+def test_dense_norm_load_and_basis(qulacs_mod):
+    s = qulacs_mod.QuantumState(8)
+    rng = np.random.default_rng(0)
+    v = rng.normal(size=256) + 1j * rng.normal(size=256)
+    s.load(v)
+    assert abs(s.get_squared_norm() - np.vdot(v, v).real) < 1e-9
+    assert np.array_equal(s.get_vector(), v)
+    s.set_computational_basis(77)
+    w = s.get_vector()
+    assert w[77] == 1 and np.count_nonzero(w) == 1
+
+
+# ------------------------------------------------------------------ compressed
+def _compressed(qulacs, c, B, I, dtype="complex128", eps_rel=1e-3, eps_abs=1e-7, flags=None, basis=None):
+    from qulacs import _native
+    f = _native.QS_FLAG_QUIET if flags is None else flags
+    cq = qulacs.CompressedQuantumState(c.get_qubit_count(), B, dtype=dtype, eps_rel=eps_rel, eps_abs=eps_abs,
+                                       flags=f)
+    if basis is not None:
+        cq.set_computational_basis(basis)
+    cq.partition_and_register_circuit(c, I, 0)
+    cq.apply_circuit()
+    return cq
+
+
+def _oracle_masks(c, n, B, I, codec=None, zero_test="exact"):
+    g = planner.describe(c._gates)
+    st = planner.partition_circuit(g, B, I)
+    maps, counts = planner.make_block_groups(g, st, n, B)
+    o = pipeline.CompressedOracle(n, B, codec=codec, zero_test=zero_test)
+    o.apply(c._gates, st, maps, counts)
+    return o, st
+
+
+def test_ghz20_config(qulacs_mod):
+    from qompsim import circuits as C
+    c = helpers.optimized(C.ghz_fanout(20), 12)
+    cq = _compressed(qulacs_mod, c, 12, 4)
+    assert [len(s) for s in cq.get_stage_list()] == [15, 4]
+    assert list(np.nonzero(cq.get_zero_mask())[0]) == [0, 15, 255]
+    v = cq.get_vector()
+    ref = np.zeros(1 << 20, dtype=np.complex128)
+    ref[0] = ref[-1] = 1 / math.sqrt(2)
+    assert np.abs(v - ref).max() < 1e-3
+    assert helpers.fidelity(ref, v) > 0.999999
+    hist = cq.get_SV_bytes_history()
+    assert len(hist) == 3 and cq.get_max_SV_bytes() == max(hist)
+    bb = cq.get_block_bytes()
+    assert np.all(bb[cq.get_zero_mask() == 0] == 0) and np.all(bb[[0, 15, 255]] > 0)
+    times = cq.get_total_times()
+    assert list(times) == ["decomp", "gate", "comp", "fused_swap", "allgather", "hmalloc", "dmalloc", "h2d", "d2h",
+                           "dfree"]
+    assert times["gate"] > 0
+
+
+def test_ghz20_stage0_mask(qulacs_mod):
+    """Register only the first stage (register_circuit_stages) and read the
+    mask between the stages: {0, 15}."""
+    from qompsim import circuits as C
+    c = helpers.optimized(C.ghz_fanout(20), 12)
+    g = planner.describe(c._gates)
+    st = planner.partition_circuit(g, 12, 4)
+    maps, counts = planner.make_block_groups(g, st, 20, 12)
+    from qulacs import _native
+    cq = qulacs_mod.CompressedQuantumState(20, 12, flags=_native.QS_FLAG_QUIET)
+    groups = [[[b for b in range(256) if maps[0][b] == gid] for gid in range(counts[0])]]
+    cq.register_circuit_stages(c, [st[0]], groups)
+    cq.apply_circuit()
+    assert list(np.nonzero(cq.get_zero_mask())[0]) == [0, 15]
+
+
+@pytest.mark.parametrize("key", ["ghz_10", "qft_8", "hea_9", "qaoa_9", "wstate_8", "bv_9", "grover_11",
+                                 "ising_8", "qsvm_8", "cc_9", "hadamard_8", "seq_hadamard_9"])
+@pytest.mark.parametrize("dtype", ["complex128", "complex64"])
+def test_compressed_golden_masks_and_values(qulacs_mod, key, dtype):
+    c = helpers.optimized(helpers.build_circuit(key), 4)
+    n = c.get_qubit_count()
+    ref = helpers.golden_states()[key]
+    for B, I in [(4, 1), (5, 2), (4, 4), (n - 2, 1)]:
+        # tight bounds: values must track FP64 closely, masks must equal the oracle's
+        cq = _compressed(qulacs_mod, c, B, I, dtype=dtype, eps_rel=2.0 ** -20, eps_abs=1e-12)
+        o, st = _oracle_masks(c, n, B, I)
+        assert cq.get_stage_list() == st
+        assert np.array_equal(cq.get_zero_mask(), o.mask()), (B, I)
+        v = cq.get_vector()
+        tol = 1e-4 if dtype == "complex128" else 2e-4
+        assert np.abs(v - ref).max() < tol, (B, I)
+        # reference default bounds
+        cq = _compressed(qulacs_mod, c, B, I, dtype=dtype)
+        assert helpers.fidelity(ref, cq.get_vector()) > 0.999, (B, I)
+
+
+@pytest.mark.parametrize("n,B,seed", [(14, 8, 1), (16, 10, 2), (16, 6, 3)])
+def test_compressed_qft_analytic(qulacs_mod, n, B, seed):
+    from qompsim import circuits as C
+    c = helpers.optimized(C.qft_basis(n, seed), B)
+    cq = _compressed(qulacs_mod, c, B, 4)
+    v = cq.get_vector()
+    ref = C.qft_expected(n, C.qft_input(n, seed))
+    f = helpers.fidelity(ref, v)
+    assert f > 0.999, f
+    # the reference model: same stages, compander + Bitcomp quantiser emulated
+    o, _ = _oracle_masks(c, n, B, 4, codec=lambda x: oc.ref_compander_roundtrip_complex(x, 1e-3, 1e-7))
+    f_ref = helpers.fidelity(ref, o.vector())
+    assert f >= f_ref - 1e-4, (f, f_ref)
+
+
+@pytest.mark.parametrize("n,seed", [(12, 11), (15, 12)])
+def test_compressed_random_circuits_vs_csim(qulacs_mod, n, seed):
+    c = helpers.random_circuit(n, 100, seed)
+    ref = csim_ref.run_circuit(n, c._gates)
+    for B in (4, 7, n - 3):
+        cq = _compressed(qulacs_mod, c, B, 3, eps_rel=2.0 ** -22, eps_abs=1e-13)
+        v = cq.get_vector()
+        assert np.abs(v - ref).max() < 1e-5, B
+        o, _ = _oracle_masks(c, n, B, 3)
+        assert np.array_equal(cq.get_zero_mask(), o.mask())
+
+
+def test_compressed_load_vector_bit_exact(qulacs_mod):
+    from qulacs import _native
+    n, B = 12, 6
+    rng = np.random.default_rng(9)
+    v = (rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)) * 1e-2
+    v[: 1 << B] = 0  # block 0 all zero -> not stored
+    m, L = oc.params(True, 1e-3, 1e-7)
+    cq = qulacs_mod.CompressedQuantumState(n, B, eps_rel=1e-3, eps_abs=1e-7, flags=_native.QS_FLAG_QUIET)
+    cq.load(v)
+    got = cq.get_vector(renormalize=False)
+    assert np.array_equal(got, oc.roundtrip_complex(v, m, L))
+    mask = cq.get_zero_mask()
+    assert mask[0] == 0 and mask[1:].all()
+
+
+def test_compressed_export_import_roundtrip(qulacs_mod):
+    from qompsim import circuits as C
+    from qulacs import _native
+    c = helpers.optimized(C.qft_basis(14, 2), 8)
+    cq = _compressed(qulacs_mod, c, 8, 4)
+    blob = cq.export_store()
+    v = cq.get_vector(renormalize=False)
+    other = qulacs_mod.CompressedQuantumState(14, 8, flags=_native.QS_FLAG_QUIET)
+    other.import_store(blob)
+    assert np.array_equal(other.get_vector(renormalize=False), v)
+    assert np.array_equal(other.get_zero_mask(), cq.get_zero_mask())
+    bad = bytearray(blob)
+    bad[0] ^= 0xFF
+    with pytest.raises(_native.QompsimError) as e:
+        other.import_store(bytes(bad))
+    assert e.value.status == _native.QS_ERR_CORRUPT
+    with pytest.raises(_native.QompsimError) as e:
+        other.import_store(blob[:-16])
+    assert e.value.status == _native.QS_ERR_CORRUPT
+
+
+def test_compressed_error_paths(qulacs_mod, monkeypatch):
+    import qulacs
+    from qulacs import _native
+    cq = qulacs.CompressedQuantumState(10, 5, flags=_native.QS_FLAG_QUIET)
+    with pytest.raises(_native.QompsimError) as e:
+        cq.apply_circuit()
+    assert e.value.status == _native.QS_ERR_STATE
+    with pytest.raises(_native.QompsimError) as e:
+        qulacs.CompressedQuantumState(10, 3, flags=_native.QS_FLAG_QUIET)
+    assert e.value.status == _native.QS_ERR_ARG
+    with pytest.raises(_native.QompsimError) as e:
+        qulacs.CompressedQuantumState(10, 5, eps_rel=0.0, flags=_native.QS_FLAG_QUIET)
+    assert e.value.status == _native.QS_ERR_ARG
+    # an arena too small for the state: the kernel refuses to write past it
+    monkeypatch.setenv("QOMPSIM_ARENA_BYTES", "4096")
+    small = qulacs.CompressedQuantumState(12, 6, flags=_native.QS_FLAG_QUIET)
+    c = qulacs.QuantumCircuit(12)
+    for q in range(12):
+        c.add_H_gate(q)
+    small.partition_and_register_circuit(c, 2, 0)
+    with pytest.raises(_native.QompsimError) as e:
+        small.apply_circuit()
+    assert e.value.status == _native.QS_ERR_CAPACITY
+
+
+def test_reference_controls_flag(qulacs_mod):
+    """QS_FLAG_REFERENCE_CONTROLS applies a controlled 2x2 uncontrolled (Q3)."""
+    import qulacs
+    from qulacs import gate as G, _native
+    c = qulacs.QuantumCircuit(8)
+    c.add_H_gate(5)
+    g = G.DenseMatrix(0, [[0, 1], [1, 0]])
+    g.add_control_qubit(5, 1)
+    c.add_gate(g)
+    ok = _compressed(qulacs, c, 4, 2, eps_rel=2.0 ** -20, eps_abs=1e-12)
+    ref = csim_ref.run_circuit(8, c._gates)
+    assert np.abs(ok.get_vector() - ref).max() < 1e-5
+    quirk = _compressed(qulacs, c, 4, 2, eps_rel=2.0 ** -20, eps_abs=1e-12,
+                        flags=_native.QS_FLAG_QUIET | _native.QS_FLAG_REFERENCE_CONTROLS)
+    o = pipeline.CompressedOracle(8, 4, reference_controls=True)
+    g_ = planner.describe(c._gates)
+    st = planner.partition_circuit(g_, 4, 2)
+    maps, counts = planner.make_block_groups(g_, st, 8, 4)
+    o.apply(c._gates, st, maps, counts)
+    assert np.abs(quirk.get_vector() - o.vector()).max() < 1e-5
+    assert np.abs(quirk.get_vector() - ref).max() > 0.1
