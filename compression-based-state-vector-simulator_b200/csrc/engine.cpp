@@ -140,6 +140,7 @@ qs::KGate to_kgate(const CGate &cg, const std::vector<int> &tile_qubits, int C) 
     std::memset(&k, 0, sizeof(k));
     k.nq = cg.nq;
     k.diag = cg.diag ? 1 : 0;
+    k.mixmask = (cg.mix[0] ? 1 : 0) | (cg.nq == 2 && cg.mix[1] ? 2 : 0);
     for (int i = 0; i < cg.nq; ++i) {
         k.q[i] = cg.q[i];
         if (cg.q[i] < C) {
@@ -155,6 +156,135 @@ qs::KGate to_kgate(const CGate &cg, const std::vector<int> &tile_qubits, int C) 
         k.m[2 * r + 1] = cg.m[r].imag();
     }
     return k;
+}
+
+// Group the gates [g0, g1) of a pass (already in KGate form) into register
+// sweeps: consecutive gates whose mixing tile bits fit in RB bits share a
+// sweep; the sweep's bit set is padded with the lowest free tile bits.
+std::vector<qs::Sweep> plan_sweeps(const std::vector<qs::KGate> &kg, size_t g0, size_t g1, int nb, int RB) {
+    std::vector<qs::Sweep> out;
+    std::set<int> S;
+    size_t start = g0;
+    auto close = [&](size_t end) {
+        qs::Sweep sw{};
+        sw.g0 = (int32_t)(start - g0);
+        sw.g1 = (int32_t)(end - g0);
+        for (int b = 0; b < nb && (int)S.size() < RB; ++b) S.insert(b);
+        int k = 0;
+        for (int b : S) sw.sbits[k++] = b;
+        out.push_back(sw);
+        S.clear();
+        start = end;
+    };
+    for (size_t i = g0; i < g1; ++i) {
+        std::set<int> need = S;
+        for (int b = 0; b < kg[i].nq; ++b)
+            if ((kg[i].mixmask >> b) & 1) need.insert(kg[i].tpos[b]);
+        if ((int)need.size() > RB) {
+            close(i);
+            for (int b = 0; b < kg[i].nq; ++b)
+                if ((kg[i].mixmask >> b) & 1) S.insert(kg[i].tpos[b]);
+        } else {
+            S = need;
+        }
+    }
+    if (g1 > start || out.empty()) close(g1);
+    return out;
+}
+
+// Resolve the gates [g0, g1) of a pass against their sweeps into op records
+// and sub-matrix variants (appended to *ops and *pool).  Sweep gate ranges are
+// relative to g0; op k of the pass is gate g0 + k.
+void build_ops(const std::vector<qs::KGate> &kg, size_t g0, const std::vector<qs::Sweep> &sweeps, int RB,
+               std::vector<qs::ROp> *ops, std::vector<cplx> *pool) {
+    for (const auto &sw : sweeps) {
+        for (int gi = sw.g0; gi < sw.g1; ++gi) {
+            const qs::KGate &g = kg[g0 + gi];
+            int reg[2] = {-1, -1}, src[2] = {0, 0};
+            std::vector<int> fixed;  // gate-qubit indices that select a variant
+            for (int i = 0; i < g.nq; ++i) {
+                const int p = g.tpos[i];
+                int k = -1;
+                for (int kk = 0; kk < RB; ++kk)
+                    if (p >= 0 && sw.sbits[kk] == p) k = kk;
+                if (k >= 0) {
+                    reg[i] = k;
+                } else {
+                    src[i] = p >= 0 ? p : 64 + g.q[i];
+                    fixed.push_back(i);
+                }
+            }
+            const int dim = 1 << g.nq;
+            auto M = [&](int r, int c) { return cplx(g.m[2 * (r * dim + c)], g.m[2 * (r * dim + c) + 1]); };
+            std::vector<int> regs;
+            for (int i = 0; i < g.nq; ++i)
+                if (reg[i] >= 0) regs.push_back(i);
+            qs::ROp op{};
+            op.nsel = (uint8_t)fixed.size();
+            for (size_t j = 0; j < fixed.size(); ++j) op.sel[j] = (uint8_t)src[fixed[j]];
+            op.mat = (uint32_t)pool->size();
+            const int nvar = 1 << fixed.size();
+            // full-matrix index of register pattern x under variant v
+            auto full = [&](int x, int v) {
+                int idx = 0;
+                for (size_t r = 0; r < regs.size(); ++r)
+                    if ((x >> r) & 1) idx |= 1 << regs[r];
+                for (size_t j = 0; j < fixed.size(); ++j)
+                    if ((v >> j) & 1) idx |= 1 << fixed[j];
+                return idx;
+            };
+            const int rd = 1 << regs.size();
+            bool diag = true;
+            for (int v = 0; v < nvar; ++v)
+                for (int x = 0; x < rd; ++x)
+                    for (int y = 0; y < rd; ++y)
+                        if (x != y && M(full(x, v), full(y, v)) != cplx(0, 0)) diag = false;
+            if (regs.empty()) {
+                op.kind = qs::OP_SCALAR;
+                op.vstride = 1;
+                for (int v = 0; v < nvar; ++v) pool->push_back(M(full(0, v), full(0, v)));
+            } else if (regs.size() == 1) {
+                op.k0 = (uint8_t)reg[regs[0]];
+                if (diag) {
+                    op.kind = qs::OP_D2;
+                    op.vstride = 2;
+                    for (int v = 0; v < nvar; ++v) {
+                        pool->push_back(M(full(0, v), full(0, v)));
+                        pool->push_back(M(full(1, v), full(1, v)));
+                    }
+                } else {
+                    op.kind = qs::OP_M2;
+                    op.vstride = 4;
+                    for (int v = 0; v < nvar; ++v)
+                        for (int x = 0; x < 2; ++x)
+                            for (int y = 0; y < 2; ++y) pool->push_back(M(full(x, v), full(y, v)));
+                }
+            } else {
+                op.k0 = (uint8_t)reg[0];
+                op.k1 = (uint8_t)reg[1];
+                if (diag) {
+                    op.kind = qs::OP_D4;
+                    op.vstride = 4;
+                    for (int x = 0; x < 4; ++x) pool->push_back(M(x, x));
+                } else {
+                    op.kind = qs::OP_M4;
+                    op.vstride = 16;
+                    for (int x = 0; x < 16; ++x) pool->push_back(M(x / 4, x % 4));
+                }
+            }
+            ops->push_back(op);
+        }
+    }
+}
+
+template <typename Real>
+std::vector<Real> pool_as(const std::vector<cplx> &pool) {
+    std::vector<Real> out(2 * pool.size());
+    for (size_t i = 0; i < pool.size(); ++i) {
+        out[2 * i] = (Real)pool[i].real();
+        out[2 * i + 1] = (Real)pool[i].imag();
+    }
+    return out;
 }
 
 struct PassPlan {
@@ -248,8 +378,12 @@ struct qs_state {
         int j;
         int32_t tq[qs::kMaxTileQubits];
         uint32_t gate_off, ngates;
+        uint32_t sweep_off, nsweeps;
         bool first, final;
     };
+    qs::Sweep *sweeps_dev = nullptr;
+    qs::ROp *ops_dev = nullptr;
+    void *pool_dev = nullptr;
     std::vector<DevPass> passes;
     std::vector<uint64_t> stage_amps;   // amplitudes in active groups (for stats), filled on demand
 
@@ -290,6 +424,9 @@ struct qs_state {
         if (group_active) cudaFree(group_active);
         if (b2g_dev) cudaFree(b2g_dev);
         if (kgates) cudaFree(kgates);
+        if (sweeps_dev) cudaFree(sweeps_dev);
+        if (ops_dev) cudaFree(ops_dev);
+        if (pool_dev) cudaFree(pool_dev);
         if (history_dev) cudaFree(history_dev);
         for (auto e : pass_ev) cudaEventDestroy(e);
         if (error_dev) cudaFree(error_dev);
@@ -403,7 +540,7 @@ qs_status qs_create(qs_state **out, uint32_t n, uint32_t block_size, qs_dtype dt
     const char *cap_env = std::getenv("QOMPSIM_ARENA_BYTES");
     h->capacity = cap_env ? (uint64_t)std::strtoull(cap_env, nullptr, 10) : std::min<uint64_t>(worst, avail / 2);
     h->capacity = (h->capacity + 127) / 128 * 128;
-    if (h->capacity < 4096) {
+    if (h->capacity < std::min<uint64_t>(worst, 4096)) {
         h->err = "not enough device memory for the compressed store";
         return cleanup(QS_ERR_CAPACITY);
     }
@@ -528,6 +665,10 @@ static qs_status build_device_plan(qs_state *h) {
     const int jmax = std::min(h->tile_log2 - C, qs::kMaxTileQubits);
     const int jmin = std::min(3, jmax);
     std::vector<qs::KGate> kg;
+    std::vector<qs::Sweep> sw;
+    std::vector<qs::ROp> ops;
+    std::vector<cplx> pool;
+    const int RB = h->f64 ? qs::kRegBitsF64 : qs::kRegBitsF32;
     h->passes.clear();
     for (uint32_t s = 0; s < h->stages.size(); ++s) {
         for (uint32_t gi : h->stages[s])
@@ -544,16 +685,39 @@ static qs_status build_device_plan(qs_state *h) {
             dp.first = p == 0;
             dp.final = p + 1 == pl.size();
             for (uint32_t gi : pl[p].gates) kg.push_back(to_kgate(h->cgates[gi], pl[p].tile, C));
+            auto swp = plan_sweeps(kg, dp.gate_off, kg.size(), C + dp.j, RB);
+            build_ops(kg, dp.gate_off, swp, RB, &ops, &pool);
+            dp.sweep_off = (uint32_t)sw.size();
+            dp.nsweeps = (uint32_t)swp.size();
+            sw.insert(sw.end(), swp.begin(), swp.end());
             h->passes.push_back(dp);
         }
     }
     if (h->kgates) { cudaFree(h->kgates); h->kgates = nullptr; }
+    if (h->sweeps_dev) { cudaFree(h->sweeps_dev); h->sweeps_dev = nullptr; }
+    if (h->ops_dev) { cudaFree(h->ops_dev); h->ops_dev = nullptr; }
+    if (h->pool_dev) { cudaFree(h->pool_dev); h->pool_dev = nullptr; }
+    if (!ops.empty()) {
+        CUDA_TRY(h, cudaMalloc(&h->ops_dev, ops.size() * sizeof(qs::ROp)));
+        CUDA_TRY(h, cudaMemcpy(h->ops_dev, ops.data(), ops.size() * sizeof(qs::ROp), cudaMemcpyHostToDevice));
+    }
+    if (!pool.empty()) {
+        if (h->f64) {
+            auto pv = pool_as<double>(pool);
+            CUDA_TRY(h, cudaMalloc(&h->pool_dev, pv.size() * sizeof(double)));
+            CUDA_TRY(h, cudaMemcpy(h->pool_dev, pv.data(), pv.size() * sizeof(double), cudaMemcpyHostToDevice));
+        } else {
+            auto pv = pool_as<float>(pool);
+            CUDA_TRY(h, cudaMalloc(&h->pool_dev, pv.size() * sizeof(float)));
+            CUDA_TRY(h, cudaMemcpy(h->pool_dev, pv.data(), pv.size() * sizeof(float), cudaMemcpyHostToDevice));
+        }
+    }
+    if (!sw.empty()) {
+        CUDA_TRY(h, cudaMalloc(&h->sweeps_dev, sw.size() * sizeof(qs::Sweep)));
+        CUDA_TRY(h, cudaMemcpy(h->sweeps_dev, sw.data(), sw.size() * sizeof(qs::Sweep), cudaMemcpyHostToDevice));
+    }
     if (h->b2g_dev) { cudaFree(h->b2g_dev); h->b2g_dev = nullptr; }
     if (h->history_dev) { cudaFree(h->history_dev); h->history_dev = nullptr; }
-    if (!kg.empty()) {
-        CUDA_TRY(h, cudaMalloc(&h->kgates, kg.size() * sizeof(qs::KGate)));
-        CUDA_TRY(h, cudaMemcpy(h->kgates, kg.data(), kg.size() * sizeof(qs::KGate), cudaMemcpyHostToDevice));
-    }
     const size_t ns = h->stages.size();
     if (ns) {
         CUDA_TRY(h, cudaMalloc(&h->b2g_dev, ns * h->nb * sizeof(uint32_t)));
@@ -711,8 +875,10 @@ qs_status qs_apply_circuit(qs_state *h) {
             a.j = dp.j;
             for (int k = 0; k < dp.j; ++k) a.tq[k] = dp.tq[k];
             a.n_tiles = uint64_t(1) << (h->n - C - dp.j);
-            a.gates = h->kgates + dp.gate_off;
-            a.ngates = (int)dp.ngates;
+            a.ops = h->ops_dev + dp.gate_off;
+            a.pool = h->pool_dev;
+            a.sweeps = h->sweeps_dev + dp.sweep_off;
+            a.nsweeps = (int)dp.nsweeps;
             a.codec = h->codec;
             a.meta_in = h->meta[h->cur];
             a.arena_in = h->arena[h->cur];
@@ -725,7 +891,7 @@ qs_status qs_apply_circuit(qs_state *h) {
             a.mask = h->mask;
             a.first_pass = dp.first;
             a.final_pass = dp.final;
-            a.exact_zero = (h->flags & QS_FLAG_CODE_ZERO_TEST) ? 0 : 1;
+            a.exact_zero = (h->flags & QS_FLAG_EXACT_ZERO_TEST) ? 1 : 0;
             a.block_nz = h->block_nz;
             a.block_bytes = h->block_acc;
             a.error = h->error_dev;
@@ -1009,10 +1175,19 @@ struct qs_dense {
     std::string err = "no error";
     qs::KGate *kg = nullptr;
     size_t kg_cap = 0;
+    qs::Sweep *sw = nullptr;
+    size_t sw_cap = 0;
+    qs::ROp *ops = nullptr;
+    size_t ops_cap = 0;
+    void *pool = nullptr;
+    size_t pool_cap = 0;  // bytes
     double *dscratch = nullptr;
     ~qs_dense() {
         if (state) cudaFree(state);
         if (kg) cudaFree(kg);
+        if (sw) cudaFree(sw);
+        if (ops) cudaFree(ops);
+        if (pool) cudaFree(pool);
         if (dscratch) cudaFree(dscratch);
     }
     uint64_t dim() const { return uint64_t(1) << n; }
@@ -1116,24 +1291,74 @@ qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) 
     const int tl = env_int("QOMPSIM_DENSE_TILE_LOG2", h->f64 ? 12 : 13);
     const int tile_log2 = std::min<int>((int)h->n, std::min<int>(tl, C + qs::kMaxTileQubits));
     const int jmax = tile_log2 - C;
+    const int RB = h->f64 ? qs::kRegBitsF64 : qs::kRegBitsF32;
+    if ((int)h->n < RB) return qs_dense_apply_gates_pergate(h, gates, count);
     std::vector<uint32_t> ids(count);
     for (size_t i = 0; i < count; ++i) ids[i] = (uint32_t)i;
     auto pl = plan_passes(ids, cg, C, jmax, std::min(jmax, 3), C, (int)h->n);
     std::vector<qs::KGate> kg;
-    for (auto &p : pl)
-        for (uint32_t gi : p.gates) kg.push_back(to_kgate(cg[gi], p.tile, C));
-    s = dense_upload_gates(h, kg);
-    if (s != QS_OK) return s;
-    size_t off = 0;
+    std::vector<qs::Sweep> sw;
+    std::vector<qs::ROp> ops;
+    std::vector<cplx> pool;
+    std::vector<std::pair<size_t, size_t>> sweep_ranges;
     for (auto &p : pl) {
+        // a tile must hold at least the RB register bits
+        std::set<int> t(p.tile.begin(), p.tile.end());
+        for (int q = C; q < (int)h->n && C + (int)t.size() < RB; ++q) t.insert(q);
+        p.tile.assign(t.begin(), t.end());
+        const size_t g0 = kg.size();
+        for (uint32_t gi : p.gates) kg.push_back(to_kgate(cg[gi], p.tile, C));
+        auto swp = plan_sweeps(kg, g0, kg.size(), C + (int)p.tile.size(), RB);
+        build_ops(kg, g0, swp, RB, &ops, &pool);
+        sweep_ranges.push_back({sw.size(), swp.size()});
+        sw.insert(sw.end(), swp.begin(), swp.end());
+    }
+    if (ops.size() > h->ops_cap) {
+        if (h->ops) cudaFree(h->ops);
+        h->ops = nullptr;
+        h->ops_cap = 0;
+        CUDA_TRY(h, cudaMalloc(&h->ops, ops.size() * sizeof(qs::ROp)));
+        h->ops_cap = ops.size();
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(h->ops, ops.data(), ops.size() * sizeof(qs::ROp), cudaMemcpyHostToDevice, h->stream));
+    {
+        const size_t bytes = pool.size() * 2 * (h->f64 ? sizeof(double) : sizeof(float));
+        if (bytes > h->pool_cap) {
+            if (h->pool) cudaFree(h->pool);
+            h->pool = nullptr;
+            h->pool_cap = 0;
+            CUDA_TRY(h, cudaMalloc(&h->pool, bytes));
+            h->pool_cap = bytes;
+        }
+        if (h->f64) {
+            auto pv = pool_as<double>(pool);
+            CUDA_TRY(h, cudaMemcpy(h->pool, pv.data(), bytes, cudaMemcpyHostToDevice));
+        } else {
+            auto pv = pool_as<float>(pool);
+            CUDA_TRY(h, cudaMemcpy(h->pool, pv.data(), bytes, cudaMemcpyHostToDevice));
+        }
+    }
+    if (sw.size() > h->sw_cap) {
+        if (h->sw) cudaFree(h->sw);
+        h->sw = nullptr;
+        h->sw_cap = 0;
+        CUDA_TRY(h, cudaMalloc(&h->sw, sw.size() * sizeof(qs::Sweep)));
+        h->sw_cap = sw.size();
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(h->sw, sw.data(), sw.size() * sizeof(qs::Sweep), cudaMemcpyHostToDevice, h->stream));
+    size_t off = 0;
+    for (size_t pi = 0; pi < pl.size(); ++pi) {
+        auto &p = pl[pi];
         qs::DensePassArgs a{};
         a.n = (int)h->n;
         a.C = C;
         a.j = (int)p.tile.size();
         for (int k = 0; k < a.j; ++k) a.tq[k] = p.tile[k] - C;
         a.n_tiles = uint64_t(1) << (h->n - C - a.j);
-        a.gates = h->kg + off;
-        a.ngates = (int)p.gates.size();
+        a.ops = h->ops + off;
+        a.pool = h->pool;
+        a.sweeps = h->sw + sweep_ranges[pi].first;
+        a.nsweeps = (int)sweep_ranges[pi].second;
         a.state = h->state;
         off += p.gates.size();
         CUDA_TRY(h, qs::launch_dense_pass(h->f64, a, tile_log2, h->stream));

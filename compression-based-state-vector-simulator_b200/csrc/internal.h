@@ -37,9 +37,39 @@ struct KGate {
     int32_t q[2];
     int32_t tpos[2];
     int32_t diag;
-    int32_t pad[2];
+    int32_t mixmask;    // bit i: the gate mixes amplitudes along q[i]
+    int32_t pad;
     double m[32];
 };
+
+// Register blocking: a sweep applies gates g0..g1-1 of a pass in one pass
+// over the tile in shared memory.  Each thread holds 2^RB amplitudes whose
+// tile indices differ in the sweep's RB tile bits `sbits` (ascending); every
+// gate of the sweep mixes amplitudes only along those bits (diagonal action
+// on any other bit is allowed).  RB = 3 for complex128, 4 for complex64.
+constexpr int kRegBitsF64 = 3;
+constexpr int kRegBitsF32 = 4;
+struct Sweep {
+    int32_t g0, g1;
+    int32_t sbits[4];
+};
+
+// A gate resolved against its sweep (host-built).  Register bits k0/k1 index
+// the sweep bits; the gate's other qubits are fixed for a register group and
+// select one of 2^nsel pre-computed sub-matrix variants: selector source
+// sel[j] < 64 is a tile bit (its value comes from the group), sel[j] >= 64 is
+// qubit sel[j]-64 outside the tile (its value comes from the tile).
+enum : uint8_t { OP_SCALAR = 0, OP_D2 = 1, OP_M2 = 2, OP_D4 = 3, OP_M4 = 4 };
+struct ROp {
+    uint8_t kind;
+    uint8_t k0, k1;      // register bits; for D4/M4 k0 <-> matrix bit 0
+    uint8_t nsel;
+    uint8_t sel[2];
+    uint8_t pad[2];
+    uint32_t mat;        // pool index of variant 0 (complex entries)
+    uint32_t vstride;    // complex entries per variant: 1, 2, 4 or 16
+};
+static_assert(sizeof(ROp) == 16, "ROp is one 16-byte load");
 static_assert(sizeof(KGate) == 288, "KGate layout");
 
 struct CodecParams {
@@ -52,8 +82,10 @@ struct PassArgs {
     int32_t n, B, C, j;                 // qubits, block log2, chunk log2, tile qubits above C
     int32_t tq[kMaxTileQubits];         // tile qubits minus C (chunk-index bit), ascending
     uint64_t n_tiles;                   // 2^(n - C - j)
-    const KGate *gates;
-    int32_t ngates;
+    const ROp *ops;
+    const void *pool;                   // double2 (complex128) or float2 (complex64)
+    const Sweep *sweeps;
+    int32_t nsweeps;
     CodecParams codec;
     const ChunkMeta *meta_in;
     const uint32_t *arena_in;
@@ -76,8 +108,10 @@ struct DensePassArgs {
     int32_t n, C, j;
     int32_t tq[kMaxTileQubits];
     uint64_t n_tiles;
-    const KGate *gates;
-    int32_t ngates;
+    const ROp *ops;
+    const void *pool;
+    const Sweep *sweeps;
+    int32_t nsweeps;
     void *state;
 };
 

@@ -67,132 +67,266 @@ __device__ __forceinline__ uint64_t deposit_bits(uint32_t c, const int32_t *pos,
     return r;
 }
 
-// ------------------------------------------------------------ tile gates
-// All routines run on every thread of the CTA over a tile of 2^nb elements.
+// ------------------------------------------------------------ tile layout
+// Element e of a tile lives at shared-memory slot swz(e) = e ^ ((e >> S1) & m):
+// an XOR of the low S1 bits with the next ones, so that a warp whose lanes
+// differ in any set of tile bits spreads over the banks.  m is limited to
+// bits below the chunk size, so an element never leaves its chunk's region.
+template <typename R> struct Layout;
+template <> struct Layout<double> { static constexpr int S1 = 3; static constexpr int RB = kRegBitsF64; };
+template <> struct Layout<float> { static constexpr int S1 = 4; static constexpr int RB = kRegBitsF32; };
 
-template <typename T>
-__device__ void tile_2x2(T *t, int nb, int p, T e0, T e1, T e2, T e3) {
-    const int half = 1 << (nb - 1);
-    const int lowmask = (1 << p) - 1;
-    for (int i = threadIdx.x; i < half; i += blockDim.x) {
-        const int i0 = ((i & ~lowmask) << 1) | (i & lowmask);
-        const int i1 = i0 | (1 << p);
-        const T a = t[i0], b = t[i1];
-        t[i0] = cfma(e0, a, cmul(e1, b));
-        t[i1] = cfma(e2, a, cmul(e3, b));
+template <typename R>
+__host__ __device__ __forceinline__ int swizzle_mask(int C) {
+    const int room = C - Layout<R>::S1;  // chunk bits above S1
+    const int bits = room < Layout<R>::S1 ? (room > 0 ? room : 0) : Layout<R>::S1;
+    return (1 << bits) - 1;
+}
+
+template <typename R>
+__device__ __forceinline__ int swz(int e, int m) {
+    return e ^ ((e >> Layout<R>::S1) & m);
+}
+
+// ------------------------------------------------------------ register gates
+// v[s], s < NS = 2^RB, holds the tile element whose sweep bits equal s.
+template <int NS, int K, typename T>
+__device__ __forceinline__ void r_2x2(T (&v)[NS], T e0, T e1, T e2, T e3) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        if ((s >> K) & 1) continue;
+        const T a = v[s], b = v[s | (1 << K)];
+        v[s] = cfma(e0, a, cmul(e1, b));
+        v[s | (1 << K)] = cfma(e2, a, cmul(e3, b));
     }
 }
 
-template <typename T>
-__device__ void tile_diag2(T *t, int nb, int p, T d0, T d1) {
-    const int size = 1 << nb;
-    for (int i = threadIdx.x; i < size; i += blockDim.x) {
-        t[i] = cmul(((i >> p) & 1) ? d1 : d0, t[i]);
-    }
+template <int NS, int K, typename T>
+__device__ __forceinline__ void r_diag2(T (&v)[NS], T d0, T d1) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) v[s] = cmul(((s >> K) & 1) ? d1 : d0, v[s]);
 }
 
-template <typename T>
-__device__ void tile_4x4(T *t, int nb, int pa, int pb, const T *m) {
-    const int quarter = 1 << (nb - 2);
-    const int lo = pa < pb ? pa : pb, hi = pa < pb ? pb : pa;
-    const int mlo = (1 << lo) - 1, mhi = (1 << hi) - 1;
-    for (int i = threadIdx.x; i < quarter; i += blockDim.x) {
-        // insert zeros at lo, then at hi
-        int b = ((i & ~mlo) << 1) | (i & mlo);
-        b = ((b & ~mhi) << 1) | (b & mhi);
-        const int ia = 1 << pa, ib = 1 << pb;
-        const T v0 = t[b], v1 = t[b | ia], v2 = t[b | ib], v3 = t[b | ia | ib];
+template <int NS, int KA, int KB, typename T>
+__device__ __forceinline__ void r_4x4(T (&v)[NS], const T *__restrict__ m) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        if (((s >> KA) & 1) || ((s >> KB) & 1)) continue;
+        const int i0 = s, i1 = s | (1 << KA), i2 = s | (1 << KB), i3 = s | (1 << KA) | (1 << KB);
+        const T x0 = v[i0], x1 = v[i1], x2 = v[i2], x3 = v[i3];
         T o[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            T acc = cmul(m[4 * r + 0], v0);
-            acc = cfma(m[4 * r + 1], v1, acc);
-            acc = cfma(m[4 * r + 2], v2, acc);
-            acc = cfma(m[4 * r + 3], v3, acc);
+            T acc = cmul(m[4 * r + 0], x0);
+            acc = cfma(m[4 * r + 1], x1, acc);
+            acc = cfma(m[4 * r + 2], x2, acc);
+            acc = cfma(m[4 * r + 3], x3, acc);
             o[r] = acc;
         }
-        t[b] = o[0];
-        t[b | ia] = o[1];
-        t[b | ib] = o[2];
-        t[b | ia | ib] = o[3];
+        v[i0] = o[0];
+        v[i1] = o[1];
+        v[i2] = o[2];
+        v[i3] = o[3];
+    }
+}
+
+template <int NS, int KA, int KB, typename T>
+__device__ __forceinline__ void r_diag4(T (&v)[NS], T d0, T d1, T d2, T d3) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int k = ((s >> KA) & 1) | (((s >> KB) & 1) << 1);
+        v[s] = cmul(k == 0 ? d0 : (k == 1 ? d1 : (k == 2 ? d2 : d3)), v[s]);
     }
 }
 
 template <typename T>
-__device__ void tile_diag4(T *t, int nb, int pa, int pb, T d0, T d1, T d2, T d3) {
-    const int size = 1 << nb;
-    for (int i = threadIdx.x; i < size; i += blockDim.x) {
-        const int k = ((i >> pa) & 1) | (((i >> pb) & 1) << 1);
-        const T d = k == 0 ? d0 : (k == 1 ? d1 : (k == 2 ? d2 : d3));
-        t[i] = cmul(d, t[i]);
-    }
-}
+__device__ __forceinline__ bool is_one(T c) { return c.x == 1 && c.y == 0; }
 
 template <typename T>
-__device__ void tile_scale(T *t, int nb, T s) {
-    if (s.x == 1 && s.y == 0) return;
-    const int size = 1 << nb;
-    for (int i = threadIdx.x; i < size; i += blockDim.x) t[i] = cmul(s, t[i]);
+__device__ __forceinline__ T c_one() { T r; r.x = 1; r.y = 0; return r; }
+
+// Pending diagonal factors of a register group: the amplitude with register
+// index s still has to be multiplied by z * prod_k (bit k of s ? d1[k] : d0[k]).
+// Diagonal gates accumulate here (one complex product per gate and group);
+// a mixing gate on bit k first applies the factors of bit k.
+template <int RB, typename T>
+struct Pending {
+    T z, d0[RB], d1[RB];
+    __device__ __forceinline__ void reset() {
+        z = c_one<T>();
+#pragma unroll
+        for (int k = 0; k < RB; ++k) d0[k] = d1[k] = c_one<T>();
+    }
+};
+
+template <int RB, typename T>
+__device__ __forceinline__ void pend_d2(Pending<RB, T> &p, int k, T a, T b) {
+#define QS_PD(K)                                         \
+    case K:                                              \
+        if constexpr (K < RB) {                          \
+            p.d0[K] = cmul(p.d0[K], a);                  \
+            p.d1[K] = cmul(p.d1[K], b);                  \
+        }                                                \
+        break;
+    switch (k) { QS_PD(0) QS_PD(1) QS_PD(2) QS_PD(3) default: break; }
+#undef QS_PD
 }
 
-// Apply one gate to the tile whose element 0 is global amplitude base_amp
-// (all tile bits zero there, so qubits outside the tile read their fixed
-// value from base_amp).
+template <int RB, typename T>
+__device__ __forceinline__ void flush_bit(T (&v)[1 << RB], Pending<RB, T> &p, int k) {
+    constexpr int NS = 1 << RB;
+#define QS_FB(K)                                                          \
+    case K:                                                               \
+        if constexpr (K < RB) {                                           \
+            if (!is_one(p.d0[K]) || !is_one(p.d1[K])) {                   \
+                r_diag2<NS, K>(v, p.d0[K], p.d1[K]);                      \
+                p.d0[K] = p.d1[K] = c_one<T>();                           \
+            }                                                             \
+        }                                                                 \
+        break;
+    switch (k) { QS_FB(0) QS_FB(1) QS_FB(2) QS_FB(3) default: break; }
+#undef QS_FB
+}
+
+template <int RB, typename T>
+__device__ __forceinline__ void flush_all(T (&v)[1 << RB], Pending<RB, T> &p) {
+    constexpr int NS = 1 << RB;
+    bool any = !is_one(p.z);
+#pragma unroll
+    for (int k = 0; k < RB; ++k) any |= !is_one(p.d0[k]) || !is_one(p.d1[k]);
+    if (!any) return;
+    T f[NS];
+    f[0] = p.z;
+#pragma unroll
+    for (int k = 0; k < RB; ++k) {
+#pragma unroll
+        for (int s = 0; s < (1 << k); ++s) {
+            f[s | (1 << k)] = cmul(f[s], p.d1[k]);
+            f[s] = cmul(f[s], p.d0[k]);
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) v[s] = cmul(f[s], v[s]);
+    p.reset();
+}
+
+template <int RB, typename T>
+__device__ __forceinline__ void d_m2(T (&v)[1 << RB], int k, const T *m) {
+    constexpr int NS = 1 << RB;
+#define QS_CASE2(K)                                               \
+    case K:                                                       \
+        if constexpr (K < RB) r_2x2<NS, K>(v, m[0], m[1], m[2], m[3]); \
+        break;
+    switch (k) { QS_CASE2(0) QS_CASE2(1) QS_CASE2(2) QS_CASE2(3) default: break; }
+#undef QS_CASE2
+}
+
+template <int RB, typename T>
+__device__ __forceinline__ void d_44(T (&v)[1 << RB], int ka, int kb, bool diag, const T *m) {
+    constexpr int NS = 1 << RB;
+#define QS_CASE4(A, B)                                                            \
+    case (A) * 4 + (B):                                                           \
+        if constexpr ((A) < RB && (B) < RB && (A) != (B)) {                       \
+            if (diag) r_diag4<NS, A, B>(v, m[0], m[1], m[2], m[3]);               \
+            else r_4x4<NS, A, B>(v, m);                                           \
+        }                                                                         \
+        break;
+    switch (ka * 4 + kb) {
+        QS_CASE4(0, 1) QS_CASE4(0, 2) QS_CASE4(0, 3) QS_CASE4(1, 0) QS_CASE4(1, 2) QS_CASE4(1, 3)
+        QS_CASE4(2, 0) QS_CASE4(2, 1) QS_CASE4(2, 3) QS_CASE4(3, 0) QS_CASE4(3, 1) QS_CASE4(3, 2)
+        default: break;
+    }
+#undef QS_CASE4
+}
+
+// Apply every sweep of a pass to a tile of 2^nb elements whose element 0 is
+// global amplitude base_amp.
 template <typename R>
-__device__ void tile_apply_gate(typename Cplx<R>::T *t, int nb, const KGate &g, uint64_t base_amp) {
+__device__ void tile_sweeps(typename Cplx<R>::T *tile, int nb, int swm, const Sweep *__restrict__ sweeps,
+                            int nsweeps, const ROp *__restrict__ ops, const typename Cplx<R>::T *__restrict__ pool,
+                            uint64_t base_amp) {
     using T = typename Cplx<R>::T;
-    const double *m = g.m;
-    auto M = [&](int r, int c) -> T {
-        const int k = 2 * (r * (g.nq == 1 ? 2 : 4) + c);
-        return make_c<T, R>(m[k], m[k + 1]);
-    };
-    if (g.nq == 1) {
-        const int p = g.tpos[0];
-        if (p >= 0) {
-            if (g.diag) tile_diag2(t, nb, p, M(0, 0), M(1, 1));
-            else tile_2x2(t, nb, p, M(0, 0), M(0, 1), M(1, 0), M(1, 1));
-        } else {
-            const int v = (int)((base_amp >> g.q[0]) & 1);
-            tile_scale(t, nb, M(v, v));
-        }
-        return;
-    }
-    const bool in0 = g.tpos[0] >= 0, in1 = g.tpos[1] >= 0;
-    if (in0 && in1) {
-        if (g.diag) {
-            tile_diag4(t, nb, g.tpos[0], g.tpos[1], M(0, 0), M(1, 1), M(2, 2), M(3, 3));
-        } else {
-            T mm[16];
+    constexpr int RB = Layout<R>::RB;
+    constexpr int NS = 1 << RB;
+    const int groups = 1 << (nb - RB);
+    for (int w = 0; w < nsweeps; ++w) {
+        const Sweep sw = sweeps[w];
+        int sb[RB];
 #pragma unroll
-            for (int r = 0; r < 4; ++r)
+        for (int k = 0; k < RB; ++k) sb[k] = sw.sbits[k];
+        int off[NS];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) mm[4 * r + c] = M(r, c);
-            tile_4x4(t, nb, g.tpos[0], g.tpos[1], mm);
+        for (int s = 0; s < NS; ++s) {
+            int o = 0;
+#pragma unroll
+            for (int k = 0; k < RB; ++k) o |= ((s >> k) & 1) << sb[k];
+            off[s] = o;
         }
-    } else if (in0 || in1) {
-        const int b = in0 ? 0 : 1;             // matrix bit that varies in the tile
-        const int p = in0 ? g.tpos[0] : g.tpos[1];
-        const int v = (int)((base_amp >> g.q[1 - b]) & 1);
-        auto idx = [&](int x) { return b == 0 ? (x | (v << 1)) : (v | (x << 1)); };
-        if (g.diag) tile_diag2(t, nb, p, M(idx(0), idx(0)), M(idx(1), idx(1)));
-        else tile_2x2(t, nb, p, M(idx(0), idx(0)), M(idx(0), idx(1)), M(idx(1), idx(0)), M(idx(1), idx(1)));
-    } else {
-        const int v0 = (int)((base_amp >> g.q[0]) & 1), v1 = (int)((base_amp >> g.q[1]) & 1);
-        const int k = v0 | (v1 << 1);
-        tile_scale(t, nb, M(k, k));
+        for (int grp = threadIdx.x; grp < groups; grp += blockDim.x) {
+            int base = grp;
+#pragma unroll
+            for (int k = 0; k < RB; ++k) {
+                const int t = sb[k];
+                base = ((base >> t) << (t + 1)) | (base & ((1 << t) - 1));
+            }
+            T v[NS];
+#pragma unroll
+            for (int s = 0; s < NS; ++s) v[s] = tile[swz<R>(base | off[s], swm)];
+            Pending<RB, T> pend;
+            pend.reset();
+            for (int k = sw.g0; k < sw.g1; ++k) {
+                const ROp o = ops[k];
+                int var = 0;
+                for (int jj = 0; jj < o.nsel; ++jj) {
+                    const int src = o.sel[jj];
+                    const int bit = src < 64 ? (base >> src) & 1 : (int)((base_amp >> (src - 64)) & 1);
+                    var |= bit << jj;
+                }
+                const T *m = pool + o.mat + (uint32_t)var * o.vstride;
+                switch (o.kind) {
+                    case OP_SCALAR: pend.z = cmul(pend.z, m[0]); break;
+                    case OP_D2: pend_d2<RB>(pend, o.k0, m[0], m[1]); break;
+                    case OP_M2:
+                        flush_bit<RB>(v, pend, o.k0);
+                        d_m2<RB>(v, o.k0, m);
+                        break;
+                    case OP_D4: d_44<RB>(v, o.k0, o.k1, true, m); break;
+                    default:
+                        flush_bit<RB>(v, pend, o.k0);
+                        flush_bit<RB>(v, pend, o.k1);
+                        d_44<RB>(v, o.k0, o.k1, false, m);
+                        break;
+                }
+            }
+            flush_all<RB>(v, pend);
+#pragma unroll
+            for (int s = 0; s < NS; ++s) tile[swz<R>(base | off[s], swm)] = v[s];
+        }
+        __syncthreads();
     }
 }
 
 // ------------------------------------------------------------ chunk codec
 // Per-warp decode of one chunk into comp[lane + 32 i] (i < per_lane).
+struct LinearSlot {
+    __device__ __forceinline__ int operator()(int c) const { return c; }
+};
+
+// Component c of chunk `chunk` inside a swizzled tile.
 template <typename R>
+struct TileSlot {
+    int elem0, swm;
+    __device__ __forceinline__ int operator()(int c) const { return 2 * swz<R>(elem0 + (c >> 1), swm) + (c & 1); }
+};
+
+template <typename R, typename Slot = LinearSlot>
 __device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena, const ChunkMeta md,
                                              int per_lane, CodecParams p, R *comp, uint32_t *wstage,
-                                             int lane) {
+                                             int lane, Slot slot = Slot()) {
     const uint32_t w = md.width;
     if (w == 0) {
         const R v = dequantize(md.base, p, R());
-        for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = v;
+        for (int i = 0; i < per_lane; ++i) comp[slot(lane + 32 * i)] = v;
         return;
     }
     const uint32_t rows = (uint32_t)(((uint32_t)per_lane * w + 31) >> 5);
@@ -216,23 +350,23 @@ __device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena,
         const uint32_t u = (uint32_t)(buf & mask);
         buf >>= w;
         nbits -= w;
-        comp[lane + 32 * i] = dequantize((int32_t)((uint32_t)md.base + u), p, R());
+        comp[slot(lane + 32 * i)] = dequantize((int32_t)((uint32_t)md.base + u), p, R());
     }
 }
 
 // Per-warp quantisation of one chunk held in comp[]: codes overwrite the
 // chunk's own shared memory as int32 (all values are read first).  Returns
 // base/width/non-zero flag (valid in every lane).
-template <typename R>
+template <typename R, typename Slot = LinearSlot>
 __device__ __forceinline__ void quantize_chunk(R *comp, int per_lane, CodecParams p, bool exact_zero,
                                                int lane, int32_t *base_out, uint32_t *width_out,
-                                               bool *nz_out) {
+                                               bool *nz_out, Slot slot = Slot(), int32_t *codes = nullptr) {
     R v[kMaxPerLane];
 #pragma unroll
     for (int i = 0; i < kMaxPerLane; ++i)
-        if (i < per_lane) v[i] = comp[lane + 32 * i];
+        if (i < per_lane) v[i] = comp[slot(lane + 32 * i)];
     __syncwarp();
-    int32_t *codes = reinterpret_cast<int32_t *>(comp);
+    if (codes == nullptr) codes = reinterpret_cast<int32_t *>(comp);
     int32_t lo = INT_MAX, hi = INT_MIN;
     bool nz = false;
 #pragma unroll
@@ -289,11 +423,14 @@ size_t pass_smem_bytes(bool f64, int nb, int j) {
 
 // ------------------------------------------------------------ pass kernel
 template <typename R>
-__global__ void __launch_bounds__(kPassThreads) pass_kernel(const PassArgs a) {
+__global__ void __launch_bounds__(kPassThreads, 2) pass_kernel(const PassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ unsigned long long s_tile_off;
     __shared__ int s_flag;
+    __shared__ int32_t s_tq[kMaxTileQubits];
+    if (threadIdx.x < kMaxTileQubits) s_tq[threadIdx.x] = a.tq[threadIdx.x];
+    __syncthreads();
 
     const int C = a.C, j = a.j, nb = C + j;
     const int nchunks = 1 << j;
@@ -301,6 +438,7 @@ __global__ void __launch_bounds__(kPassThreads) pass_kernel(const PassArgs a) {
     const int per_lane = ncomp >> 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int blk_shift = a.B - C;
+    const int swm = swizzle_mask<R>(C);
 
     T *tile = reinterpret_cast<T *>(smem);
     uint32_t *stage_all = reinterpret_cast<uint32_t *>(smem + (sizeof(T) << nb));
@@ -314,7 +452,7 @@ __global__ void __launch_bounds__(kPassThreads) pass_kernel(const PassArgs a) {
     unsigned long long rd = 0, wr = 0, ntiles = 0;
 
     for (uint64_t tile_id = blockIdx.x; tile_id < a.n_tiles; tile_id += gridDim.x) {
-        const uint64_t chunk_base = insert_zero_bits(tile_id, a.tq, j);
+        const uint64_t chunk_base = insert_zero_bits(tile_id, s_tq, j);
         const uint64_t block0 = chunk_base >> blk_shift;
         if (!a.group_active[a.block_to_group[block0]]) continue;  // uniform in the CTA
         if (threadIdx.x == 0) s_flag = *reinterpret_cast<volatile int32_t *>(a.error);
@@ -324,7 +462,7 @@ __global__ void __launch_bounds__(kPassThreads) pass_kernel(const PassArgs a) {
 
         // ---- decode
         for (int c = warp; c < nchunks; c += nwarps) {
-            const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, a.tq, j);
+            const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
             const uint64_t blk = chunk >> blk_shift;
             R *comp = reinterpret_cast<R *>(tile) + (size_t)c * ncomp;
             if (a.first_pass && !a.mask[blk]) {
@@ -332,17 +470,15 @@ __global__ void __launch_bounds__(kPassThreads) pass_kernel(const PassArgs a) {
                 continue;
             }
             const ChunkMeta md = a.meta_in[chunk];
-            decode_chunk<R>(a.arena_in, md, per_lane, a.codec, comp, wstage, lane);
+            decode_chunk<R>(a.arena_in, md, per_lane, a.codec, reinterpret_cast<R *>(tile), wstage, lane,
+                            TileSlot<R>{c << C, swm});
             if (lane == 0) rd += payload_bytes(C, md.width) + sizeof(ChunkMeta);
         }
         __syncthreads();
 
         // ---- gates
         const uint64_t base_amp = chunk_base << C;
-        for (int k = 0; k < a.ngates; ++k) {
-            tile_apply_gate<R>(tile, nb, a.gates[k], base_amp);
-            __syncthreads();
-        }
+        tile_sweeps<R>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool), base_amp);
 
         // ---- quantise (codes replace values in shared memory)
         for (int c = warp; c < nchunks; c += nwarps) {
@@ -350,7 +486,8 @@ __global__ void __launch_bounds__(kPassThreads) pass_kernel(const PassArgs a) {
             int32_t base;
             uint32_t width;
             bool nz;
-            quantize_chunk<R>(comp, per_lane, a.codec, a.exact_zero != 0, lane, &base, &width, &nz);
+            quantize_chunk<R>(reinterpret_cast<R *>(tile), per_lane, a.codec, a.exact_zero != 0, lane, &base,
+                              &width, &nz, TileSlot<R>{c << C, swm}, reinterpret_cast<int32_t *>(comp));
             if (lane == 0) {
                 s_base[c] = base;
                 s_width[c] = width;
@@ -381,7 +518,7 @@ __global__ void __launch_bounds__(kPassThreads) pass_kernel(const PassArgs a) {
 
         // ---- pack and store
         for (int c = warp; c < nchunks; c += nwarps) {
-            const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, a.tq, j);
+            const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
             const int32_t *codes = reinterpret_cast<const int32_t *>(reinterpret_cast<R *>(tile) + (size_t)c * ncomp);
             const unsigned long long off = s_tile_off + s_off[c];
             const uint32_t w = s_width[c];
@@ -410,7 +547,7 @@ __global__ void __launch_bounds__(kPassThreads) pass_kernel(const PassArgs a) {
 
 // ------------------------------------------------------------ dense pass
 template <typename R>
-__global__ void __launch_bounds__(kPassThreads) dense_pass_kernel(const DensePassArgs a) {
+__global__ void __launch_bounds__(kPassThreads, 2) dense_pass_kernel(const DensePassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem[];
     T *tile = reinterpret_cast<T *>(smem);
@@ -418,21 +555,22 @@ __global__ void __launch_bounds__(kPassThreads) dense_pass_kernel(const DensePas
     const int C = a.C, j = a.j, nb = C + j;
     const int size = 1 << nb;
     const int cmask = (1 << C) - 1;
+    const int swm = swizzle_mask<R>(C);
+    __shared__ int32_t s_tq[kMaxTileQubits];
+    if (threadIdx.x < kMaxTileQubits) s_tq[threadIdx.x] = a.tq[threadIdx.x];
+    __syncthreads();
     for (uint64_t tile_id = blockIdx.x; tile_id < a.n_tiles; tile_id += gridDim.x) {
-        const uint64_t chunk_base = insert_zero_bits(tile_id, a.tq, j);
+        const uint64_t chunk_base = insert_zero_bits(tile_id, s_tq, j);
         for (int e = threadIdx.x; e < size; e += blockDim.x) {
-            const uint64_t amp = ((chunk_base | deposit_bits((uint32_t)(e >> C), a.tq, j)) << C) | (uint64_t)(e & cmask);
-            tile[e] = st[amp];
+            const uint64_t amp = ((chunk_base | deposit_bits((uint32_t)(e >> C), s_tq, j)) << C) | (uint64_t)(e & cmask);
+            tile[swz<R>(e, swm)] = st[amp];
         }
         __syncthreads();
-        const uint64_t base_amp = chunk_base << C;
-        for (int k = 0; k < a.ngates; ++k) {
-            tile_apply_gate<R>(tile, nb, a.gates[k], base_amp);
-            __syncthreads();
-        }
+        tile_sweeps<R>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool),
+                       chunk_base << C);
         for (int e = threadIdx.x; e < size; e += blockDim.x) {
-            const uint64_t amp = ((chunk_base | deposit_bits((uint32_t)(e >> C), a.tq, j)) << C) | (uint64_t)(e & cmask);
-            st[amp] = tile[e];
+            const uint64_t amp = ((chunk_base | deposit_bits((uint32_t)(e >> C), s_tq, j)) << C) | (uint64_t)(e & cmask);
+            st[amp] = tile[swz<R>(e, swm)];
         }
         __syncthreads();
     }

@@ -264,9 +264,9 @@ class CompressedQuantumState:
 
     Error bounds come from BITCOMP_REL_EB (default 1e-3) and BITCOMP_ABS_EB
     (default 1e-7) at construction, as in the reference.  QOMPSIM_DTYPE picks
-    complex128 (default) or complex64.  QOMPSIM_ZERO_TEST=code switches the
-    zero-block test to quantised codes; QOMPSIM_REFERENCE_CONTROLS=1
-    reproduces the reference's control handling."""
+    complex128 (default) or complex64.  QOMPSIM_ZERO_TEST=exact selects the
+    reference GPU build's exact zero-block test (default: all codes zero);
+    QOMPSIM_REFERENCE_CONTROLS=1 reproduces the reference's control handling."""
 
     def __init__(self, qubit_count: int, block_size: int, dtype=None, eps_rel: Optional[float] = None,
                  eps_abs: Optional[float] = None, flags: Optional[int] = None):
@@ -278,8 +278,8 @@ class CompressedQuantumState:
         self._eps_abs = _env_float("BITCOMP_ABS_EB", 1e-7) if eps_abs is None else float(eps_abs)
         if flags is None:
             flags = 0
-            if os.environ.get("QOMPSIM_ZERO_TEST", "exact") == "code":
-                flags |= _n.QS_FLAG_CODE_ZERO_TEST
+            if os.environ.get("QOMPSIM_ZERO_TEST", "code") == "exact":
+                flags |= _n.QS_FLAG_EXACT_ZERO_TEST
             if os.environ.get("QOMPSIM_REFERENCE_CONTROLS", "0") == "1":
                 flags |= _n.QS_FLAG_REFERENCE_CONTROLS
             if os.environ.get("QOMPSIM_QUIET", "0") == "1":

@@ -30,7 +30,7 @@ QS_ERR_NOMEM = 8
 QS_COMPLEX128 = 0
 QS_COMPLEX64 = 1
 
-QS_FLAG_CODE_ZERO_TEST = 0x1
+QS_FLAG_EXACT_ZERO_TEST = 0x1
 QS_FLAG_REFERENCE_CONTROLS = 0x2
 QS_FLAG_QUIET = 0x4
 QS_FLAG_PROFILE = 0x8

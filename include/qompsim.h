@@ -50,9 +50,13 @@ typedef enum qs_dtype {
 } qs_dtype;
 
 /* Flags of qs_create. */
-#define QS_FLAG_CODE_ZERO_TEST 0x1u  /* a previously-zero block stays zero when all of its
-                                        quantised codes are 0, instead of the reference's
-                                        exact |a|^2 != 0 test (cuda_complex_helper.cuh:96-106) */
+#define QS_FLAG_EXACT_ZERO_TEST 0x1u /* the reference GPU build's exact |a|^2 != 0 test
+                                        (cuda_complex_helper.cuh:96-106) for blocks that were
+                                        zero before a stage.  Default: the block stays zero
+                                        when every amplitude quantises to code 0, i.e. |re|,
+                                        |im| <= 2^-(L+1) -- the CPU build's threshold test
+                                        (compressed_state.hpp:939-951) at the codec's
+                                        resolution, immune to FMA rounding residues */
 #define QS_FLAG_REFERENCE_CONTROLS 0x2u /* reproduce the reference dispatch: controls are
                                         honoured for "CNOT" only and 2x2 / 4x4 matrices are
                                         applied uncontrolled, 4x4 bit0 on the lower target

@@ -13,8 +13,9 @@ apply_1q_gate (:1066-1144), apply_cnot (:1146-1264), apply_2q_gate
 * every block of an active group is processed, zero blocks as zeros (Q8);
 * after the gates only blocks that were zero before the stage are tested
   (Q1): `zero_test` selects the GPU build's exact test
-  (cuda_complex_helper.cuh:96-106), "code" (all quantised codes 0) or a
-  threshold (the CPU build's ALL_ZERO_THRESHOLD, :939-951);
+  (cuda_complex_helper.cuh:96-106), ("code", L) -- every component
+  quantises to code 0, |x| <= 2^-(L+1) -- or a float threshold (the CPU
+  build's ALL_ZERO_THRESHOLD, :939-951);
 * then every processed block goes through `codec` (a function on complex128
   arrays) -- the lossy round trip of compression.
 
@@ -224,8 +225,10 @@ class CompressedOracle:
     def _is_zero(self, v: np.ndarray) -> bool:
         if self.zero_test == "exact":
             return not np.any((v.real * v.real + v.imag * v.imag) != 0.0)
-        if self.zero_test == "code":
-            return not np.any(self.codec(v) != 0)
+        if isinstance(self.zero_test, tuple) and self.zero_test[0] == "code":
+            # every component quantises to code 0: rint(|x| 2^L) == 0
+            thr = 2.0 ** -(self.zero_test[1] + 1)
+            return not np.any((np.abs(v.real) > thr) | (np.abs(v.imag) > thr))
         return not np.any((np.abs(v.real) > self.zero_test) | (np.abs(v.imag) > self.zero_test))
 
     def apply(self, gates: Sequence, stages: Sequence[Sequence[int]], maps, counts) -> None:
