@@ -277,6 +277,92 @@ void build_ops(const std::vector<qs::KGate> &kg, size_t g0, const std::vector<qs
     }
 }
 
+// Merge runs of diagonal ops: a SCALAR or D2 op followed by SCALAR / D2 ops
+// on the same register bit becomes one D2 (or SCALAR) op whose variants
+// range over the union of the selector bits (at most kMaxSel).  The merged
+// op's variant v multiplies the factors of every member at its own variant
+// (v restricted to the member's selector bits).  Applied per sweep.
+void merge_diagonal_ops(const std::vector<qs::Sweep> &sweeps, size_t op0, std::vector<qs::ROp> *ops,
+                        std::vector<cplx> *pool, std::vector<qs::Sweep> *out_sweeps) {
+    std::vector<qs::ROp> out;
+    std::vector<cplx> outpool;
+    out_sweeps->clear();
+    for (const auto &sw : sweeps) {
+        qs::Sweep ns = sw;
+        ns.g0 = (int32_t)out.size();
+        size_t i = op0 + sw.g0;
+        const size_t end = op0 + sw.g1;
+        while (i < end) {
+            const qs::ROp &a = (*ops)[i];
+            auto is_diag1 = [](const qs::ROp &o) { return o.kind == qs::OP_SCALAR || o.kind == qs::OP_D2; };
+            if (!is_diag1(a)) {
+                qs::ROp c = a;
+                c.mat = (uint32_t)outpool.size();
+                const int nvar = 1 << a.nsel;
+                for (int v = 0; v < nvar; ++v)
+                    for (uint32_t e = 0; e < a.vstride; ++e) outpool.push_back((*pool)[a.mat + v * a.vstride + e]);
+                out.push_back(c);
+                ++i;
+                continue;
+            }
+            // grow a run [i, j) of diagonal ops on one register bit (or scalars)
+            int k = a.kind == qs::OP_D2 ? a.k0 : -1;
+            std::vector<int> sels(a.sel, a.sel + a.nsel);
+            size_t j = i + 1;
+            while (j < end && is_diag1((*ops)[j])) {
+                const qs::ROp &b = (*ops)[j];
+                if (b.kind == qs::OP_D2 && k >= 0 && b.k0 != k) break;
+                std::vector<int> u = sels;
+                for (int t = 0; t < b.nsel; ++t)
+                    if (std::find(u.begin(), u.end(), (int)b.sel[t]) == u.end()) u.push_back(b.sel[t]);
+                if ((int)u.size() > qs::kMaxSel) break;
+                sels = u;
+                if (b.kind == qs::OP_D2) k = b.k0;
+                ++j;
+            }
+            qs::ROp m{};
+            m.kind = k >= 0 ? qs::OP_D2 : qs::OP_SCALAR;
+            m.k0 = (uint8_t)(k >= 0 ? k : 0);
+            m.nsel = (uint8_t)sels.size();
+            for (size_t t = 0; t < sels.size(); ++t) m.sel[t] = (uint8_t)sels[t];
+            m.vstride = k >= 0 ? 2 : 1;
+            m.mat = (uint32_t)outpool.size();
+            const int nvar = 1 << sels.size();
+            for (int v = 0; v < nvar; ++v) {
+                cplx f0 = 1.0, f1 = 1.0;
+                for (size_t t = i; t < j; ++t) {
+                    const qs::ROp &b = (*ops)[t];
+                    int bv = 0;
+                    for (int q = 0; q < b.nsel; ++q) {
+                        const int pos = (int)(std::find(sels.begin(), sels.end(), (int)b.sel[q]) - sels.begin());
+                        bv |= ((v >> pos) & 1) << q;
+                    }
+                    if (b.kind == qs::OP_SCALAR) {
+                        const cplx z = (*pool)[b.mat + bv];
+                        f0 *= z;
+                        f1 *= z;
+                    } else {
+                        f0 *= (*pool)[b.mat + 2 * bv];
+                        f1 *= (*pool)[b.mat + 2 * bv + 1];
+                    }
+                }
+                outpool.push_back(f0);
+                if (k >= 0) outpool.push_back(f1);
+            }
+            out.push_back(m);
+            i = j;
+        }
+        ns.g1 = (int32_t)out.size();
+        out_sweeps->push_back(ns);
+    }
+    // replace this pass's ops [op0, ...) and pool suffix
+    ops->resize(op0);
+    const uint32_t pbase = (uint32_t)pool->size();
+    for (auto &o : out) o.mat += pbase;
+    ops->insert(ops->end(), out.begin(), out.end());
+    pool->insert(pool->end(), outpool.begin(), outpool.end());
+}
+
 template <typename Real>
 std::vector<Real> pool_as(const std::vector<cplx> &pool) {
     std::vector<Real> out(2 * pool.size());
@@ -379,6 +465,7 @@ struct qs_state {
         int32_t tq[qs::kMaxTileQubits];
         uint32_t gate_off, ngates;
         uint32_t sweep_off, nsweeps;
+        uint32_t op_off;
         bool first, final;
     };
     qs::Sweep *sweeps_dev = nullptr;
@@ -686,7 +773,12 @@ static qs_status build_device_plan(qs_state *h) {
             dp.final = p + 1 == pl.size();
             for (uint32_t gi : pl[p].gates) kg.push_back(to_kgate(h->cgates[gi], pl[p].tile, C));
             auto swp = plan_sweeps(kg, dp.gate_off, kg.size(), C + dp.j, RB);
+            const size_t op0 = ops.size();
             build_ops(kg, dp.gate_off, swp, RB, &ops, &pool);
+            std::vector<qs::Sweep> merged;
+            merge_diagonal_ops(swp, op0, &ops, &pool, &merged);
+            swp.swap(merged);
+            dp.op_off = (uint32_t)op0;
             dp.sweep_off = (uint32_t)sw.size();
             dp.nsweeps = (uint32_t)swp.size();
             sw.insert(sw.end(), swp.begin(), swp.end());
@@ -875,7 +967,7 @@ qs_status qs_apply_circuit(qs_state *h) {
             a.j = dp.j;
             for (int k = 0; k < dp.j; ++k) a.tq[k] = dp.tq[k];
             a.n_tiles = uint64_t(1) << (h->n - C - dp.j);
-            a.ops = h->ops_dev + dp.gate_off;
+            a.ops = h->ops_dev + dp.op_off;
             a.pool = h->pool_dev;
             a.sweeps = h->sweeps_dev + dp.sweep_off;
             a.nsweeps = (int)dp.nsweeps;
@@ -1301,6 +1393,7 @@ qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) 
     std::vector<qs::ROp> ops;
     std::vector<cplx> pool;
     std::vector<std::pair<size_t, size_t>> sweep_ranges;
+    std::vector<size_t> op_offsets;
     for (auto &p : pl) {
         // a tile must hold at least the RB register bits
         std::set<int> t(p.tile.begin(), p.tile.end());
@@ -1309,7 +1402,12 @@ qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) 
         const size_t g0 = kg.size();
         for (uint32_t gi : p.gates) kg.push_back(to_kgate(cg[gi], p.tile, C));
         auto swp = plan_sweeps(kg, g0, kg.size(), C + (int)p.tile.size(), RB);
+        const size_t op0 = ops.size();
         build_ops(kg, g0, swp, RB, &ops, &pool);
+        std::vector<qs::Sweep> merged;
+        merge_diagonal_ops(swp, op0, &ops, &pool, &merged);
+        swp.swap(merged);
+        op_offsets.push_back(op0);
         sweep_ranges.push_back({sw.size(), swp.size()});
         sw.insert(sw.end(), swp.begin(), swp.end());
     }
@@ -1355,7 +1453,7 @@ qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) 
         a.j = (int)p.tile.size();
         for (int k = 0; k < a.j; ++k) a.tq[k] = p.tile[k] - C;
         a.n_tiles = uint64_t(1) << (h->n - C - a.j);
-        a.ops = h->ops + off;
+        a.ops = h->ops + op_offsets[pi];
         a.pool = h->pool;
         a.sweeps = h->sw + sweep_ranges[pi].first;
         a.nsweeps = (int)sweep_ranges[pi].second;

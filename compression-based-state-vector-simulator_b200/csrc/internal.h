@@ -60,12 +60,12 @@ struct Sweep {
 // sel[j] < 64 is a tile bit (its value comes from the group), sel[j] >= 64 is
 // qubit sel[j]-64 outside the tile (its value comes from the tile).
 enum : uint8_t { OP_SCALAR = 0, OP_D2 = 1, OP_M2 = 2, OP_D4 = 3, OP_M4 = 4 };
+constexpr int kMaxSel = 4;
 struct ROp {
     uint8_t kind;
     uint8_t k0, k1;      // register bits; for D4/M4 k0 <-> matrix bit 0
-    uint8_t nsel;
-    uint8_t sel[2];
-    uint8_t pad[2];
+    uint8_t nsel;        // 0..kMaxSel selector bits
+    uint8_t sel[kMaxSel];
     uint32_t mat;        // pool index of variant 0 (complex entries)
     uint32_t vstride;    // complex entries per variant: 1, 2, 4 or 16
 };

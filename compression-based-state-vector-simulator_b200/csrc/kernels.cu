@@ -274,13 +274,19 @@ __device__ void tile_sweeps(typename Cplx<R>::T *tile, int nb, int swm, const Sw
             for (int s = 0; s < NS; ++s) v[s] = tile[swz<R>(base | off[s], swm)];
             Pending<RB, T> pend;
             pend.reset();
+            ROp nxt{};
+            if (sw.g0 < sw.g1) nxt = ops[sw.g0];
             for (int k = sw.g0; k < sw.g1; ++k) {
-                const ROp o = ops[k];
+                const ROp o = nxt;
+                if (k + 1 < sw.g1) nxt = ops[k + 1];
                 int var = 0;
-                for (int jj = 0; jj < o.nsel; ++jj) {
-                    const int src = o.sel[jj];
-                    const int bit = src < 64 ? (base >> src) & 1 : (int)((base_amp >> (src - 64)) & 1);
-                    var |= bit << jj;
+#pragma unroll
+                for (int jj = 0; jj < kMaxSel; ++jj) {
+                    if (jj < o.nsel) {
+                        const int src = o.sel[jj];
+                        const int bit = src < 64 ? (base >> src) & 1 : (int)((base_amp >> (src - 64)) & 1);
+                        var |= bit << jj;
+                    }
                 }
                 const T *m = pool + o.mat + (uint32_t)var * o.vstride;
                 switch (o.kind) {
