@@ -1572,4 +1572,33 @@ qs_status qs_codec_test(qs_dtype dtype, double eps_rel, double eps_abs, uint32_t
     return QS_OK;
 }
 
+// Allocation-free codec round trip (see qompsim.h): device pointers in and
+// out, scratch in a file-scope device array, no cudaMalloc / cudaFree.
+qs_status qs_codec_roundtrip_noalloc(qs_dtype dtype, double eps_rel, double eps_abs, uint32_t chunk_log2,
+                                     const void *d_vals, uint64_t nchunks, int32_t *d_bases, uint32_t *d_widths,
+                                     void *d_decoded, void *stream) {
+    qs::CodecParams p;
+    if (dtype != QS_COMPLEX128 && dtype != QS_COMPLEX64) return dfail(nullptr, QS_ERR_ARG, "unknown dtype");
+    const bool f64 = dtype == QS_COMPLEX128;
+    if (!qs::codec_params(f64, eps_rel, eps_abs, &p))
+        return dfail(nullptr, QS_ERR_ARG, "eps_rel must lie in [2^-24, 1)");
+    if (chunk_log2 < (uint32_t)qs::kMinChunkLog2 || chunk_log2 > (uint32_t)qs::kMaxChunkLog2)
+        return dfail(nullptr, QS_ERR_ARG, "chunk_log2 must lie in [4, 8]");
+    if (nchunks == 0) return QS_OK;
+    if (!d_vals || !d_bases || !d_widths || !d_decoded) return dfail(nullptr, QS_ERR_ARG, "NULL device pointer");
+    const uint64_t words_per_chunk = uint64_t(2) << chunk_log2;
+    const uint64_t cap = qs::noalloc_scratch_words();
+    if (nchunks > cap / words_per_chunk)
+        return dfail(nullptr, QS_ERR_ARG,
+                     "qs_codec_roundtrip_noalloc: " + std::to_string(nchunks) + " chunks of 2^" +
+                         std::to_string(chunk_log2) + " amplitudes exceed its fixed scratch of " +
+                         std::to_string(cap * 4) + " bytes (at most " + std::to_string(cap / words_per_chunk) +
+                         " chunks per call)");
+    cudaError_t e = qs::launch_codec_roundtrip_noalloc(f64, d_vals, (int)chunk_log2, p, nchunks, d_bases, d_widths,
+                                                       d_decoded, (cudaStream_t)stream);
+    if (e != cudaSuccess)
+        return dfail(nullptr, QS_ERR_CUDA, std::string("qs_codec_roundtrip_noalloc: ") + cudaGetErrorString(e));
+    return QS_OK;
+}
+
 }  // extern "C"

@@ -154,6 +154,12 @@ cudaError_t launch_codec_test(bool f64, const void *vals, int C, CodecParams cod
                               uint32_t *words, int32_t *bases, uint32_t *widths, void *decoded,
                               cudaStream_t stream);
 
+// Allocation-free variant of launch_codec_test: the packed words live in a
+// file-scope device array of noalloc_scratch_words() words.
+cudaError_t launch_codec_roundtrip_noalloc(bool f64, const void *vals, int C, CodecParams codec, uint64_t nchunks,
+                                           int32_t *bases, uint32_t *widths, void *decoded, cudaStream_t stream);
+uint64_t noalloc_scratch_words();
+
 int sm_count();
 
 }  // namespace qs

@@ -16,6 +16,7 @@
 // and writes the packed chunks back with coalesced stores.
 #include <cstdio>
 #include <climits>
+#include <mutex>
 
 #include "codec.cuh"
 #include "internal.h"
@@ -838,6 +839,12 @@ __global__ void from_c128_kernel(const double *in, uint64_t ncomp, R *s) {
 
 int g_sm_count = 0;
 
+// Scratch of the allocation-free codec round trip (qs_codec_roundtrip_noalloc):
+// the packed words between encode and decode.  Every GPU that loads the
+// library holds these 4 MiB until the process exits.
+constexpr uint64_t kNoAllocScratchWords = uint64_t(1) << 20;
+static __device__ __align__(256) uint32_t g_noalloc_words[kNoAllocScratchWords];
+
 unsigned grid_for(uint64_t work, unsigned per_block, unsigned cap_per_sm = 8) {
     const uint64_t need = (work + per_block - 1) / per_block;
     const uint64_t cap = (uint64_t)sm_count() * cap_per_sm;
@@ -964,6 +971,40 @@ cudaError_t launch_encode(bool f64, const double *vals, int B, int C, CodecParam
 
 cudaError_t launch_codec_test(bool f64, const void *vals, int C, CodecParams p, uint64_t nchunks, uint32_t *words,
                               int32_t *bases, uint32_t *widths, void *decoded, cudaStream_t s) {
+    const unsigned grid = grid_for(nchunks, kPassThreads / 32, 8);
+    if (f64)
+        codec_test_kernel<double><<<grid, kPassThreads, 0, s>>>((const double *)vals, C, p, nchunks, words, bases,
+                                                               widths, (double *)decoded);
+    else
+        codec_test_kernel<float><<<grid, kPassThreads, 0, s>>>((const float *)vals, C, p, nchunks, words, bases, widths,
+                                                              (float *)decoded);
+    return cudaGetLastError();
+}
+
+uint64_t noalloc_scratch_words() { return kNoAllocScratchWords; }
+
+// Host code may not use g_noalloc_words directly: in host code the name is a
+// host-side stand-in, not a device address.  The device address is looked up
+// once per device, with that device current, and cached.
+cudaError_t launch_codec_roundtrip_noalloc(bool f64, const void *vals, int C, CodecParams p, uint64_t nchunks,
+                                           int32_t *bases, uint32_t *widths, void *decoded, cudaStream_t s) {
+    static std::mutex mu;
+    static void *addr[64] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    uint32_t *words = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (addr[dev] == nullptr) {
+            void *ptr = nullptr;
+            e = cudaGetSymbolAddress(&ptr, g_noalloc_words);
+            if (e != cudaSuccess) return e;
+            addr[dev] = ptr;
+        }
+        words = static_cast<uint32_t *>(addr[dev]);
+    }
     const unsigned grid = grid_for(nchunks, kPassThreads / 32, 8);
     if (f64)
         codec_test_kernel<double><<<grid, kPassThreads, 0, s>>>((const double *)vals, C, p, nchunks, words, bases,

@@ -118,6 +118,7 @@ SIGNATURES = [
     ("qs_codec_params", ct.c_int, [ct.c_int, _D, _D, ct.POINTER(_I32), ct.POINTER(_I32)]),
     ("qs_codec_test", ct.c_int, [ct.c_int, _D, _D, _U32, _P, _U64, ct.POINTER(_U32),
                                  ct.POINTER(_I32), ct.POINTER(_U32), _P]),
+    ("qs_codec_roundtrip_noalloc", ct.c_int, [ct.c_int, _D, _D, _U32, _P, _U64, _P, _P, _P, _P]),
 ]
 
 _lib = None

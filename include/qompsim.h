@@ -245,6 +245,32 @@ qs_status qs_codec_test(qs_dtype dtype, double eps_rel, double eps_abs, uint32_t
                         const void *vals, uint64_t nchunks, uint32_t *words, int32_t *bases,
                         uint32_t *widths, void *decoded);
 
+/* Allocation-free variant of qs_codec_test, for callers that cannot call
+ * cudaMalloc: code that runs inside another framework's memory pool, that
+ * has reserved all device memory up front, or that must not allocate (an
+ * allocation may synchronise the device) in the middle of a running
+ * pipeline.  No counterpart in the reference.
+ *
+ * All pointers are DEVICE pointers owned by the caller: d_vals holds
+ * nchunks * 2^(chunk_log2+1) values of the dtype (interleaved re, im);
+ * d_bases / d_widths receive each chunk's frame of reference and d_decoded the
+ * round-tripped values, exactly as qs_codec_test returns them.  The packed
+ * words between encode and decode live in a file-scope device array of
+ * 4 MiB that every GPU loading the library holds until the process exits;
+ * a call may cover at most 2^20 / 2^(chunk_log2+1) chunks (larger calls
+ * return QS_ERR_ARG, nothing is launched).  The call allocates nothing,
+ * enqueues one kernel on `stream` (a cudaStream_t, NULL = default stream)
+ * and does not synchronise.  Its first call on a device looks up the
+ * array's device address (once per device, with that device current), so
+ * make that first call before any stream capture.  Every call shares the
+ * one array: calls that overlap on the GPU (different streams, no ordering
+ * between them) race on it.  Nothing in the array needs to start at zero;
+ * it keeps the last call's words.  Errors are reported through
+ * qs_dense_last_error(NULL). */
+qs_status qs_codec_roundtrip_noalloc(qs_dtype dtype, double eps_rel, double eps_abs, uint32_t chunk_log2,
+                                     const void *d_vals, uint64_t nchunks, int32_t *d_bases,
+                                     uint32_t *d_widths, void *d_decoded, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
