@@ -67,9 +67,13 @@ __host__ __device__ inline int32_t quantize(float x, CodecParams p) {
     if (abits < thr) {
         float a;
 #ifdef __CUDA_ARCH__
+        // rint(a * 2^L) without a conversion instruction: a * 2^L < 2^23 here,
+        // so fma(a, 2^L, 2^23) rounds it to an integer (nearest, ties to even)
+        // in the low mantissa bits.
         a = __uint_as_float(abits);
         const float scale = __uint_as_float(uint32_t(p.L + 127) << 23);  // 2^L exactly
-        c = (int64_t)__float2ll_rn(__fmul_rn(a, scale));
+        const float r = __fmaf_rn(a, scale, 8388608.0f);
+        c = (int64_t)(__float_as_uint(r) - 0x4b000000u);
 #else
         std::memcpy(&a, &abits, 4);
         c = (int64_t)std::nearbyint(a * std::ldexp(1.0f, p.L));
@@ -89,8 +93,10 @@ __host__ __device__ inline float dequantize_f32(int32_t q, CodecParams p) {
     float a;
     if (c <= (int64_t(1) << p.m)) {
 #ifdef __CUDA_ARCH__
+        // (float)c for c <= 2^23 without a conversion instruction
         const float iscale = __uint_as_float(uint32_t(127 - p.L) << 23);  // 2^-L exactly
-        a = __fmul_rn((float)c, iscale);
+        const float cf = __uint_as_float(0x4b000000u + (uint32_t)c) - 8388608.0f;
+        a = __fmul_rn(cf, iscale);
 #else
         a = (float)c * std::ldexp(1.0f, -p.L);
 #endif
@@ -124,9 +130,11 @@ __host__ __device__ inline int32_t quantize(double x, CodecParams p) {
     if (abits < thr) {
         double a;
 #ifdef __CUDA_ARCH__
+        // rint(a * 2^L) via fma(a, 2^L, 2^52): exact integer in the low bits
         a = __longlong_as_double((long long)abits);
         const double scale = __longlong_as_double((long long)(uint64_t(p.L + 1023) << 52));
-        c = (int64_t)__double2ll_rn(__dmul_rn(a, scale));
+        const double r = __fma_rn(a, scale, 4503599627370496.0);
+        c = (int64_t)((uint64_t)__double_as_longlong(r) - 0x4330000000000000ull);
 #else
         std::memcpy(&a, &abits, 8);
         c = (int64_t)std::nearbyint(a * std::ldexp(1.0, p.L));
@@ -146,8 +154,10 @@ __host__ __device__ inline double dequantize_f64(int32_t q, CodecParams p) {
     double a;
     if (c <= (int64_t(1) << p.m)) {
 #ifdef __CUDA_ARCH__
+        // (double)c for c <= 2^24 without a conversion instruction
         const double iscale = __longlong_as_double((long long)(uint64_t(1023 - p.L) << 52));
-        a = __dmul_rn((double)c, iscale);
+        const double cf = __longlong_as_double((long long)(0x4330000000000000ull + (uint64_t)c)) - 4503599627370496.0;
+        a = __dmul_rn(cf, iscale);
 #else
         a = (double)c * std::ldexp(1.0, -p.L);
 #endif

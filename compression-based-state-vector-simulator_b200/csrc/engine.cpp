@@ -466,6 +466,7 @@ struct qs_state {
         uint32_t gate_off, ngates;
         uint32_t sweep_off, nsweeps;
         uint32_t op_off;
+        int rb;
         bool first, final;
     };
     qs::Sweep *sweeps_dev = nullptr;
@@ -750,12 +751,12 @@ static void make_block_groups(qs_state *h) {
 static qs_status build_device_plan(qs_state *h) {
     const int C = (int)h->C;
     const int jmax = std::min(h->tile_log2 - C, qs::kMaxTileQubits);
-    const int jmin = std::min(3, jmax);
+    const int RBmain = h->f64 ? qs::kRegBitsF64 : qs::kRegBitsF32;
+    const int jmin = std::min(jmax, std::max(3, RBmain - C));
     std::vector<qs::KGate> kg;
     std::vector<qs::Sweep> sw;
     std::vector<qs::ROp> ops;
     std::vector<cplx> pool;
-    const int RB = h->f64 ? qs::kRegBitsF64 : qs::kRegBitsF32;
     h->passes.clear();
     for (uint32_t s = 0; s < h->stages.size(); ++s) {
         for (uint32_t gi : h->stages[s])
@@ -772,6 +773,8 @@ static qs_status build_device_plan(qs_state *h) {
             dp.first = p == 0;
             dp.final = p + 1 == pl.size();
             for (uint32_t gi : pl[p].gates) kg.push_back(to_kgate(h->cgates[gi], pl[p].tile, C));
+            const int RB = C + dp.j >= RBmain ? RBmain : 3;  // small tiles use 8-amplitude groups
+            dp.rb = RB;
             auto swp = plan_sweeps(kg, dp.gate_off, kg.size(), C + dp.j, RB);
             const size_t op0 = ops.size();
             build_ops(kg, dp.gate_off, swp, RB, &ops, &pool);
@@ -780,6 +783,12 @@ static qs_status build_device_plan(qs_state *h) {
             swp.swap(merged);
             dp.op_off = (uint32_t)op0;
             dp.sweep_off = (uint32_t)sw.size();
+            if (std::getenv("QOMPSIM_DEBUG_PLAN")) {
+                printf("stage %u pass %zu: j=%d gates=%u sweeps=%zu ops=%zu tile=[", s, p, dp.j, dp.ngates, swp.size(),
+                       ops.size() - op0);
+                for (int t : pl[p].tile) printf(" %d", t);
+                printf(" ]\n");
+            }
             dp.nsweeps = (uint32_t)swp.size();
             sw.insert(sw.end(), swp.begin(), swp.end());
             h->passes.push_back(dp);
@@ -819,6 +828,8 @@ static qs_status build_device_plan(qs_state *h) {
         uint32_t gmax = *std::max_element(h->num_groups.begin(), h->num_groups.end());
         if (gmax > h->nb) return fail(h, QS_ERR_ARG, "num_groups larger than the number of blocks");
     }
+    h->st.sweeps = sw.size();
+    h->st.ops = ops.size();
     h->history_cap = 2 * ns + 1;
     CUDA_TRY(h, cudaMalloc(&h->history_dev, h->history_cap * sizeof(unsigned long long)));
     for (auto e : h->pass_ev) cudaEventDestroy(e);
@@ -971,6 +982,7 @@ qs_status qs_apply_circuit(qs_state *h) {
             a.pool = h->pool_dev;
             a.sweeps = h->sweeps_dev + dp.sweep_off;
             a.nsweeps = (int)dp.nsweeps;
+            a.rb = dp.rb;
             a.codec = h->codec;
             a.meta_in = h->meta[h->cur];
             a.arena_in = h->arena[h->cur];
@@ -1383,8 +1395,8 @@ qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) 
     const int tl = env_int("QOMPSIM_DENSE_TILE_LOG2", h->f64 ? 12 : 13);
     const int tile_log2 = std::min<int>((int)h->n, std::min<int>(tl, C + qs::kMaxTileQubits));
     const int jmax = tile_log2 - C;
-    const int RB = h->f64 ? qs::kRegBitsF64 : qs::kRegBitsF32;
-    if ((int)h->n < RB) return qs_dense_apply_gates_pergate(h, gates, count);
+    const int RBmain = h->f64 ? qs::kRegBitsF64 : qs::kRegBitsF32;
+    if ((int)h->n < 3) return qs_dense_apply_gates_pergate(h, gates, count);
     std::vector<uint32_t> ids(count);
     for (size_t i = 0; i < count; ++i) ids[i] = (uint32_t)i;
     auto pl = plan_passes(ids, cg, C, jmax, std::min(jmax, 3), C, (int)h->n);
@@ -1394,11 +1406,14 @@ qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) 
     std::vector<cplx> pool;
     std::vector<std::pair<size_t, size_t>> sweep_ranges;
     std::vector<size_t> op_offsets;
+    std::vector<int> pass_rb;
     for (auto &p : pl) {
         // a tile must hold at least the RB register bits
         std::set<int> t(p.tile.begin(), p.tile.end());
-        for (int q = C; q < (int)h->n && C + (int)t.size() < RB; ++q) t.insert(q);
+        for (int q = C; q < (int)h->n && C + (int)t.size() < RBmain; ++q) t.insert(q);
         p.tile.assign(t.begin(), t.end());
+        const int RB = C + (int)t.size() >= RBmain ? RBmain : 3;
+        pass_rb.push_back(RB);
         const size_t g0 = kg.size();
         for (uint32_t gi : p.gates) kg.push_back(to_kgate(cg[gi], p.tile, C));
         auto swp = plan_sweeps(kg, g0, kg.size(), C + (int)p.tile.size(), RB);
@@ -1457,6 +1472,7 @@ qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) 
         a.pool = h->pool;
         a.sweeps = h->sw + sweep_ranges[pi].first;
         a.nsweeps = (int)sweep_ranges[pi].second;
+        a.rb = pass_rb[pi];
         a.state = h->state;
         off += p.gates.size();
         CUDA_TRY(h, qs::launch_dense_pass(h->f64, a, tile_log2, h->stream));

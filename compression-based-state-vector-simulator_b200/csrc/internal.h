@@ -49,10 +49,14 @@ struct KGate {
 // on any other bit is allowed).  RB = 3 for complex128, 4 for complex64.
 constexpr int kRegBitsF64 = 3;
 constexpr int kRegBitsF32 = 4;
+constexpr int kMaxRegBits = 5;
 struct Sweep {
     int32_t g0, g1;
-    int32_t sbits[4];
+    int32_t sbits[6];
 };
+// Threads of the fused pass kernels (compressed and dense): 4 warps, three
+// CTAs per SM, so that a thread can hold 2^RB amplitudes in registers.
+constexpr int kSweepThreads = 128;
 
 // A gate resolved against its sweep (host-built).  Register bits k0/k1 index
 // the sweep bits; the gate's other qubits are fixed for a register group and
@@ -86,6 +90,7 @@ struct PassArgs {
     const void *pool;                   // double2 (complex128) or float2 (complex64)
     const Sweep *sweeps;
     int32_t nsweeps;
+    int32_t rb;                         // register bits of the sweeps (3 or the dtype's RB)
     CodecParams codec;
     const ChunkMeta *meta_in;
     const uint32_t *arena_in;
@@ -112,6 +117,7 @@ struct DensePassArgs {
     const void *pool;
     const Sweep *sweeps;
     int32_t nsweeps;
+    int32_t rb;
     void *state;
 };
 

@@ -74,8 +74,8 @@ __device__ __forceinline__ uint64_t deposit_bits(uint32_t c, const int32_t *pos,
 // differ in any set of tile bits spreads over the banks.  m is limited to
 // bits below the chunk size, so an element never leaves its chunk's region.
 template <typename R> struct Layout;
-template <> struct Layout<double> { static constexpr int S1 = 3; static constexpr int RB = kRegBitsF64; };
-template <> struct Layout<float> { static constexpr int S1 = 4; static constexpr int RB = kRegBitsF32; };
+template <> struct Layout<double> { static constexpr int S1 = 3; };
+template <> struct Layout<float> { static constexpr int S1 = 4; };
 
 template <typename R>
 __host__ __device__ __forceinline__ int swizzle_mask(int C) {
@@ -169,7 +169,7 @@ __device__ __forceinline__ void pend_d2(Pending<RB, T> &p, int k, T a, T b) {
             p.d1[K] = cmul(p.d1[K], b);                  \
         }                                                \
         break;
-    switch (k) { QS_PD(0) QS_PD(1) QS_PD(2) QS_PD(3) default: break; }
+    switch (k) { QS_PD(0) QS_PD(1) QS_PD(2) QS_PD(3) QS_PD(4) default: break; }
 #undef QS_PD
 }
 
@@ -185,30 +185,26 @@ __device__ __forceinline__ void flush_bit(T (&v)[1 << RB], Pending<RB, T> &p, in
             }                                                             \
         }                                                                 \
         break;
-    switch (k) { QS_FB(0) QS_FB(1) QS_FB(2) QS_FB(3) default: break; }
+    switch (k) { QS_FB(0) QS_FB(1) QS_FB(2) QS_FB(3) QS_FB(4) default: break; }
 #undef QS_FB
 }
 
 template <int RB, typename T>
 __device__ __forceinline__ void flush_all(T (&v)[1 << RB], Pending<RB, T> &p) {
     constexpr int NS = 1 << RB;
-    bool any = !is_one(p.z);
-#pragma unroll
-    for (int k = 0; k < RB; ++k) any |= !is_one(p.d0[k]) || !is_one(p.d1[k]);
-    if (!any) return;
-    T f[NS];
-    f[0] = p.z;
-#pragma unroll
-    for (int k = 0; k < RB; ++k) {
-#pragma unroll
-        for (int s = 0; s < (1 << k); ++s) {
-            f[s | (1 << k)] = cmul(f[s], p.d1[k]);
-            f[s] = cmul(f[s], p.d0[k]);
-        }
+    if (!is_one(p.z)) {  // fold the scalar into bit 0
+        p.d0[0] = cmul(p.d0[0], p.z);
+        p.d1[0] = cmul(p.d1[0], p.z);
+        p.z = c_one<T>();
     }
 #pragma unroll
-    for (int s = 0; s < NS; ++s) v[s] = cmul(f[s], v[s]);
-    p.reset();
+    for (int k = 0; k < RB; ++k) {
+        if (!is_one(p.d0[k]) || !is_one(p.d1[k])) {
+#pragma unroll
+            for (int s = 0; s < NS; ++s) v[s] = cmul(((s >> k) & 1) ? p.d1[k] : p.d0[k], v[s]);
+            p.d0[k] = p.d1[k] = c_one<T>();
+        }
+    }
 }
 
 template <int RB, typename T>
@@ -218,7 +214,7 @@ __device__ __forceinline__ void d_m2(T (&v)[1 << RB], int k, const T *m) {
     case K:                                                       \
         if constexpr (K < RB) r_2x2<NS, K>(v, m[0], m[1], m[2], m[3]); \
         break;
-    switch (k) { QS_CASE2(0) QS_CASE2(1) QS_CASE2(2) QS_CASE2(3) default: break; }
+    switch (k) { QS_CASE2(0) QS_CASE2(1) QS_CASE2(2) QS_CASE2(3) QS_CASE2(4) default: break; }
 #undef QS_CASE2
 }
 
@@ -226,15 +222,17 @@ template <int RB, typename T>
 __device__ __forceinline__ void d_44(T (&v)[1 << RB], int ka, int kb, bool diag, const T *m) {
     constexpr int NS = 1 << RB;
 #define QS_CASE4(A, B)                                                            \
-    case (A) * 4 + (B):                                                           \
+    case (A) * 8 + (B):                                                           \
         if constexpr ((A) < RB && (B) < RB && (A) != (B)) {                       \
             if (diag) r_diag4<NS, A, B>(v, m[0], m[1], m[2], m[3]);               \
             else r_4x4<NS, A, B>(v, m);                                           \
         }                                                                         \
         break;
-    switch (ka * 4 + kb) {
-        QS_CASE4(0, 1) QS_CASE4(0, 2) QS_CASE4(0, 3) QS_CASE4(1, 0) QS_CASE4(1, 2) QS_CASE4(1, 3)
-        QS_CASE4(2, 0) QS_CASE4(2, 1) QS_CASE4(2, 3) QS_CASE4(3, 0) QS_CASE4(3, 1) QS_CASE4(3, 2)
+    switch (ka * 8 + kb) {
+        QS_CASE4(0, 1) QS_CASE4(0, 2) QS_CASE4(0, 3) QS_CASE4(0, 4) QS_CASE4(1, 0) QS_CASE4(1, 2)
+        QS_CASE4(1, 3) QS_CASE4(1, 4) QS_CASE4(2, 0) QS_CASE4(2, 1) QS_CASE4(2, 3) QS_CASE4(2, 4)
+        QS_CASE4(3, 0) QS_CASE4(3, 1) QS_CASE4(3, 2) QS_CASE4(3, 4) QS_CASE4(4, 0) QS_CASE4(4, 1)
+        QS_CASE4(4, 2) QS_CASE4(4, 3)
         default: break;
     }
 #undef QS_CASE4
@@ -242,12 +240,11 @@ __device__ __forceinline__ void d_44(T (&v)[1 << RB], int ka, int kb, bool diag,
 
 // Apply every sweep of a pass to a tile of 2^nb elements whose element 0 is
 // global amplitude base_amp.
-template <typename R>
+template <typename R, int RB>
 __device__ void tile_sweeps(typename Cplx<R>::T *tile, int nb, int swm, const Sweep *__restrict__ sweeps,
                             int nsweeps, const ROp *__restrict__ ops, const typename Cplx<R>::T *__restrict__ pool,
                             uint64_t base_amp) {
     using T = typename Cplx<R>::T;
-    constexpr int RB = Layout<R>::RB;
     constexpr int NS = 1 << RB;
     const int groups = 1 << (nb - RB);
     for (int w = 0; w < nsweeps; ++w) {
@@ -422,15 +419,15 @@ __device__ __forceinline__ size_t align_up(size_t x, size_t a) { return (x + a -
 
 size_t pass_smem_bytes(bool f64, int nb, int j) {
     const size_t tile = (f64 ? 16 : 8) << nb;
-    const size_t stage = (size_t)(kPassThreads / 32) * kMaxPerLane * 32 * 4;
+    const size_t stage = (size_t)(kSweepThreads / 32) * kMaxPerLane * 32 * 4;
     const size_t tables = ((size_t)3 * 4 << j) + 8;
     const size_t offs = (size_t)8 << j;
     return tile + stage + ((tables + 7) / 8) * 8 + offs;
 }
 
 // ------------------------------------------------------------ pass kernel
-template <typename R>
-__global__ void __launch_bounds__(kPassThreads, 2) pass_kernel(const PassArgs a) {
+template <typename R, int RB>
+__global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ unsigned long long s_tile_off;
@@ -485,7 +482,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) pass_kernel(const PassArgs a)
 
         // ---- gates
         const uint64_t base_amp = chunk_base << C;
-        tile_sweeps<R>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool), base_amp);
+        tile_sweeps<R, RB>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool), base_amp);
 
         // ---- quantise (codes replace values in shared memory)
         for (int c = warp; c < nchunks; c += nwarps) {
@@ -553,8 +550,8 @@ __global__ void __launch_bounds__(kPassThreads, 2) pass_kernel(const PassArgs a)
 }
 
 // ------------------------------------------------------------ dense pass
-template <typename R>
-__global__ void __launch_bounds__(kPassThreads, 2) dense_pass_kernel(const DensePassArgs a) {
+template <typename R, int RB>
+__global__ void __launch_bounds__(kSweepThreads, 3) dense_pass_kernel(const DensePassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem[];
     T *tile = reinterpret_cast<T *>(smem);
@@ -573,8 +570,8 @@ __global__ void __launch_bounds__(kPassThreads, 2) dense_pass_kernel(const Dense
             tile[swz<R>(e, swm)] = st[amp];
         }
         __syncthreads();
-        tile_sweeps<R>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool),
-                       chunk_base << C);
+        tile_sweeps<R, RB>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool),
+                           chunk_base << C);
         for (int e = threadIdx.x; e < size; e += blockDim.x) {
             const uint64_t amp = ((chunk_base | deposit_bits((uint32_t)(e >> C), s_tq, j)) << C) | (uint64_t)(e & cmask);
             st[amp] = tile[swz<R>(e, swm)];
@@ -865,46 +862,48 @@ int sm_count() {
     return g_sm_count;
 }
 
-template <typename R>
+template <typename R, int RB>
 static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
     const int nb = a.C + a.j;
     const size_t smem = pass_smem_bytes(sizeof(R) == 8, nb, a.j);
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<R>, kPassThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<R, RB>, kSweepThreads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t grid = (uint64_t)per_sm * sm_count();
     if (grid > a.n_tiles) grid = a.n_tiles;
     if (grid == 0) grid = 1;
-    pass_kernel<R><<<(unsigned)grid, kPassThreads, smem, s>>>(a);
+    pass_kernel<R, RB><<<(unsigned)grid, kSweepThreads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pass(bool f64, const PassArgs &a, int, cudaStream_t s) {
-    return f64 ? launch_pass_t<double>(a, s) : launch_pass_t<float>(a, s);
+    if (f64) return a.rb == kRegBitsF64 ? launch_pass_t<double, kRegBitsF64>(a, s) : launch_pass_t<double, 3>(a, s);
+    return a.rb == kRegBitsF32 ? launch_pass_t<float, kRegBitsF32>(a, s) : launch_pass_t<float, 3>(a, s);
 }
 
-template <typename R>
+template <typename R, int RB>
 static cudaError_t launch_dense_pass_t(const DensePassArgs &a, cudaStream_t s) {
     const int nb = a.C + a.j;
     const size_t smem = (size_t)(2 * sizeof(R)) << nb;
-    cudaError_t e = cudaFuncSetAttribute(dense_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(dense_pass_kernel<R, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense_pass_kernel<R>, kPassThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense_pass_kernel<R, RB>, kSweepThreads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t grid = (uint64_t)per_sm * sm_count();
     if (grid > a.n_tiles) grid = a.n_tiles;
     if (grid == 0) grid = 1;
-    dense_pass_kernel<R><<<(unsigned)grid, kPassThreads, smem, s>>>(a);
+    dense_pass_kernel<R, RB><<<(unsigned)grid, kSweepThreads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_dense_pass(bool f64, const DensePassArgs &a, int, cudaStream_t s) {
-    return f64 ? launch_dense_pass_t<double>(a, s) : launch_dense_pass_t<float>(a, s);
+    if (f64) return a.rb == kRegBitsF64 ? launch_dense_pass_t<double, kRegBitsF64>(a, s) : launch_dense_pass_t<double, 3>(a, s);
+    return a.rb == kRegBitsF32 ? launch_dense_pass_t<float, kRegBitsF32>(a, s) : launch_dense_pass_t<float, 3>(a, s);
 }
 
 cudaError_t launch_pergate(bool f64, void *state, int n, const KGate *g, cudaStream_t s) {

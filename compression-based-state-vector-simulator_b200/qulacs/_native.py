@@ -68,6 +68,8 @@ class qs_stats(ct.Structure):
         ("linear_exp", ct.c_int32),
         ("chunk_log2", ct.c_int32),
         ("tile_log2", ct.c_int32),
+        ("sweeps", ct.c_uint64),
+        ("ops", ct.c_uint64),
     ]
 
 

@@ -95,6 +95,8 @@ typedef struct qs_stats {
     int32_t linear_exp;          /* quantiser parameter L (absolute step 2^-L)          */
     int32_t chunk_log2;          /* amplitudes per chunk = 2^chunk_log2                 */
     int32_t tile_log2;           /* largest tile = 2^tile_log2 amplitudes               */
+    uint64_t sweeps;             /* register sweeps over all passes (plan)              */
+    uint64_t ops;                /* gate op records over all passes (plan)              */
 } qs_stats;
 
 /* ---------------------------------------------------------------- errors */
