@@ -69,13 +69,13 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(name: str):
-    """DRAM bytes per pass launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"pass_kernel_{name}.json")
+def ncu_traffic_ratio():
+    """DRAM bytes / algorithmic bytes of the fused pass, from the committed
+    ncu capture (profiles/pass_kernel_traffic.json), if present."""
+    p = os.path.join(ROOT, "profiles", "pass_kernel_traffic.json")
     if os.path.exists(p):
         with open(p) as f:
-            d = json.load(f)
-        return d.get("dram_bytes_per_launch")
+            return float(json.load(f)["dram_to_algorithmic_ratio"])
     return None
 
 
@@ -305,7 +305,8 @@ def run_ours(args, spec):
     if rank == 0:
         peak, peak_kind = measured_peaks()
         achieved = (pass_bytes / max(1, passes)) / (pass_ms / max(1, passes) * 1e-3) / 1e9 if pass_ms > 0 else None
-        traffic = ncu_traffic(spec["name"])
+        ratio = ncu_traffic_ratio()
+        traffic = ratio * pass_bytes / max(1, passes) if ratio is not None else None
         launches_per_step = int(st["passes"]) + 4 * int(st["stages"]) + 1
         value = world * updates_per_step * args.steps / (ms * 1e-3)
         out = {
@@ -323,7 +324,9 @@ def run_ours(args, spec):
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
-                         "kernel": "pass_kernel<double>", "pass_ms_per_step": pass_ms / args.steps,
+                         "traffic_source": "ncu DRAM/algorithmic ratio of QFT n=26 (profiles/) x bytes per launch",
+                         "kernel": f"pass_kernel<{'double' if spec['dtype'] == 'complex128' else 'float'}>",
+                         "pass_ms_per_step": pass_ms / args.steps,
                          "bytes_per_launch": pass_bytes / max(1, passes)},
             "e2e": {"value": world * updates_per_step * args.steps / (e2e_ms * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": len(blob_in), "d2h_bytes_per_step": int(d2h),

@@ -1198,6 +1198,122 @@ qs_status qs_load_vector(qs_state *h, const double *vec) {
     return done(QS_OK);
 }
 
+// ---- Pauli expectation values
+// Terms are batched so that each batch's flip qubits at or above the chunk
+// size fit in one tile; each batch is one read-only pass.
+qs_status qs_expectation_pauli(qs_state *h, const uint64_t *x_masks, const uint64_t *z_masks, size_t nterms,
+                               double *out) {
+    if (!h || (nterms && (!x_masks || !z_masks || !out))) return fail(h, QS_ERR_ARG, "NULL argument");
+    const int C = (int)h->C;
+    const int jmax = std::min(h->tile_log2 - C, qs::kMaxTileQubits);
+    const uint64_t full = h->n >= 64 ? ~0ull : ((1ull << h->n) - 1);
+    for (size_t t = 0; t < nterms; ++t) {
+        if ((x_masks[t] | z_masks[t]) & ~full) return fail(h, QS_ERR_ARG, "Pauli term acts outside the register");
+        int hi = 0;
+        for (int q = C; q < (int)h->n; ++q) hi += (x_masks[t] >> q) & 1;
+        if (hi > jmax) return fail(h, QS_ERR_ARG, "Pauli term flips more qubits than a tile holds");
+    }
+    // greedy batches
+    std::vector<std::vector<size_t>> batches;
+    std::vector<std::set<int>> tiles;
+    for (size_t t = 0; t < nterms; ++t) {
+        std::set<int> need;
+        for (int q = C; q < (int)h->n; ++q)
+            if ((x_masks[t] >> q) & 1) need.insert(q);
+        bool placed = false;
+        for (size_t b = 0; b < batches.size() && !placed; ++b) {
+            std::set<int> u = tiles[b];
+            u.insert(need.begin(), need.end());
+            if ((int)u.size() <= jmax && batches[b].size() < 256) {
+                tiles[b] = u;
+                batches[b].push_back(t);
+                placed = true;
+            }
+        }
+        if (!placed) {
+            batches.push_back({t});
+            tiles.push_back(need);
+        }
+    }
+    double *dout = nullptr;
+    qs::PauliTerm *dterms = nullptr;
+    qs_status rs = QS_OK;
+    cudaError_t e = cudaMalloc(&dout, std::max<size_t>(1, 2 * nterms) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&dterms, std::max<size_t>(1, nterms) * sizeof(qs::PauliTerm));
+    if (e == cudaSuccess) e = cudaMemsetAsync(dout, 0, std::max<size_t>(1, 2 * nterms) * sizeof(double), h->stream);
+    std::vector<qs::PauliTerm> host(nterms);
+    for (size_t b = 0; b < batches.size() && e == cudaSuccess; ++b) {
+        std::set<int> tq = tiles[b];
+        for (int q = C; q < (int)h->n && (int)tq.size() < std::min(3, jmax); ++q) tq.insert(q);
+        std::vector<int> tv(tq.begin(), tq.end());
+        auto local = [&](uint64_t m, uint64_t *outside) {
+            uint32_t r = 0;
+            uint64_t o = 0;
+            for (int q = 0; q < (int)h->n; ++q) {
+                if (!((m >> q) & 1)) continue;
+                if (q < C) r |= 1u << q;
+                else {
+                    auto it = std::find(tv.begin(), tv.end(), q);
+                    if (it != tv.end()) r |= 1u << (C + (int)(it - tv.begin()));
+                    else o |= 1ull << q;
+                }
+            }
+            if (outside) *outside = o;
+            return r;
+        };
+        std::vector<qs::PauliTerm> bt;
+        for (size_t t : batches[b]) {
+            qs::PauliTerm pt{};
+            uint64_t dummy = 0;
+            pt.xt = local(x_masks[t], &dummy);
+            pt.zt = local(z_masks[t], &pt.zo);
+            pt.xg = x_masks[t];
+            pt.zg = z_masks[t];
+            bt.push_back(pt);
+        }
+        // the batch's terms are laid out contiguously in dterms at offset of the first
+        const size_t off = batches[b][0];
+        (void)off;
+        qs::PauliTerm *bdev = nullptr;
+        double *bout = nullptr;
+        e = cudaMalloc(&bdev, bt.size() * sizeof(qs::PauliTerm));
+        if (e == cudaSuccess) e = cudaMalloc(&bout, 2 * bt.size() * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemcpyAsync(bdev, bt.data(), bt.size() * sizeof(qs::PauliTerm), cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(bout, 0, 2 * bt.size() * sizeof(double), h->stream);
+        if (e == cudaSuccess) {
+            qs::ExpectArgs a{};
+            a.n = (int)h->n;
+            a.B = (int)h->B;
+            a.C = C;
+            a.j = (int)tv.size();
+            for (int k = 0; k < a.j; ++k) a.tq[k] = tv[k] - C;
+            a.n_tiles = uint64_t(1) << (h->n - C - a.j);
+            a.meta = h->meta[h->cur];
+            a.arena = h->arena[h->cur];
+            a.mask = h->mask;
+            a.codec = h->codec;
+            a.terms = bdev;
+            a.nterms = (int)bt.size();
+            a.out = bout;
+            e = qs::launch_expect(h->f64, a, h->stream);
+        }
+        std::vector<double> hb(2 * bt.size());
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hb.data(), bout, hb.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e == cudaSuccess)
+            for (size_t k = 0; k < batches[b].size(); ++k) {
+                out[2 * batches[b][k]] = hb[2 * k];
+                out[2 * batches[b][k] + 1] = hb[2 * k + 1];
+            }
+        if (bdev) cudaFree(bdev);
+        if (bout) cudaFree(bout);
+    }
+    if (e != cudaSuccess) rs = fail(h, QS_ERR_CUDA, std::string("expectation: ") + cudaGetErrorString(e));
+    if (dout) cudaFree(dout);
+    if (dterms) cudaFree(dterms);
+    return rs;
+}
+
 // ---- store serialisation
 struct StoreHeader {
     char magic[8];
@@ -1547,6 +1663,36 @@ qs_status qs_dense_norm_squared(qs_dense *h, double *out) {
 qs_status qs_dense_device_ptr(qs_dense *h, void **out) {
     if (!h || !out) return dfail(h, QS_ERR_ARG, "NULL argument");
     *out = h->state;
+    return QS_OK;
+}
+
+qs_status qs_dense_expectation_pauli(qs_dense *h, const uint64_t *x_masks, const uint64_t *z_masks, size_t nterms,
+                                     double *out) {
+    if (!h || (nterms && (!x_masks || !z_masks || !out))) return dfail(h, QS_ERR_ARG, "NULL argument");
+    const uint64_t full = h->n >= 64 ? ~0ull : ((1ull << h->n) - 1);
+    std::vector<qs::PauliTerm> pts(nterms);
+    for (size_t t = 0; t < nterms; ++t) {
+        if ((x_masks[t] | z_masks[t]) & ~full) return dfail(h, QS_ERR_ARG, "Pauli term acts outside the register");
+        pts[t] = qs::PauliTerm{};
+        pts[t].xg = x_masks[t];
+        pts[t].zg = z_masks[t];
+    }
+    if (!nterms) return QS_OK;
+    qs::PauliTerm *dt = nullptr;
+    double *dout = nullptr;
+    cudaError_t e = cudaMalloc(&dt, nterms * sizeof(qs::PauliTerm));
+    if (e == cudaSuccess) e = cudaMalloc(&dout, 2 * nterms * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt, pts.data(), nterms * sizeof(qs::PauliTerm), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dout, 0, 2 * nterms * sizeof(double), h->stream);
+    for (size_t t0 = 0; t0 < nterms && e == cudaSuccess; t0 += 256) {
+        const int cnt = (int)std::min<size_t>(256, nterms - t0);
+        e = qs::launch_dense_expect(h->f64, h->state, (int)h->n, dt + t0, cnt, dout + 2 * t0, h->stream);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, 2 * nterms * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (dt) cudaFree(dt);
+    if (dout) cudaFree(dout);
+    if (e != cudaSuccess) return dfail(h, QS_ERR_CUDA, std::string("expectation: ") + cudaGetErrorString(e));
     return QS_OK;
 }
 

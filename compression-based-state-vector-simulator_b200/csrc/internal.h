@@ -121,7 +121,62 @@ struct DensePassArgs {
     void *state;
 };
 
+// A Pauli string as the expectation kernels read it: P|x> = i^ny (-1)^{|x & z|} |x ^ x_flip>.
+// Tile-local masks (bits of the tile index) plus the parity of z-qubits that
+// lie outside the tile (taken from the tile's base amplitude).
+struct PauliTerm {
+    uint32_t xt, zt;   // flip / sign masks over tile bits
+    uint64_t zo;       // sign mask over qubits outside the tile (global bit positions)
+    uint64_t xg, zg;   // the same string over global qubits (dense kernel)
+};
+
+// One read-only pass over the compressed store accumulating, for each term t,
+// S_t = sum_x conj(psi_{x ^ xflip}) (-1)^{|x & z|} psi_x into out[2t], out[2t+1].
+struct ExpectArgs {
+    int32_t n, B, C, j;
+    int32_t tq[kMaxTileQubits];
+    uint64_t n_tiles;
+    const ChunkMeta *meta;
+    const uint32_t *arena;
+    const uint8_t *mask;
+    CodecParams codec;
+    const PauliTerm *terms;
+    int32_t nterms;
+    double *out;
+};
+
+// Backward (adjoint) pass over two uncompressed states psi and lam: gates are
+// applied in the listed order (the caller lists U_k^dagger in reverse circuit
+// order); before a gate with slot >= 0, S_slot = sum_x conj(lam[x ^ gen.x])
+// (-1)^{|x & gen.z|} psi[x] is accumulated into out[2 slot], out[2 slot + 1].
+struct AdjGate {
+    KGate g;           // the gate to apply (tile positions resolved)
+    PauliTerm gen;     // generator of the parametric gate (tile-local masks)
+    int32_t slot;      // -1: no derivative at this gate
+    int32_t pad;
+};
+struct AdjPassArgs {
+    int32_t n, C, j;
+    int32_t tq[kMaxTileQubits];
+    uint64_t n_tiles;
+    const AdjGate *gates;
+    int32_t ngates;
+    void *psi;
+    void *lam;
+    double *out;
+    int32_t nslots;
+};
+
 // ---- launchers (kernels.cu); all asynchronous on `stream` ----
+cudaError_t launch_adjoint_pass(bool f64, const AdjPassArgs &a, cudaStream_t stream);
+cudaError_t launch_dense_transition(bool f64, const void *bra, const void *ket, int n, const PauliTerm *terms,
+                                    int nterms, double *out, cudaStream_t stream);
+// out = sum_t coef_t P_t in (coefs complex interleaved; PauliTerm global masks, ny folded into coefs)
+cudaError_t launch_dense_pauli_sum(bool f64, const void *in, void *out, int n, const PauliTerm *terms,
+                                   const double *coefs, int nterms, cudaStream_t stream);
+cudaError_t launch_expect(bool f64, const ExpectArgs &a, cudaStream_t stream);
+cudaError_t launch_dense_expect(bool f64, const void *state, int n, const PauliTerm *terms, int nterms, double *out,
+                                cudaStream_t stream);
 cudaError_t launch_pass(bool f64, const PassArgs &a, int tile_log2, cudaStream_t stream);
 cudaError_t launch_dense_pass(bool f64, const DensePassArgs &a, int tile_log2, cudaStream_t stream);
 cudaError_t launch_pergate(bool f64, void *state, int n, const KGate *gate_dev, cudaStream_t stream);

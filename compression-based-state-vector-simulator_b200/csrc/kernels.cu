@@ -834,6 +834,245 @@ __global__ void from_c128_kernel(const double *in, uint64_t ncomp, R *s) {
         s[i] = (R)in[i];
 }
 
+// ------------------------------------------------------------ Pauli expectation
+constexpr int kExpectThreads = 256;
+constexpr int kMaxTermsPerLaunch = 256;
+
+__device__ __forceinline__ double block_warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kExpectThreads) expect_kernel(const ExpectArgs a) {
+    using T = typename Cplx<R>::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double s_acc[2 * kMaxTermsPerLaunch];
+    __shared__ int32_t s_tq[kMaxTileQubits];
+    const int C = a.C, j = a.j, nb = C + j;
+    const int nchunks = 1 << j;
+    const int ncomp = 2 << C;
+    const int per_lane = ncomp >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int blk_shift = a.B - C;
+    const int swm = swizzle_mask<R>(C);
+    T *tile = reinterpret_cast<T *>(smem);
+    uint32_t *wstage = reinterpret_cast<uint32_t *>(smem + (sizeof(T) << nb)) + warp * (kMaxPerLane * 32);
+    for (int i = threadIdx.x; i < 2 * a.nterms; i += blockDim.x) s_acc[i] = 0.0;
+    if (threadIdx.x < kMaxTileQubits) s_tq[threadIdx.x] = a.tq[threadIdx.x];
+    __syncthreads();
+    const int size = 1 << nb;
+    for (uint64_t tile_id = blockIdx.x; tile_id < a.n_tiles; tile_id += gridDim.x) {
+        const uint64_t chunk_base = insert_zero_bits(tile_id, s_tq, j);
+        bool any = false;
+        for (int c = 0; c < nchunks; ++c) any |= a.mask[(chunk_base | deposit_bits((uint32_t)c, s_tq, j)) >> blk_shift] != 0;
+        if (!any) continue;  // uniform: every thread reads the same mask bytes
+        for (int c = warp; c < nchunks; c += nwarps) {
+            const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
+            R *comp = reinterpret_cast<R *>(tile) + (size_t)c * ncomp;
+            if (!a.mask[chunk >> blk_shift]) {
+                for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = R(0);
+                continue;
+            }
+            decode_chunk<R>(a.arena, a.meta[chunk], per_lane, a.codec, reinterpret_cast<R *>(tile), wstage, lane,
+                            TileSlot<R>{c << C, swm});
+        }
+        __syncthreads();
+        const uint64_t base_amp = chunk_base << C;
+        for (int t = 0; t < a.nterms; ++t) {
+            const PauliTerm pt = a.terms[t];
+            const int outer = __popcll(base_amp & pt.zo) & 1;
+            double re = 0.0, im = 0.0;
+            for (int x = threadIdx.x; x < size; x += blockDim.x) {
+                const T ax = tile[swz<R>(x, swm)];
+                const T by = tile[swz<R>(x ^ (int)pt.xt, swm)];
+                // conj(by) * ax
+                double pr = (double)by.x * (double)ax.x + (double)by.y * (double)ax.y;
+                double pi = (double)by.x * (double)ax.y - (double)by.y * (double)ax.x;
+                if ((__popc((uint32_t)x & pt.zt) + outer) & 1) { pr = -pr; pi = -pi; }
+                re += pr;
+                im += pi;
+            }
+            re = block_warp_sum(re);
+            im = block_warp_sum(im);
+            if (lane == 0) {
+                atomicAdd(&s_acc[2 * t], re);
+                atomicAdd(&s_acc[2 * t + 1], im);
+            }
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * a.nterms; i += blockDim.x)
+        if (s_acc[i] != 0.0) atomicAdd(&a.out[i], s_acc[i]);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kExpectThreads) dense_expect_kernel(const typename Cplx<R>::T *__restrict__ bra,
+                                                                      const typename Cplx<R>::T *__restrict__ st, int n,
+                                                                      const PauliTerm *terms, int nterms, double *out) {
+    using T = typename Cplx<R>::T;
+    __shared__ double s_acc[2 * kMaxTermsPerLaunch];
+    const int lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < 2 * nterms; i += blockDim.x) s_acc[i] = 0.0;
+    __syncthreads();
+    const uint64_t dim = uint64_t(1) << n;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (int t = 0; t < nterms; ++t) {
+        const PauliTerm pt = terms[t];
+        double re = 0.0, im = 0.0;
+        for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < dim; x += stride) {
+            const T ax = st[x];
+            const T by = bra[x ^ pt.xg];
+            double pr = (double)by.x * (double)ax.x + (double)by.y * (double)ax.y;
+            double pi = (double)by.x * (double)ax.y - (double)by.y * (double)ax.x;
+            if (__popcll(x & pt.zg) & 1) { pr = -pr; pi = -pi; }
+            re += pr;
+            im += pi;
+        }
+        re = block_warp_sum(re);
+        im = block_warp_sum(im);
+        if (lane == 0) {
+            atomicAdd(&s_acc[2 * t], re);
+            atomicAdd(&s_acc[2 * t + 1], im);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * nterms; i += blockDim.x)
+        if (s_acc[i] != 0.0) atomicAdd(&out[i], s_acc[i]);
+}
+
+// ------------------------------------------------------------ adjoint backward pass
+// One gate on a shared-memory tile (linear layout); the gate's qubits outside
+// the tile are fixed by base_amp and must be non-mixing.
+template <typename R>
+__device__ void smem_apply_gate(typename Cplx<R>::T *t, int nb, const KGate &g, uint64_t base_amp) {
+    using T = typename Cplx<R>::T;
+    const int dim = 1 << g.nq;
+    int pos[2] = {-1, -1}, fixv[2] = {0, 0};
+    for (int i = 0; i < g.nq; ++i) {
+        pos[i] = g.tpos[i];
+        if (pos[i] < 0) fixv[i] = (int)((base_amp >> g.q[i]) & 1);
+    }
+    int vb[2], nv = 0;  // matrix bits that vary inside the tile
+    for (int i = 0; i < g.nq; ++i)
+        if (pos[i] >= 0) vb[nv++] = i;
+    int fixidx = 0;
+    for (int i = 0; i < g.nq; ++i)
+        if (pos[i] < 0) fixidx |= fixv[i] << i;
+    auto M = [&](int r, int c) { return make_c<T, R>(g.m[2 * (r * dim + c)], g.m[2 * (r * dim + c) + 1]); };
+    auto full = [&](int x) {  // matrix index of local pattern x
+        int idx = fixidx;
+        for (int k = 0; k < nv; ++k)
+            if ((x >> k) & 1) idx |= 1 << vb[k];
+        return idx;
+    };
+    const int size = 1 << nb;
+    if (nv == 0) {
+        const T c = M(fixidx, fixidx);
+        for (int i = threadIdx.x; i < size; i += blockDim.x) t[i] = cmul(c, t[i]);
+    } else if (nv == 1) {
+        const int p = pos[vb[0]];
+        const T e0 = M(full(0), full(0)), e1 = M(full(0), full(1)), e2 = M(full(1), full(0)), e3 = M(full(1), full(1));
+        const int lowmask = (1 << p) - 1;
+        for (int i = threadIdx.x; i < size / 2; i += blockDim.x) {
+            const int i0 = ((i & ~lowmask) << 1) | (i & lowmask), i1 = i0 | (1 << p);
+            const T a = t[i0], b = t[i1];
+            t[i0] = cfma(e0, a, cmul(e1, b));
+            t[i1] = cfma(e2, a, cmul(e3, b));
+        }
+    } else {
+        const int pa = pos[0], pb = pos[1];
+        const int lo = pa < pb ? pa : pb, hi = pa < pb ? pb : pa;
+        const int mlo = (1 << lo) - 1, mhi = (1 << hi) - 1;
+        T mm[16];
+        for (int k = 0; k < 16; ++k) mm[k] = M(k / 4, k % 4);
+        for (int i = threadIdx.x; i < size / 4; i += blockDim.x) {
+            int b = ((i & ~mlo) << 1) | (i & mlo);
+            b = ((b & ~mhi) << 1) | (b & mhi);
+            const int ia = 1 << pa, ib = 1 << pb;
+            const T v0 = t[b], v1 = t[b | ia], v2 = t[b | ib], v3 = t[b | ia | ib];
+            T o[4];
+            for (int r = 0; r < 4; ++r) {
+                T acc = cmul(mm[4 * r], v0);
+                acc = cfma(mm[4 * r + 1], v1, acc);
+                acc = cfma(mm[4 * r + 2], v2, acc);
+                acc = cfma(mm[4 * r + 3], v3, acc);
+                o[r] = acc;
+            }
+            t[b] = o[0];
+            t[b | ia] = o[1];
+            t[b | ib] = o[2];
+            t[b | ia | ib] = o[3];
+        }
+    }
+}
+
+constexpr int kAdjThreads = 256;
+constexpr int kMaxAdjSlots = 128;
+
+template <typename R>
+__global__ void __launch_bounds__(kAdjThreads) adjoint_pass_kernel(const AdjPassArgs a) {
+    using T = typename Cplx<R>::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double s_acc[2 * kMaxAdjSlots];
+    __shared__ int32_t s_tq[kMaxTileQubits];
+    const int C = a.C, j = a.j, nb = C + j, size = 1 << nb;
+    const int cmask = (1 << C) - 1;
+    const int lane = threadIdx.x & 31;
+    T *tp = reinterpret_cast<T *>(smem);
+    T *tl = tp + size;
+    T *psi = reinterpret_cast<T *>(a.psi);
+    T *lam = reinterpret_cast<T *>(a.lam);
+    for (int i = threadIdx.x; i < 2 * a.nslots; i += blockDim.x) s_acc[i] = 0.0;
+    if (threadIdx.x < kMaxTileQubits) s_tq[threadIdx.x] = a.tq[threadIdx.x];
+    __syncthreads();
+    for (uint64_t tile_id = blockIdx.x; tile_id < a.n_tiles; tile_id += gridDim.x) {
+        const uint64_t chunk_base = insert_zero_bits(tile_id, s_tq, j);
+        for (int e = threadIdx.x; e < size; e += blockDim.x) {
+            const uint64_t amp = ((chunk_base | deposit_bits((uint32_t)(e >> C), s_tq, j)) << C) | (uint64_t)(e & cmask);
+            tp[e] = psi[amp];
+            tl[e] = lam[amp];
+        }
+        __syncthreads();
+        const uint64_t base_amp = chunk_base << C;
+        for (int k = 0; k < a.ngates; ++k) {
+            const AdjGate &ag = a.gates[k];
+            if (ag.slot >= 0) {
+                const int outer = __popcll(base_amp & ag.gen.zo) & 1;
+                double re = 0.0, im = 0.0;
+                for (int x = threadIdx.x; x < size; x += blockDim.x) {
+                    const T ax = tp[x];
+                    const T by = tl[x ^ (int)ag.gen.xt];
+                    double pr = (double)by.x * (double)ax.x + (double)by.y * (double)ax.y;
+                    double pi = (double)by.x * (double)ax.y - (double)by.y * (double)ax.x;
+                    if ((__popc((uint32_t)x & ag.gen.zt) + outer) & 1) { pr = -pr; pi = -pi; }
+                    re += pr;
+                    im += pi;
+                }
+                re = block_warp_sum(re);
+                im = block_warp_sum(im);
+                if (lane == 0) {
+                    atomicAdd(&s_acc[2 * ag.slot], re);
+                    atomicAdd(&s_acc[2 * ag.slot + 1], im);
+                }
+                __syncthreads();
+            }
+            smem_apply_gate<R>(tp, nb, ag.g, base_amp);
+            smem_apply_gate<R>(tl, nb, ag.g, base_amp);
+            __syncthreads();
+        }
+        for (int e = threadIdx.x; e < size; e += blockDim.x) {
+            const uint64_t amp = ((chunk_base | deposit_bits((uint32_t)(e >> C), s_tq, j)) << C) | (uint64_t)(e & cmask);
+            psi[amp] = tp[e];
+            lam[amp] = tl[e];
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < 2 * a.nslots; i += blockDim.x)
+        if (s_acc[i] != 0.0) atomicAdd(&a.out[i], s_acc[i]);
+}
+
 int g_sm_count = 0;
 
 // Scratch of the allocation-free codec round trip (qs_codec_roundtrip_noalloc):
@@ -982,6 +1221,28 @@ cudaError_t launch_codec_test(bool f64, const void *vals, int C, CodecParams p, 
 
 uint64_t noalloc_scratch_words() { return kNoAllocScratchWords; }
 
+template <typename R>
+static cudaError_t launch_adjoint_pass_t(const AdjPassArgs &a, cudaStream_t s) {
+    if (a.nslots > kMaxAdjSlots) return cudaErrorInvalidValue;
+    const int nb = a.C + a.j;
+    const size_t smem = (size_t)(4 * sizeof(R)) << nb;
+    cudaError_t e = cudaFuncSetAttribute(adjoint_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_pass_kernel<R>, kAdjThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    uint64_t grid = (uint64_t)per_sm * sm_count();
+    if (grid > a.n_tiles) grid = a.n_tiles;
+    if (grid == 0) grid = 1;
+    adjoint_pass_kernel<R><<<(unsigned)grid, kAdjThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_pass(bool f64, const AdjPassArgs &a, cudaStream_t s) {
+    return f64 ? launch_adjoint_pass_t<double>(a, s) : launch_adjoint_pass_t<float>(a, s);
+}
+
 // Host code may not use g_noalloc_words directly: in host code the name is a
 // host-side stand-in, not a device address.  The device address is looked up
 // once per device, with that device current, and cached.
@@ -1011,6 +1272,87 @@ cudaError_t launch_codec_roundtrip_noalloc(bool f64, const void *vals, int C, Co
     else
         codec_test_kernel<float><<<grid, kPassThreads, 0, s>>>((const float *)vals, C, p, nchunks, words, bases, widths,
                                                               (float *)decoded);
+    return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t launch_expect_t(const ExpectArgs &a, cudaStream_t s) {
+    if (a.nterms > kMaxTermsPerLaunch) return cudaErrorInvalidValue;
+    const int nb = a.C + a.j;
+    const size_t smem = ((size_t)(2 * sizeof(R)) << nb) + (size_t)(kExpectThreads / 32) * kMaxPerLane * 32 * 4;
+    cudaError_t e = cudaFuncSetAttribute(expect_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, expect_kernel<R>, kExpectThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    uint64_t grid = (uint64_t)per_sm * sm_count();
+    if (grid > a.n_tiles) grid = a.n_tiles;
+    if (grid == 0) grid = 1;
+    expect_kernel<R><<<(unsigned)grid, kExpectThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_expect(bool f64, const ExpectArgs &a, cudaStream_t s) {
+    return f64 ? launch_expect_t<double>(a, s) : launch_expect_t<float>(a, s);
+}
+
+cudaError_t launch_dense_expect(bool f64, const void *state, int n, const PauliTerm *terms, int nterms, double *out,
+                                cudaStream_t s) {
+    if (nterms > kMaxTermsPerLaunch) return cudaErrorInvalidValue;
+    const unsigned grid = grid_for(uint64_t(1) << n, kExpectThreads, 8);
+    if (f64)
+        dense_expect_kernel<double><<<grid, kExpectThreads, 0, s>>>((const double2 *)state, (const double2 *)state, n,
+                                                                   terms, nterms, out);
+    else
+        dense_expect_kernel<float><<<grid, kExpectThreads, 0, s>>>((const float2 *)state, (const float2 *)state, n, terms,
+                                                                  nterms, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dense_transition(bool f64, const void *bra, const void *ket, int n, const PauliTerm *terms,
+                                    int nterms, double *out, cudaStream_t s) {
+    if (nterms > kMaxTermsPerLaunch) return cudaErrorInvalidValue;
+    const unsigned grid = grid_for(uint64_t(1) << n, kExpectThreads, 8);
+    if (f64)
+        dense_expect_kernel<double><<<grid, kExpectThreads, 0, s>>>((const double2 *)bra, (const double2 *)ket, n, terms,
+                                                                   nterms, out);
+    else
+        dense_expect_kernel<float><<<grid, kExpectThreads, 0, s>>>((const float2 *)bra, (const float2 *)ket, n, terms,
+                                                                  nterms, out);
+    return cudaGetLastError();
+}
+
+template <typename R>
+__global__ void dense_pauli_sum_kernel(const typename Cplx<R>::T *__restrict__ in, typename Cplx<R>::T *__restrict__ out,
+                                       int n, const PauliTerm *__restrict__ terms, const double *__restrict__ coefs,
+                                       int nterms) {
+    using T = typename Cplx<R>::T;
+    const uint64_t dim = uint64_t(1) << n;
+    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < dim; x += (uint64_t)gridDim.x * blockDim.x) {
+        double re = 0.0, im = 0.0;
+        for (int t = 0; t < nterms; ++t) {
+            const uint64_t y = x ^ terms[t].xg;
+            const T v = in[y];
+            double cr = coefs[2 * t], ci = coefs[2 * t + 1];
+            if (__popcll(y & terms[t].zg) & 1) { cr = -cr; ci = -ci; }
+            re += cr * (double)v.x - ci * (double)v.y;
+            im += cr * (double)v.y + ci * (double)v.x;
+        }
+        T o;
+        o.x = (R)re;
+        o.y = (R)im;
+        out[x] = o;
+    }
+}
+
+cudaError_t launch_dense_pauli_sum(bool f64, const void *in, void *out, int n, const PauliTerm *terms,
+                                   const double *coefs, int nterms, cudaStream_t s) {
+    const unsigned grid = grid_for(uint64_t(1) << n, 256, 8);
+    if (f64)
+        dense_pauli_sum_kernel<double><<<grid, 256, 0, s>>>((const double2 *)in, (double2 *)out, n, terms, coefs, nterms);
+    else
+        dense_pauli_sum_kernel<float><<<grid, 256, 0, s>>>((const float2 *)in, (float2 *)out, n, terms, coefs, nterms);
     return cudaGetLastError();
 }
 

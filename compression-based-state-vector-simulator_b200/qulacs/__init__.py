@@ -175,6 +175,84 @@ class ParametricQuantumCircuit(QuantumCircuit):
 
 
 # =====================================================================
+# observables
+# =====================================================================
+_PAULI_IDS = {"I": 0, "X": 1, "Y": 2, "Z": 3}
+
+
+def _parse_pauli(pauli: str):
+    """'X 0 Z 3 Y 5' -> (x_mask, z_mask, number of Y factors)."""
+    tok = pauli.split()
+    if len(tok) % 2:
+        raise ValueError(f"malformed Pauli string {pauli!r}")
+    xm = zm = ny = 0
+    for a, b in zip(tok[0::2], tok[1::2]):
+        p, q = a.upper(), int(b)
+        if p not in _PAULI_IDS:
+            raise ValueError(f"unknown Pauli {a!r}")
+        bit = 1 << q
+        if (xm | zm) & bit:
+            raise ValueError(f"qubit {q} appears twice in {pauli!r}")
+        if p in ("X", "Y"):
+            xm |= bit
+        if p in ("Z", "Y"):
+            zm |= bit
+        ny += p == "Y"
+    return xm, zm, ny
+
+
+class Observable:
+    """A sum of Pauli strings with real coefficients (src/cppsim/observable.hpp).
+
+    get_expectation_value(state) evaluates every term on the device with FP64
+    accumulation (qs_expectation_pauli / qs_dense_expectation_pauli).  On a
+    CompressedQuantumState the value is divided by the state's squared norm,
+    as the reference renormalises the compressed state on readout."""
+
+    def __init__(self, qubit_count: int):
+        self._n = int(qubit_count)
+        self._terms: List[tuple] = []   # (coef, x_mask, z_mask, ny, text)
+
+    def add_operator(self, coef, pauli: str) -> None:
+        xm, zm, ny = _parse_pauli(pauli)
+        if (xm | zm) >> self._n:
+            raise ValueError("Pauli string acts outside the observable's qubits")
+        self._terms.append((complex(coef), xm, zm, ny, pauli))
+
+    def get_term_count(self) -> int:
+        return len(self._terms)
+
+    def get_qubit_count(self) -> int:
+        return self._n
+
+    def term_masks(self):
+        return ([t[1] for t in self._terms], [t[2] for t in self._terms], [t[3] for t in self._terms],
+                [t[0] for t in self._terms])
+
+    def get_term_values(self, state) -> np.ndarray:
+        """<P_t> for every term (complex, without coefficients)."""
+        xs, zs, nys, _ = self.term_masks()
+        sums = state._pauli_sums(xs + [0], zs + [0])
+        norm = sums[-1].real if isinstance(state, CompressedQuantumState) else 1.0
+        return np.array([(1j ** ny) * v / norm for ny, v in zip(nys, sums[:-1])])
+
+    def get_expectation_value(self, state) -> float:
+        vals = self.get_term_values(state)
+        coefs = np.array([t[0] for t in self._terms])
+        return float(np.real(np.sum(coefs * vals)))
+
+
+def _pauli_sums(fn, handle, checker, xs, zs):
+    n = len(xs)
+    xa = np.ascontiguousarray(np.asarray(xs, dtype=np.uint64))
+    za = np.ascontiguousarray(np.asarray(zs, dtype=np.uint64))
+    out = np.zeros(2 * max(1, n), dtype=np.float64)
+    checker(fn(handle, xa.ctypes.data_as(_n.ct.POINTER(_n.ct.c_uint64)), za.ctypes.data_as(_n.ct.POINTER(_n.ct.c_uint64)),
+               n, out.ctypes.data_as(_n.ct.POINTER(_n.ct.c_double))))
+    return out[0:2 * n:2] + 1j * out[1:2 * n:2]
+
+
+# =====================================================================
 # uncompressed state
 # =====================================================================
 class QuantumState:
@@ -238,6 +316,9 @@ class QuantumState:
         fn = _n.lib().qs_dense_apply_gates_pergate if (self._pergate if pergate is None else pergate) \
             else _n.lib().qs_dense_apply_gates
         self._check(fn(self._h, arr, len(gates)))
+
+    def _pauli_sums(self, xs, zs):
+        return _pauli_sums(_n.lib().qs_dense_expectation_pauli, self._h, self._check, xs, zs)
 
     def device_pointer(self) -> int:
         p = _n.ct.c_void_p()
@@ -391,6 +472,9 @@ class CompressedQuantumState:
     def set_computational_basis(self, basis: int) -> None:
         self._check(_n.lib().qs_set_basis_state(self._h, int(basis)))
 
+    def _pauli_sums(self, xs, zs):
+        return _pauli_sums(_n.lib().qs_expectation_pauli, self._h, self._check, xs, zs)
+
     def set_zero_state(self) -> None:
         self.set_computational_basis(0)
 
@@ -461,6 +545,6 @@ class CompressedQuantumState:
 
 
 __all__ = [
-    "QuantumState", "QuantumCircuit", "ParametricQuantumCircuit", "CompressedQuantumState",
+    "QuantumState", "QuantumCircuit", "ParametricQuantumCircuit", "CompressedQuantumState", "Observable",
     "QuantumGateBase", "QuantumGateMatrix", "check_build_for_mpi", "gate", "circuit", "QompsimError",
 ]

@@ -97,6 +97,8 @@ SIGNATURES = [
     ("qs_apply_circuit", ct.c_int, [_P]),
     ("qs_get_vector", ct.c_int, [_P, ct.POINTER(_D), ct.c_int]),
     ("qs_norm_squared", ct.c_int, [_P, ct.POINTER(_D)]),
+    ("qs_expectation_pauli", ct.c_int, [_P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
+    ("qs_dense_expectation_pauli", ct.c_int, [_P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
     ("qs_get_zero_mask", ct.c_int, [_P, ct.POINTER(ct.c_uint8)]),
     ("qs_get_block_bytes", ct.c_int, [_P, ct.POINTER(_U64)]),
     ("qs_get_max_sv_bytes", ct.c_int, [_P, ct.POINTER(_U64)]),

@@ -169,6 +169,19 @@ qs_status qs_get_vector(qs_state *h, double *out, int renormalize);
 /* Squared norm of the compressed state, accumulated in FP64. */
 qs_status qs_norm_squared(qs_state *h, double *out);
 
+/* Pauli expectation sums on the compressed state, FP64 accumulation: for
+ * term t with flip mask x_masks[t] (qubits carrying X or Y) and sign mask
+ * z_masks[t] (qubits carrying Z or Y), out[2t] + i out[2t+1] =
+ * sum_x conj(psi[x ^ x]) (-1)^{popcount(x & z)} psi[x].  The caller applies
+ * i^(number of Y factors) and the coefficients, and divides by the squared
+ * norm (the term with both masks 0).  Replaces Observable /
+ * get_expectation_value on the reference's uncompressed states
+ * (src/cppsim/observable.hpp:80); the reference has no expectation value on
+ * its compressed state.  A term may flip at most tile_log2 - chunk_log2
+ * qubits at or above the chunk size. */
+qs_status qs_expectation_pauli(qs_state *h, const uint64_t *x_masks, const uint64_t *z_masks, size_t nterms,
+                               double *out);
+
 /* Zero-block mask: out[b] = 1 when block b is stored (the reference's
  * block_pointers[b] != nullptr, compressed_state.hpp:18-19, 319-325). */
 qs_status qs_get_zero_mask(qs_state *h, uint8_t *out);
@@ -227,6 +240,10 @@ qs_status qs_dense_get_vector(qs_dense *h, double *out);
 qs_status qs_dense_set_vector(qs_dense *h, const double *in);
 qs_status qs_dense_set_basis_state(qs_dense *h, uint64_t basis);
 qs_status qs_dense_norm_squared(qs_dense *h, double *out);
+
+/* The same Pauli expectation sums on the uncompressed state. */
+qs_status qs_dense_expectation_pauli(qs_dense *h, const uint64_t *x_masks, const uint64_t *z_masks, size_t nterms,
+                                     double *out);
 
 /* Device pointer of the amplitudes (interleaved re, im of the dtype). */
 qs_status qs_dense_device_ptr(qs_dense *h, void **out);
