@@ -150,12 +150,21 @@ def barrier(pg, torch):
     torch.cuda.synchronize()
 
 
-def max_over_ranks(pg, torch, x: float) -> float:
+def max_over_ranks(pg, torch, x: float, device: str = "cuda") -> float:
+    """The largest x over all ranks (timings are taken as the max over ranks)."""
     if pg is None:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate(pg, torch, local_ms: float, updates_per_step: int, steps: int, world: int, device: str = "cuda"):
+    """Whole-job figure of N replicas: every rank applied `steps` circuits of
+    `updates_per_step` amplitude-gate updates; the job took the slowest
+    rank's time.  Returns (ms, updates/s)."""
+    ms = max_over_ranks(pg, torch, local_ms, device)
+    return ms, world * updates_per_step * steps / (ms * 1e-3)
 
 
 # ----------------------------------------------------------------- CPU baseline
@@ -193,8 +202,8 @@ def cpu_sample(spec, budget_s: float = 12.0):
 
 
 def run_reference(args, spec):
-    world, rank, _, _ = dist_setup(args) if int(os.environ.get("WORLD_SIZE", "1")) > 1 else (1, 0, 0, None)
-    if rank != 0:
+    # under torchrun only rank 0 runs the CPU baseline; the others exit at once
+    if int(os.environ.get("RANK", "0")) != 0:
         return
     from oracle import csim_ref
     if not csim_ref.available():
@@ -261,8 +270,7 @@ def run_ours(args, spec):
             passes += int(s["passes"])
         end.record()
         torch.cuda.synchronize()
-    ms = start.elapsed_time(end)
-    ms = max_over_ranks(pg, torch, ms)
+    ms, value = aggregate(pg, torch, start.elapsed_time(end), updates_per_step, args.steps, world)
     barrier(pg, torch)
     clocks = clk.summary()
 
@@ -308,7 +316,6 @@ def run_ours(args, spec):
         ratio = ncu_traffic_ratio()
         traffic = ratio * pass_bytes / max(1, passes) if ratio is not None else None
         launches_per_step = int(st["passes"]) + 4 * int(st["stages"]) + 1
-        value = world * updates_per_step * args.steps / (ms * 1e-3)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,

@@ -493,6 +493,16 @@ struct qs_state {
     int cur = 0;
     uint64_t arena_used = 0;
 
+    struct Checkpoint {
+        qs::ChunkMeta *meta = nullptr;
+        uint32_t *arena = nullptr;
+        uint64_t arena_cap = 0, used = 0;
+        uint8_t *mask = nullptr;
+        unsigned long long *block_bytes = nullptr;
+        std::vector<uint64_t> history;
+    };
+    std::vector<Checkpoint> ckpt;
+
     std::vector<uint64_t> history;
     double times[10] = {0};
     qs_stats st{};
@@ -519,6 +529,15 @@ struct qs_state {
         for (auto e : pass_ev) cudaEventDestroy(e);
         if (error_dev) cudaFree(error_dev);
         if (dscratch) cudaFree(dscratch);
+        for (auto &c : ckpt) free_checkpoint(c);
+    }
+
+    static void free_checkpoint(Checkpoint &c) {
+        if (c.meta) cudaFree(c.meta);
+        if (c.arena) cudaFree(c.arena);
+        if (c.mask) cudaFree(c.mask);
+        if (c.block_bytes) cudaFree(c.block_bytes);
+        c = Checkpoint();
     }
 
     bool quiet() const { return (flags & QS_FLAG_QUIET) != 0; }
@@ -1314,6 +1333,63 @@ qs_status qs_expectation_pauli(qs_state *h, const uint64_t *x_masks, const uint6
     return rs;
 }
 
+// ---- device checkpoints of the compressed store
+qs_status qs_checkpoint(qs_state *h, uint32_t slot) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (slot >= 64) return fail(h, QS_ERR_ARG, "checkpoint slot must be < 64");
+    if (h->ckpt.size() <= slot) h->ckpt.resize(slot + 1);
+    auto &c = h->ckpt[slot];
+    const uint64_t meta_bytes = h->nchunks * sizeof(qs::ChunkMeta);
+    if (!c.meta) {
+        CUDA_TRY(h, cudaMalloc(&c.meta, meta_bytes));
+        CUDA_TRY(h, cudaMalloc(&c.mask, h->nb));
+        CUDA_TRY(h, cudaMalloc(&c.block_bytes, h->nb * sizeof(unsigned long long)));
+    }
+    if (c.arena_cap < h->arena_used) {
+        if (c.arena) cudaFree(c.arena);
+        c.arena = nullptr;
+        c.arena_cap = 0;
+        const uint64_t cap = std::max<uint64_t>(128, (h->arena_used + 127) / 128 * 128);
+        cudaError_t e = cudaMalloc(&c.arena, cap);
+        if (e != cudaSuccess)
+            return fail(h, e == cudaErrorMemoryAllocation ? QS_ERR_CAPACITY : QS_ERR_CUDA,
+                        std::string("checkpoint: ") + cudaGetErrorString(e));
+        c.arena_cap = cap;
+    }
+    cudaStream_t s = h->stream;
+    CUDA_TRY(h, cudaMemcpyAsync(c.meta, h->meta[h->cur], meta_bytes, cudaMemcpyDeviceToDevice, s));
+    if (h->arena_used)
+        CUDA_TRY(h, cudaMemcpyAsync(c.arena, h->arena[h->cur], h->arena_used, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(h, cudaMemcpyAsync(c.mask, h->mask, h->nb, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(h, cudaMemcpyAsync(c.block_bytes, h->block_bytes, h->nb * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToDevice, s));
+    c.used = h->arena_used;
+    c.history = h->history;
+    return QS_OK;
+}
+
+qs_status qs_restore(qs_state *h, uint32_t slot) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (slot >= h->ckpt.size() || !h->ckpt[slot].meta) return fail(h, QS_ERR_STATE, "no checkpoint in this slot");
+    auto &c = h->ckpt[slot];
+    cudaStream_t s = h->stream;
+    CUDA_TRY(h, cudaMemcpyAsync(h->meta[h->cur], c.meta, h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyDeviceToDevice, s));
+    if (c.used) CUDA_TRY(h, cudaMemcpyAsync(h->arena[h->cur], c.arena, c.used, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(h, cudaMemcpyAsync(h->mask, c.mask, h->nb, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(h, cudaMemcpyAsync(h->block_bytes, c.block_bytes, h->nb * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
+    h->arena_used = c.used;
+    h->history = c.history;
+    return QS_OK;
+}
+
+qs_status qs_free_checkpoint(qs_state *h, uint32_t slot) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (slot < h->ckpt.size()) qs_state::free_checkpoint(h->ckpt[slot]);
+    return QS_OK;
+}
+
 // ---- store serialisation
 struct StoreHeader {
     char magic[8];
@@ -1693,6 +1769,193 @@ qs_status qs_dense_expectation_pauli(qs_dense *h, const uint64_t *x_masks, const
     if (dt) cudaFree(dt);
     if (dout) cudaFree(dout);
     if (e != cudaSuccess) return dfail(h, QS_ERR_CUDA, std::string("expectation: ") + cudaGetErrorString(e));
+    return QS_OK;
+}
+
+qs_status qs_dense_copy(qs_dense *dst, const qs_dense *src) {
+    if (!dst || !src) return dfail(dst, QS_ERR_ARG, "NULL handle");
+    if (dst->n != src->n || dst->f64 != src->f64) return dfail(dst, QS_ERR_ARG, "states differ in size or dtype");
+    CUDA_TRY(dst, cudaMemcpyAsync(dst->state, src->state, dst->dim() * dst->amp_bytes(), cudaMemcpyDeviceToDevice,
+                                  dst->stream));
+    CUDA_TRY(dst, cudaStreamSynchronize(dst->stream));
+    return QS_OK;
+}
+
+static qs_status pauli_terms(qs_dense *h, const uint64_t *x, const uint64_t *z, size_t nterms,
+                             std::vector<qs::PauliTerm> *out) {
+    const uint64_t full = h->n >= 64 ? ~0ull : ((1ull << h->n) - 1);
+    out->resize(nterms);
+    for (size_t t = 0; t < nterms; ++t) {
+        if ((x[t] | z[t]) & ~full) return dfail(h, QS_ERR_ARG, "Pauli term acts outside the register");
+        (*out)[t] = qs::PauliTerm{};
+        (*out)[t].xg = x[t];
+        (*out)[t].zg = z[t];
+    }
+    return QS_OK;
+}
+
+qs_status qs_dense_apply_pauli_sum(qs_dense *out, const qs_dense *in, const uint64_t *x_masks, const uint64_t *z_masks,
+                                   const double *coefs, size_t nterms) {
+    if (!out || !in || (nterms && (!x_masks || !z_masks || !coefs))) return dfail(out, QS_ERR_ARG, "NULL argument");
+    if (out == in) return dfail(out, QS_ERR_ARG, "in and out must be different states");
+    if (out->n != in->n || out->f64 != in->f64) return dfail(out, QS_ERR_ARG, "states differ in size or dtype");
+    std::vector<qs::PauliTerm> pts;
+    qs_status st = pauli_terms(out, x_masks, z_masks, nterms, &pts);
+    if (st != QS_OK) return st;
+    qs::PauliTerm *dt = nullptr;
+    double *dc = nullptr;
+    cudaError_t e = cudaMalloc(&dt, std::max<size_t>(1, nterms) * sizeof(qs::PauliTerm));
+    if (e == cudaSuccess) e = cudaMalloc(&dc, std::max<size_t>(1, 2 * nterms) * sizeof(double));
+    if (e == cudaSuccess && nterms)
+        e = cudaMemcpyAsync(dt, pts.data(), nterms * sizeof(qs::PauliTerm), cudaMemcpyHostToDevice, out->stream);
+    if (e == cudaSuccess && nterms)
+        e = cudaMemcpyAsync(dc, coefs, 2 * nterms * sizeof(double), cudaMemcpyHostToDevice, out->stream);
+    if (e == cudaSuccess)
+        e = qs::launch_dense_pauli_sum(out->f64, in->state, out->state, (int)out->n, dt, dc, (int)nterms, out->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(out->stream);
+    if (dt) cudaFree(dt);
+    if (dc) cudaFree(dc);
+    if (e != cudaSuccess) return dfail(out, QS_ERR_CUDA, std::string("apply_pauli_sum: ") + cudaGetErrorString(e));
+    return QS_OK;
+}
+
+qs_status qs_dense_transition_pauli(const qs_dense *bra, qs_dense *ket, const uint64_t *x_masks,
+                                    const uint64_t *z_masks, size_t nterms, double *out) {
+    if (!bra || !ket || (nterms && (!x_masks || !z_masks || !out))) return dfail(ket, QS_ERR_ARG, "NULL argument");
+    if (bra->n != ket->n || bra->f64 != ket->f64) return dfail(ket, QS_ERR_ARG, "states differ in size or dtype");
+    std::vector<qs::PauliTerm> pts;
+    qs_status st = pauli_terms(ket, x_masks, z_masks, nterms, &pts);
+    if (st != QS_OK || !nterms) return st;
+    qs::PauliTerm *dt = nullptr;
+    double *dout = nullptr;
+    cudaError_t e = cudaMalloc(&dt, nterms * sizeof(qs::PauliTerm));
+    if (e == cudaSuccess) e = cudaMalloc(&dout, 2 * nterms * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt, pts.data(), nterms * sizeof(qs::PauliTerm), cudaMemcpyHostToDevice, ket->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dout, 0, 2 * nterms * sizeof(double), ket->stream);
+    for (size_t t0 = 0; t0 < nterms && e == cudaSuccess; t0 += 256) {
+        const int cnt = (int)std::min<size_t>(256, nterms - t0);
+        e = qs::launch_dense_transition(ket->f64, bra->state, ket->state, (int)ket->n, dt + t0, cnt, dout + 2 * t0,
+                                        ket->stream);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, 2 * nterms * sizeof(double), cudaMemcpyDeviceToHost, ket->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ket->stream);
+    if (dt) cudaFree(dt);
+    if (dout) cudaFree(dout);
+    if (e != cudaSuccess) return dfail(ket, QS_ERR_CUDA, std::string("transition: ") + cudaGetErrorString(e));
+    return QS_OK;
+}
+
+// Fused adjoint backward sweep over psi and lam (see qompsim.h).
+qs_status qs_dense_adjoint(qs_dense *psi, qs_dense *lam, const qs_gate *gates, const int32_t *slots,
+                           const uint64_t *gen_x, const uint64_t *gen_z, size_t count, double *out, uint32_t nslots) {
+    if (!psi || !lam || (count && (!gates || !slots || !gen_x || !gen_z)) || (nslots && !out))
+        return dfail(psi, QS_ERR_ARG, "NULL argument");
+    if (psi == lam || psi->n != lam->n || psi->f64 != lam->f64)
+        return dfail(psi, QS_ERR_ARG, "psi and lam must be distinct states of one size and dtype");
+    if (psi->stream != lam->stream) return dfail(psi, QS_ERR_ARG, "psi and lam must share a stream");
+    for (size_t i = 0; i < count; ++i)
+        if (slots[i] >= (int32_t)nslots) return dfail(psi, QS_ERR_ARG, "slot index out of range");
+    std::vector<CGate> cg;
+    qs_status st = dense_canon(psi, gates, count, &cg);
+    if (st != QS_OK) return st;
+    const int n = (int)psi->n;
+    const int C = std::min(n, 5);
+    const int tile_log2 = std::min(n, std::min(psi->f64 ? 11 : 12, C + qs::kMaxTileQubits));
+    const int jmax = tile_log2 - C;
+    // generators' flip qubits must lie in the tile too: treat them as mixing
+    for (size_t i = 0; i < count; ++i)
+        if (slots[i] >= 0)
+            for (int b = 0; b < cg[i].nq; ++b)
+                if ((gen_x[i] >> cg[i].q[b]) & 1) cg[i].mix[b] = true;
+    for (size_t i = 0; i < count; ++i) {
+        uint64_t covered = 0;
+        for (int b = 0; b < cg[i].nq; ++b) covered |= 1ull << cg[i].q[b];
+        if (slots[i] >= 0 && (gen_x[i] & ~covered))
+            return dfail(psi, QS_ERR_ARG, "a generator flips a qubit its gate does not act on");
+    }
+    std::vector<uint32_t> ids(count);
+    for (size_t i = 0; i < count; ++i) ids[i] = (uint32_t)i;
+    auto pl = plan_passes(ids, cg, C, jmax, std::min(jmax, 3), C, n);
+    std::vector<double> acc(2 * (size_t)nslots, 0.0);
+    double *dout = nullptr;
+    qs::AdjGate *dg = nullptr;
+    cudaError_t e = cudaSuccess;
+    for (auto &p : pl) {
+        // local slots of this pass (at most 128)
+        for (size_t g0 = 0; g0 < p.gates.size() && e == cudaSuccess;) {
+            std::vector<qs::AdjGate> ag;
+            std::vector<int32_t> local_to_global;
+            size_t g1 = g0;
+            for (; g1 < p.gates.size(); ++g1) {
+                const uint32_t gi = p.gates[g1];
+                if (slots[gi] >= 0 && local_to_global.size() >= 128) break;
+                qs::AdjGate a{};
+                a.g = to_kgate(cg[gi], p.tile, C);
+                a.slot = -1;
+                if (slots[gi] >= 0) {
+                    a.slot = (int32_t)local_to_global.size();
+                    local_to_global.push_back(slots[gi]);
+                    uint32_t xt = 0, zt = 0;
+                    uint64_t zo = 0;
+                    for (int q = 0; q < n; ++q) {
+                        int tp = q < C ? q : -1;
+                        if (q >= C) {
+                            auto it = std::find(p.tile.begin(), p.tile.end(), q);
+                            if (it != p.tile.end()) tp = C + (int)(it - p.tile.begin());
+                        }
+                        if ((gen_x[gi] >> q) & 1) xt |= 1u << tp;  // flip qubits are in the tile
+                        if ((gen_z[gi] >> q) & 1) {
+                            if (tp >= 0) zt |= 1u << tp;
+                            else zo |= 1ull << q;
+                        }
+                    }
+                    a.gen.xt = xt;
+                    a.gen.zt = zt;
+                    a.gen.zo = zo;
+                }
+                ag.push_back(a);
+            }
+            const size_t ns = local_to_global.size();
+            if (dg) cudaFree(dg);
+            if (dout) cudaFree(dout);
+            dg = nullptr;
+            dout = nullptr;
+            e = cudaMalloc(&dg, std::max<size_t>(1, ag.size()) * sizeof(qs::AdjGate));
+            if (e == cudaSuccess) e = cudaMalloc(&dout, std::max<size_t>(1, 2 * ns) * sizeof(double));
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(dg, ag.data(), ag.size() * sizeof(qs::AdjGate), cudaMemcpyHostToDevice, psi->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(dout, 0, std::max<size_t>(1, 2 * ns) * sizeof(double), psi->stream);
+            if (e == cudaSuccess) {
+                qs::AdjPassArgs a{};
+                a.n = n;
+                a.C = C;
+                a.j = (int)p.tile.size();
+                for (int k = 0; k < a.j; ++k) a.tq[k] = p.tile[k] - C;
+                a.n_tiles = uint64_t(1) << (n - C - a.j);
+                a.gates = dg;
+                a.ngates = (int)ag.size();
+                a.psi = psi->state;
+                a.lam = lam->state;
+                a.out = dout;
+                a.nslots = (int)ns;
+                e = qs::launch_adjoint_pass(psi->f64, a, psi->stream);
+            }
+            std::vector<double> h(2 * ns);
+            if (e == cudaSuccess && ns)
+                e = cudaMemcpyAsync(h.data(), dout, 2 * ns * sizeof(double), cudaMemcpyDeviceToHost, psi->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(psi->stream);
+            if (e == cudaSuccess)
+                for (size_t k = 0; k < ns; ++k) {
+                    acc[2 * local_to_global[k]] += h[2 * k];
+                    acc[2 * local_to_global[k] + 1] += h[2 * k + 1];
+                }
+            g0 = g1;
+        }
+    }
+    if (dg) cudaFree(dg);
+    if (dout) cudaFree(dout);
+    if (e != cudaSuccess) return dfail(psi, QS_ERR_CUDA, std::string("adjoint: ") + cudaGetErrorString(e));
+    for (size_t i = 0; i < acc.size(); ++i) out[i] = acc[i];
     return QS_OK;
 }
 

@@ -140,10 +140,13 @@ class ParametricQuantumCircuit(QuantumCircuit):
         c._param_pos = list(self._param_pos)
         return c
 
-    def _add_param(self, g: ParametricRotationGate):
+    def _add_param(self, g):
         self._param_pos.append(len(self._gates))
         self._check(g)
         self._gates.append(g.copy())
+
+    def add_parametric_multi_Pauli_rotation_gate(self, targets, pauli_ids, angle):
+        self._add_param(gate.ParametricPauliRotation(targets, pauli_ids, angle))
 
     def add_parametric_RX_gate(self, i, angle): self._add_param(gate.ParametricRX(i, angle))
     def add_parametric_RY_gate(self, i, angle): self._add_param(gate.ParametricRY(i, angle))
@@ -153,7 +156,7 @@ class ParametricQuantumCircuit(QuantumCircuit):
         if position is not None and position < len(self._gates):
             self._param_pos = [p + 1 if p >= position else p for p in self._param_pos]
         super().add_gate(g, position)
-        if isinstance(g, ParametricRotationGate):
+        if g.is_parametric():
             self._param_pos.append(len(self._gates) - 1 if position is None else position)
             self._param_pos.sort()
 
@@ -516,6 +519,16 @@ class CompressedQuantumState:
         st = _n.qs_stats()
         self._check(_n.lib().qs_get_stats(self._h, _n.ct.byref(st)))
         return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def checkpoint(self, slot: int = 0) -> None:
+        """Copy the compressed store into device checkpoint `slot`."""
+        self._check(_n.lib().qs_checkpoint(self._h, int(slot)))
+
+    def restore(self, slot: int = 0) -> None:
+        self._check(_n.lib().qs_restore(self._h, int(slot)))
+
+    def free_checkpoint(self, slot: int = 0) -> None:
+        self._check(_n.lib().qs_free_checkpoint(self._h, int(slot)))
 
     def export_store(self) -> bytes:
         size = _n.ct.c_uint64()

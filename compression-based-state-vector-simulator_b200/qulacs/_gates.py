@@ -130,9 +130,10 @@ class QuantumGateBase:
 
     def get_inverse(self) -> "QuantumGateBase":
         g = self.copy()
-        g._matrix = self._matrix.conj().T.copy()
-        if isinstance(g, ParametricRotationGate):
-            g._angle = -self._angle
+        if hasattr(g, "_angle") and hasattr(g, "set_parameter_value"):
+            g.set_parameter_value(-self._angle)
+        else:
+            g._matrix = self.get_matrix().conj().T.copy()
         return g
 
     def update_quantum_state(self, state) -> None:
@@ -188,6 +189,65 @@ class ParametricRotationGate(QuantumGateBase):
     @property
     def axis(self) -> str:
         return self._axis
+
+    def generator_masks(self):
+        """(flip mask, sign mask, #Y) of the generator P of exp(i theta/2 P)."""
+        q = 1 << self.get_target_index_list()[0]
+        return {"X": (q, 0, 0), "Y": (q, q, 1), "Z": (0, q, 0)}[self._axis]
+
+
+_PAULI_1Q = {
+    1: np.array([[0, 1], [1, 0]], dtype=np.complex128),
+    2: np.array([[0, -1j], [1j, 0]], dtype=np.complex128),
+    3: np.array([[1, 0], [0, -1]], dtype=np.complex128),
+}
+_PAULI_PROP = {1: FLAG_X_COMMUTE, 2: FLAG_Y_COMMUTE, 3: FLAG_Z_COMMUTE}
+
+
+def pauli_matrix(pauli_ids) -> np.ndarray:
+    """Matrix of a Pauli string; matrix bit i <-> the i-th listed qubit."""
+    m = np.eye(1, dtype=np.complex128)
+    for pid in pauli_ids:
+        m = np.kron(_PAULI_1Q[int(pid)], m)
+    return m
+
+
+class ParametricPauliRotationGate(QuantumGateBase):
+    """exp(i theta/2 P) for a Pauli string P (src/vqcsim/parametric_gate.hpp:213+,
+    matrix cos(theta/2) I + i sin(theta/2) P as src/cppsim/gate_named_pauli.hpp:221-226)."""
+
+    def __init__(self, targets, pauli_ids, angle: float):
+        self._pids = [int(p) for p in pauli_ids]
+        if len(self._pids) != len(targets) or any(p not in (1, 2, 3) for p in self._pids):
+            raise ValueError("pauli_ids must list 1 (X), 2 (Y) or 3 (Z) per target")
+        self._angle = float(angle)
+        tl = [TargetQubitInfo(t, _PAULI_PROP[p]) for t, p in zip(targets, self._pids)]
+        super().__init__("ParametricPauliRotation", tl, [], self._mat(), FLAG_PARAMETRIC)
+
+    def _mat(self):
+        P = pauli_matrix(self._pids)
+        c, s_ = math.cos(self._angle / 2), math.sin(self._angle / 2)
+        return c * np.eye(P.shape[0], dtype=np.complex128) + 1j * s_ * P
+
+    def get_parameter_value(self) -> float:
+        return self._angle
+
+    def set_parameter_value(self, value: float) -> None:
+        self._angle = float(value)
+        self._matrix = self._mat()
+
+    def get_matrix(self) -> np.ndarray:
+        return self._mat()
+
+    def generator_masks(self):
+        xm = zm = ny = 0
+        for t, p in zip(self.get_target_index_list(), self._pids):
+            if p in (1, 2):
+                xm |= 1 << t
+            if p in (2, 3):
+                zm |= 1 << t
+            ny += p == 2
+        return xm, zm, ny
 
 
 def _rotation_matrix(axis: str, angle: float) -> np.ndarray:

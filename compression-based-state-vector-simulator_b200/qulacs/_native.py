@@ -99,6 +99,12 @@ SIGNATURES = [
     ("qs_norm_squared", ct.c_int, [_P, ct.POINTER(_D)]),
     ("qs_expectation_pauli", ct.c_int, [_P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
     ("qs_dense_expectation_pauli", ct.c_int, [_P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
+    ("qs_dense_copy", ct.c_int, [_P, _P]),
+    ("qs_dense_apply_pauli_sum", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_U64), ct.POINTER(_D), ct.c_size_t]),
+    ("qs_dense_transition_pauli", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t,
+                                             ct.POINTER(_D)]),
+    ("qs_dense_adjoint", ct.c_int, [_P, _P, ct.POINTER(qs_gate), ct.POINTER(ct.c_int32), ct.POINTER(_U64),
+                                    ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D), _U32]),
     ("qs_get_zero_mask", ct.c_int, [_P, ct.POINTER(ct.c_uint8)]),
     ("qs_get_block_bytes", ct.c_int, [_P, ct.POINTER(_U64)]),
     ("qs_get_max_sv_bytes", ct.c_int, [_P, ct.POINTER(_U64)]),
@@ -107,6 +113,9 @@ SIGNATURES = [
     ("qs_get_stats", ct.c_int, [_P, ct.POINTER(qs_stats)]),
     ("qs_export_store", ct.c_int, [_P, _P, _U64, ct.POINTER(_U64)]),
     ("qs_import_store", ct.c_int, [_P, _P, _U64]),
+    ("qs_checkpoint", ct.c_int, [_P, _U32]),
+    ("qs_restore", ct.c_int, [_P, _U32]),
+    ("qs_free_checkpoint", ct.c_int, [_P, _U32]),
     ("qs_set_basis_state", ct.c_int, [_P, _U64]),
     ("qs_load_vector", ct.c_int, [_P, ct.POINTER(_D)]),
     ("qs_dense_create", ct.c_int, [ct.POINTER(_P), _U32, ct.c_int]),

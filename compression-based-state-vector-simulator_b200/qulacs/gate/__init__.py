@@ -4,8 +4,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from .._gates import (ParametricRotationGate, QuantumGateBase, QuantumGateMatrix, cnot, cz, ibmq_matrix,
-                      merge, one_qubit_named, rotation, swap, to_matrix_gate)
+from .._gates import (ParametricPauliRotationGate, ParametricRotationGate, QuantumGateBase, QuantumGateMatrix, cnot,
+                      cz, ibmq_matrix, merge, one_qubit_named, rotation, swap, to_matrix_gate)
 
 
 def Identity(index: int) -> QuantumGateBase:
@@ -148,6 +148,10 @@ def ParametricRY(index: int, angle: float = 0.0) -> ParametricRotationGate:
 
 def ParametricRZ(index: int, angle: float = 0.0) -> ParametricRotationGate:
     return ParametricRotationGate("Z", index, angle)
+
+
+def ParametricPauliRotation(targets, pauli_ids, angle: float = 0.0) -> ParametricPauliRotationGate:
+    return ParametricPauliRotationGate(targets, pauli_ids, angle)
 
 
 __all__ = [n for n in dir() if not n.startswith("_") and n not in ("np",)]

@@ -1,0 +1,144 @@
+"""qulacs.torch -- energies and adjoint gradients of parametric circuits, and
+a torch.autograd.Function over them.
+
+energy_and_gradient(circuit, observable) runs the circuit on a device state,
+evaluates <psi|H|psi> (FP64 reductions), builds lam = H psi and walks the
+circuit backwards with the fused dual-state adjoint pass (qs_dense_adjoint):
+for a rotation U_k = exp(i theta_k/2 P_k),
+    dE/dtheta_k = 2 Re <lam_k| (i/2) P_k |psi_k> = -Im <lam_k|P_k|psi_k>,
+with lam_k = (U_N ... U_{k+1})^dagger H psi_N and psi_k the state after U_k.
+This is the reference's state/bistate backprop
+(src/vqcsim/parametric_circuit.cpp:180-306) on the GPU; the reference has no
+gradient on its compressed state.  Each pass of the backward sweep reads and
+writes both states once.
+
+parameter_shift_gradient gives the +-pi/2 shift rule of the reference's
+GradCalculator (src/vqcsim/GradCalculator.cpp:8-44) on the same device path,
+as an independent check.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from typing import Callable, Optional, Sequence
+
+import numpy as np
+
+from . import _native as _n
+from . import QuantumState, Observable
+
+
+def _masks_arrays(xs, zs):
+    xa = np.ascontiguousarray(np.asarray(xs, dtype=np.uint64))
+    za = np.ascontiguousarray(np.asarray(zs, dtype=np.uint64))
+    return xa, za
+
+
+def apply_observable(out: QuantumState, state: QuantumState, observable: Observable) -> None:
+    """out := H state (Observable.apply_to_state of the reference)."""
+    xs, zs, nys, coefs = observable.term_masks()
+    c = np.array([complex(cf) * (1j ** ny) for cf, ny in zip(coefs, nys)], dtype=np.complex128)
+    xa, za = _masks_arrays(xs, zs)
+    L = _n.lib()
+    out._check(L.qs_dense_apply_pauli_sum(out._h, state._h, xa.ctypes.data_as(ct.POINTER(ct.c_uint64)),
+                                          za.ctypes.data_as(ct.POINTER(ct.c_uint64)),
+                                          c.view(np.float64).ctypes.data_as(ct.POINTER(ct.c_double)), len(xs)))
+
+
+def energy_and_gradient(circuit, observable: Observable, dtype="complex128"):
+    """(E, dE/dtheta) for every parametric gate of `circuit`, in the order of
+    circuit parameters (get_parameter(i))."""
+    n = circuit.get_qubit_count()
+    psi = QuantumState(n, dtype=dtype)
+    circuit.update_quantum_state(psi)
+    energy = observable.get_expectation_value(psi)
+    lam = QuantumState(n, dtype=dtype)
+    apply_observable(lam, psi, observable)
+
+    gates = circuit._gates
+    param_pos = list(getattr(circuit, "_param_pos", []))
+    slot_of = {pos: i for i, pos in enumerate(param_pos)}
+    back, slots, gx, gz, gny = [], [], [], [], []
+    for k in reversed(range(len(gates))):
+        g = gates[k]
+        back.append(g.get_inverse())
+        if k in slot_of:
+            xm, zm, ny = g.generator_masks()
+            slots.append(slot_of[k])
+            gx.append(xm)
+            gz.append(zm)
+            gny.append(ny)
+        else:
+            slots.append(-1)
+            gx.append(0)
+            gz.append(0)
+            gny.append(0)
+    nslots = len(param_pos)
+    arr = _n.make_gate_array(back)
+    sl = np.ascontiguousarray(np.asarray(slots, dtype=np.int32))
+    xa, za = _masks_arrays(gx, gz)
+    out = np.zeros(2 * max(1, nslots), dtype=np.float64)
+    L = _n.lib()
+    psi._check(L.qs_dense_adjoint(psi._h, lam._h, arr, sl.ctypes.data_as(ct.POINTER(ct.c_int32)),
+                                  xa.ctypes.data_as(ct.POINTER(ct.c_uint64)),
+                                  za.ctypes.data_as(ct.POINTER(ct.c_uint64)), len(back),
+                                  out.ctypes.data_as(ct.POINTER(ct.c_double)), nslots))
+    sums = out[0:2 * nslots:2] + 1j * out[1:2 * nslots:2]
+    ny_of_slot = np.zeros(nslots, dtype=np.int64)
+    for s_, ny in zip(slots, gny):
+        if s_ >= 0:
+            ny_of_slot[s_] = ny
+    grads = -np.imag((1j ** ny_of_slot) * sums)
+    return float(energy), grads
+
+
+def energy(circuit, observable: Observable, dtype="complex128") -> float:
+    psi = QuantumState(circuit.get_qubit_count(), dtype=dtype)
+    circuit.update_quantum_state(psi)
+    return observable.get_expectation_value(psi)
+
+
+def parameter_shift_gradient(circuit, observable: Observable, dtype="complex128") -> np.ndarray:
+    """+-pi/2 shift rule per circuit parameter (GradCalculator.cpp:8-44)."""
+    c = circuit.copy()
+    out = np.zeros(c.get_parameter_count())
+    for i in range(c.get_parameter_count()):
+        t = c.get_parameter(i)
+        c.set_parameter(i, t + np.pi / 2)
+        ep = energy(c, observable, dtype)
+        c.set_parameter(i, t - np.pi / 2)
+        em = energy(c, observable, dtype)
+        c.set_parameter(i, t)
+        out[i] = 0.5 * (ep - em)
+    return out
+
+
+try:
+    import torch as _torch
+
+    class CircuitEnergyFunction(_torch.autograd.Function):
+        """E(params) = <psi(params)|H|psi(params)> with the adjoint gradient.
+
+        builder(params: np.ndarray) -> (ParametricQuantumCircuit, jac) where
+        jac[i, j] = d(circuit parameter i)/d(params j), or just the circuit
+        when its parameters are `params` themselves."""
+
+        @staticmethod
+        def forward(ctx, params, builder: Callable, observable: Observable, dtype: str = "complex128"):
+            p = params.detach().cpu().numpy().astype(np.float64)
+            built = builder(p)
+            circuit, jac = (built if isinstance(built, tuple) else (built, None))
+            e, g = energy_and_gradient(circuit, observable, dtype)
+            if jac is not None:
+                g = np.asarray(jac, dtype=np.float64).T @ g
+            ctx.save_for_backward(_torch.as_tensor(g, dtype=_torch.float64))
+            return _torch.tensor(e, dtype=_torch.float64)
+
+        @staticmethod
+        def backward(ctx, grad_out):
+            (g,) = ctx.saved_tensors
+            return grad_out * g.to(grad_out.device), None, None, None
+
+    def circuit_energy(params, builder, observable, dtype="complex128"):
+        return CircuitEnergyFunction.apply(params, builder, observable, dtype)
+except ImportError:  # torch is optional for the rest of the package
+    pass

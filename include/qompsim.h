@@ -212,6 +212,16 @@ qs_status qs_get_stats(qs_state *h, qs_stats *out);
 qs_status qs_export_store(qs_state *h, void *buf, uint64_t cap, uint64_t *size);
 qs_status qs_import_store(qs_state *h, const void *buf, uint64_t size);
 
+/* Device-side checkpoints of the compressed store (zero mask, per-block
+ * bytes, chunk headers and the payload in use): qs_checkpoint copies the
+ * current store into slot (0..63, allocated on first use, regrown when the
+ * store has grown), qs_restore copies it back.  The reference has no
+ * checkpoint of its compressed state; these are the stage checkpoints of
+ * the adjoint and a cheap way to rerun a circuit from a saved state. */
+qs_status qs_checkpoint(qs_state *h, uint32_t slot);
+qs_status qs_restore(qs_state *h, uint32_t slot);
+qs_status qs_free_checkpoint(qs_state *h, uint32_t slot);
+
 /* Reset to |basis> (basis < 2^n); the reference only has |0...0>. */
 qs_status qs_set_basis_state(qs_state *h, uint64_t basis);
 
@@ -244,6 +254,34 @@ qs_status qs_dense_norm_squared(qs_dense *h, double *out);
 /* The same Pauli expectation sums on the uncompressed state. */
 qs_status qs_dense_expectation_pauli(qs_dense *h, const uint64_t *x_masks, const uint64_t *z_masks, size_t nterms,
                                      double *out);
+
+/* dst := src (same size and dtype). */
+qs_status qs_dense_copy(qs_dense *dst, const qs_dense *src);
+
+/* out := sum_t c_t P_t in, P_t the Pauli string with flip mask x_masks[t] and
+ * sign mask z_masks[t] acting as P|y> = (-1)^{|y & z|} |y ^ x|; coefs holds
+ * the complex c_t (interleaved re, im), with any i^(number of Y) folded in.
+ * Observable::apply_to_state of the reference (used by its backprop,
+ * src/vqcsim/parametric_circuit.cpp:268-306). */
+qs_status qs_dense_apply_pauli_sum(qs_dense *out, const qs_dense *in, const uint64_t *x_masks,
+                                   const uint64_t *z_masks, const double *coefs, size_t nterms);
+
+/* Transition sums out[2t] + i out[2t+1] = sum_x conj(bra[x ^ x_t]) (-1)^{|x & z_t|} ket[x]. */
+qs_status qs_dense_transition_pauli(const qs_dense *bra, qs_dense *ket, const uint64_t *x_masks,
+                                    const uint64_t *z_masks, size_t nterms, double *out);
+
+/* Adjoint backward sweep over two states (reverse-mode differentiation of a
+ * parametric circuit; the reference's backprop_inner_product,
+ * src/vqcsim/parametric_circuit.cpp:180-266, restated as fused tile passes).
+ * gates[0..count) are applied in order to both psi and lam -- the caller
+ * lists the inverse gates U_k^dagger in reverse circuit order.  Before gate
+ * i with slots[i] >= 0, the sums sum_x conj(lam[x ^ gen_x[i]])
+ * (-1)^{|x & gen_z[i]|} psi[x] are added to out[2 slot] + i out[2 slot + 1]
+ * (nslots slots, zeroed by the call).  For a rotation exp(i theta/2 P) the
+ * derivative of <psi|H|psi> is then -Im(i^(number of Y in P) * sum). */
+qs_status qs_dense_adjoint(qs_dense *psi, qs_dense *lam, const qs_gate *gates, const int32_t *slots,
+                           const uint64_t *gen_x, const uint64_t *gen_z, size_t count, double *out,
+                           uint32_t nslots);
 
 /* Device pointer of the amplitudes (interleaved re, im of the dtype). */
 qs_status qs_dense_device_ptr(qs_dense *h, void **out);

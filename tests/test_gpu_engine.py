@@ -320,3 +320,32 @@ def test_reference_controls_flag(qulacs_mod):
     o.apply(c._gates, st, maps, counts)
     assert np.abs(quirk.get_vector() - o.vector()).max() < 1e-5
     assert np.abs(quirk.get_vector() - ref).max() > 0.1
+
+
+def test_checkpoint_restore(qulacs_mod):
+    from qompsim import circuits as C
+    from qulacs import _native
+    c = helpers.optimized(C.qft_basis(13, 4), 7)
+    cq = qulacs_mod.CompressedQuantumState(13, 7, flags=_native.QS_FLAG_QUIET)
+    cq.partition_and_register_circuit(c, 3, 0)
+    cq.set_computational_basis(5)
+    cq.checkpoint(2)
+    v0 = cq.get_vector(renormalize=False)
+    cq.apply_circuit()
+    v1 = cq.get_vector(renormalize=False)
+    cq.restore(2)
+    assert np.array_equal(cq.get_vector(renormalize=False), v0)
+    cq.apply_circuit()
+    assert np.array_equal(cq.get_vector(renormalize=False), v1)   # deterministic rerun from the checkpoint
+    with pytest.raises(_native.QompsimError) as e:
+        cq.restore(9)
+    assert e.value.status == _native.QS_ERR_STATE
+
+
+def test_run_sim_one_rank_fidelity(qulacs_mod, capsys):
+    from qompsim import run_sim
+    run_sim.run_sim("fidelity", "qft_basis", 12, block_size=6, inner_size=3)
+    out = capsys.readouterr().out
+    fid = float(out.split("Fidelity:")[1].split()[0])
+    assert fid > 0.999
+    assert "Circuit Stages: [" in out
