@@ -302,6 +302,30 @@ def run_ours(args, spec):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(pg, torch, e0.elapsed_time(e1))
 
+    # ---- the plain uncompressed per-gate path on the same gates (rank 0, N=1 only): one kernel per gate
+    # over the whole complex128 vector, and this package's fused uncompressed tile passes beside it
+    dense = None
+    if rank == 0 and world == 1 and not args.no_dense:
+        gates = list(circuit._gates)
+        ds = qulacs.QuantumState(spec["n"], dtype="complex128")
+        legs = {}
+        for name, pergate in (("pergate_c128", True), ("fused_dense_c128", False)):
+            ds.set_computational_basis(0)
+            ds._apply_gates(gates, pergate=pergate)       # warm-up
+            torch.cuda.synchronize()
+            d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            d0.record()
+            ds.set_computational_basis(0)
+            ds._apply_gates(gates, pergate=pergate)
+            d1.record()
+            torch.cuda.synchronize()
+            dms = d0.elapsed_time(d1)
+            legs[name] = {"ms_per_step": dms, "value": updates_per_step / (dms * 1e-3), "unit": UNIT,
+                          "launches_per_step": len(gates) if pergate else None}
+        del ds
+        dense = legs
+        dense["compressed_speedup_vs_pergate_c128"] = legs["pergate_c128"]["ms_per_step"] / (ms / args.steps)
+
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -341,6 +365,7 @@ def run_ours(args, spec):
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "uncompressed": dense,
         }
         print(json.dumps(out))
     if pg is not None:
@@ -355,6 +380,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="qft30")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-dense", action="store_true", help="skip the uncompressed per-gate comparison leg")
     args = ap.parse_args()
     spec = workload_spec(args.workload)
     if args.impl == "reference":
