@@ -265,9 +265,9 @@ def run_ours(args, spec):
         for _ in range(args.steps):
             step()
             s = cq.get_stats()
-            pass_ms += s["kernel_ms"]
+            pass_ms += s["kernel_ms"]                         # tile passes (pass_kernel) only
             pass_bytes += int(s["bytes_read"]) + int(s["bytes_written"])
-            passes += int(s["passes"])
+            passes += int(s["passes"]) - int(s["perm_passes"])
         end.record()
         torch.cuda.synchronize()
     ms, value = aggregate(pg, torch, start.elapsed_time(end), updates_per_step, args.steps, world)
@@ -347,6 +347,7 @@ def run_ours(args, spec):
             "data": "synthetic",
             "config": {"workload": describe(spec), "n": spec["n"], "block_size": spec["block_size"],
                        "inner_size": spec["inner_size"], "stages": int(st["stages"]), "passes": int(st["passes"]),
+                       "header_only_passes": int(st["perm_passes"]),
                        "gates": circuit.get_gate_count(), "amp_gate_updates_per_step": updates_per_step,
                        "parallelism": f"replicas x{world}",
                        "l2": "compressed store larger than L2 (126 MB); no flush between steps",

@@ -64,6 +64,19 @@ void reorder_ascending(int k, const int *order, const cplx *in, int *qout, cplx 
         for (int c = 0; c < dim; ++c) out[r * dim + c] = in[map(r) * dim + map(c)];
 }
 
+void compute_mixing(CGate *cg) {
+    const int dim = 1 << cg->nq;
+    for (int b = 0; b < cg->nq; ++b) {
+        bool mx = false;
+        for (int r = 0; r < dim; ++r)
+            for (int c = 0; c < dim; ++c)
+                if ((((r ^ c) >> b) & 1) && cg->m[r * dim + c] != cplx(0.0, 0.0)) mx = true;
+        cg->mix[b] = mx;
+    }
+    if (cg->nq == 1) cg->mix[1] = false;
+    cg->diag = !cg->mix[0] && !(cg->nq == 2 && cg->mix[1]);
+}
+
 bool canonicalize(const qs_gate &g, bool ref_controls, uint32_t n, CGate *cg, std::string *err) {
     const std::string name(g.name, strnlen(g.name, sizeof(g.name)));
     if (name == "FusedSWAP") {
@@ -123,16 +136,151 @@ bool canonicalize(const qs_gate &g, bool ref_controls, uint32_t n, CGate *cg, st
             reorder_ascending(2, order, M, cg->q, cg->m);
         }
     }
-    const int dim = 1 << cg->nq;
-    for (int b = 0; b < cg->nq; ++b) {
-        bool mx = false;
-        for (int r = 0; r < dim; ++r)
-            for (int c = 0; c < dim; ++c)
-                if ((((r ^ c) >> b) & 1) && cg->m[r * dim + c] != cplx(0.0, 0.0)) mx = true;
-        cg->mix[b] = mx;
-    }
-    cg->diag = !cg->mix[0] && !(cg->nq == 2 && cg->mix[1]);
+    compute_mixing(cg);
     return true;
+}
+
+// A gate whose qubits are all >= C and whose matrix sends every basis state
+// to one basis state with coefficient exactly 1 by moving and flipping bits
+// (I, X, SWAP and their products): it permutes whole chunks.  *swap: the
+// gate exchanges its two qubits; *flip: matrix bits flipped after that.
+bool chunk_perm_gate(const CGate &g, int C, bool *swap, int *flip) {
+    for (int i = 0; i < g.nq; ++i)
+        if (g.q[i] < C) return false;
+    const int dim = 1 << g.nq;
+    int f[4];
+    for (int c = 0; c < dim; ++c) {
+        f[c] = -1;
+        for (int r = 0; r < dim; ++r) {
+            const cplx v = g.m[r * dim + c];
+            if (v == cplx(1.0, 0.0)) {
+                if (f[c] >= 0) return false;
+                f[c] = r;
+            } else if (v != cplx(0.0, 0.0)) {
+                return false;
+            }
+        }
+        if (f[c] < 0) return false;
+    }
+    const int x = f[0];
+    *flip = x;
+    if (g.nq == 1) {
+        *swap = false;
+        return f[1] == (1 ^ x);
+    }
+    if ((f[1] ^ x) == 1 && (f[2] ^ x) == 2 && (f[3] ^ x) == 3) {
+        *swap = false;
+        return true;
+    }
+    if ((f[1] ^ x) == 2 && (f[2] ^ x) == 1 && (f[3] ^ x) == 3) {
+        *swap = true;
+        return true;
+    }
+    return false;
+}
+
+// Chunk-index permutation sigma(c) = pi(c) ^ x accumulated over the SWAP / X
+// gates of a stage (bits are qubit - C).  The stage's true state is
+// psi_true[sigma(i)] = psi_stored[i]; a later gate G is applied to the stored
+// state as sigma^-1 G sigma (relabel()), and the last pass of the stage
+// writes chunk c to position sigma(c).
+struct HostPerm {
+    std::vector<int> dst;  // dst[s] = pi(s)
+    uint64_t x = 0;
+    explicit HostPerm(int bits) : dst(bits) {
+        for (int s = 0; s < bits; ++s) dst[s] = s;
+    }
+    bool identity() const {
+        if (x) return false;
+        for (size_t s = 0; s < dst.size(); ++s)
+            if (dst[s] != (int)s) return false;
+        return true;
+    }
+    void then_swap(int a, int b) {
+        for (auto &d : dst) {
+            if (d == a) d = b;
+            else if (d == b) d = a;
+        }
+        const uint64_t ba = (x >> a) & 1, bb = (x >> b) & 1;
+        x &= ~((1ull << a) | (1ull << b));
+        x |= (ba << b) | (bb << a);
+    }
+    void then_flip(int a) { x ^= 1ull << a; }
+    int inverse(int q) const {
+        for (size_t s = 0; s < dst.size(); ++s)
+            if (dst[s] == q) return (int)s;
+        return q;
+    }
+    qs::ChunkPerm device() const {
+        qs::ChunkPerm p;
+        std::memset(&p, 0, sizeof(p));
+        p.keep = ~0ull;
+        p.flip = x;
+        for (size_t s = 0; s < dst.size(); ++s) {
+            if (dst[s] == (int)s) continue;
+            p.keep &= ~(1ull << s);
+            p.src[p.nmove] = (int8_t)s;
+            p.dst[p.nmove] = (int8_t)dst[s];
+            ++p.nmove;
+        }
+        return p;
+    }
+};
+
+CGate relabel(const CGate &g, const HostPerm &P, int C);
+
+// The gates of one stage as the device applies them: SWAP / X gates on
+// qubits >= C are folded into P (when enabled) and every other gate is
+// relabelled through the permutation accumulated before it.
+void stage_relabel(const std::vector<CGate> &cgates, const std::vector<uint32_t> &ids, int C, bool enable,
+                   std::vector<CGate> *out, HostPerm *P) {
+    out->clear();
+    for (uint32_t gi : ids) {
+        const CGate &g = cgates[gi];
+        bool sw = false;
+        int fl = 0;
+        if (enable && chunk_perm_gate(g, C, &sw, &fl)) {
+            // the gate acts after the permutation so far: sigma <- gate o sigma
+            if (sw) P->then_swap(g.q[0] - C, g.q[1] - C);
+            for (int i = 0; i < g.nq; ++i)
+                if ((fl >> i) & 1) P->then_flip(g.q[i] - C);
+            continue;
+        }
+        out->push_back(relabel(g, *P, C));
+    }
+}
+
+qs::ChunkPerm identity_perm() {
+    qs::ChunkPerm p;
+    std::memset(&p, 0, sizeof(p));
+    p.keep = ~0ull;
+    return p;
+}
+
+// sigma^-1 G sigma: G on qubit q >= C acts on stored qubit pi^-1(q - C) + C,
+// with the matrix index bit flipped where x has bit q - C.
+CGate relabel(const CGate &g, const HostPerm &P, int C) {
+    CGate o = g;
+    int F = 0;
+    int order[2] = {g.q[0], g.q[1]};
+    for (int i = 0; i < g.nq; ++i) {
+        if (g.q[i] < C) continue;
+        const int b = g.q[i] - C;
+        order[i] = P.inverse(b) + C;
+        if ((P.x >> b) & 1) F |= 1 << i;
+    }
+    const int dim = 1 << g.nq;
+    cplx M[16];
+    for (int r = 0; r < dim; ++r)
+        for (int c = 0; c < dim; ++c) M[r * dim + c] = g.m[(r ^ F) * dim + (c ^ F)];
+    if (g.nq == 2) {
+        reorder_ascending(2, order, M, o.q, o.m);
+    } else {
+        o.q[0] = order[0];
+        for (int k = 0; k < 4; ++k) o.m[k] = M[k];
+    }
+    compute_mixing(&o);
+    return o;
 }
 
 qs::KGate to_kgate(const CGate &cg, const std::vector<int> &tile_qubits, int C) {
@@ -468,6 +616,8 @@ struct qs_state {
         uint32_t op_off;
         int rb;
         bool first, final;
+        int kind;             // 0: tile pass, 1: chunk-header permutation only
+        qs::ChunkPerm perm;   // where the pass stores each chunk
     };
     qs::Sweep *sweeps_dev = nullptr;
     qs::ROp *ops_dev = nullptr;
@@ -478,7 +628,7 @@ struct qs_state {
     qs::ChunkMeta *meta[2] = {nullptr, nullptr};
     uint32_t *arena[2] = {nullptr, nullptr};
     uint64_t capacity = 0;
-    unsigned long long *counters = nullptr;  // [0..1] bump, [2..4] stats, [5] init scratch
+    unsigned long long *counters = nullptr;  // [0..1] bump, [2..4] stats, [5] init scratch, [6] header-pass bytes
     uint8_t *mask = nullptr;
     uint32_t *block_nz = nullptr;
     unsigned long long *block_bytes = nullptr, *block_acc = nullptr;
@@ -490,7 +640,8 @@ struct qs_state {
     std::vector<cudaEvent_t> pass_ev;           // QS_FLAG_PROFILE: two events per pass
     int32_t *error_dev = nullptr;
     double *dscratch = nullptr;
-    int cur = 0;
+    int cur = 0;     // payload arena in use
+    int mcur = 0;    // chunk-header array in use (header-only passes flip it alone)
     uint64_t arena_used = 0;
 
     struct Checkpoint {
@@ -551,7 +702,7 @@ struct qs_state {
         const uint64_t chunk = basis >> C;
         CUDA_TRY(this, cudaMemsetAsync(mask, 0, nb, stream));
         CUDA_TRY(this, cudaMemsetAsync(block_bytes, 0, nb * sizeof(unsigned long long), stream));
-        CUDA_TRY(this, cudaMemsetAsync(meta[cur] + blk * chunks_per_block(), 0,
+        CUDA_TRY(this, cudaMemsetAsync(meta[mcur] + blk * chunks_per_block(), 0,
                                        chunks_per_block() * sizeof(qs::ChunkMeta), stream));
         const int comp = (int)(2 * (basis & ((uint64_t(1) << C) - 1)));
         const int32_t q1 = f64 ? qs::quantize(1.0, codec) : qs::quantize(1.0f, codec);
@@ -564,7 +715,7 @@ struct qs_state {
         if (s + w > 32) words[(r + 1) * 32 + lane] |= (uint32_t)((uint64_t)q1 >> (32 - s));
         qs::ChunkMeta md{0, 0, w};
         CUDA_TRY(this, cudaMemcpyAsync(arena[cur], words.data(), words.size() * 4, cudaMemcpyHostToDevice, stream));
-        CUDA_TRY(this, cudaMemcpyAsync(meta[cur] + chunk, &md, sizeof(md), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(this, cudaMemcpyAsync(meta[mcur] + chunk, &md, sizeof(md), cudaMemcpyHostToDevice, stream));
         const uint8_t one = 1;
         CUDA_TRY(this, cudaMemcpyAsync(mask + blk, &one, 1, cudaMemcpyHostToDevice, stream));
         const unsigned long long bytes = words.size() * 4 + chunks_per_block() * sizeof(qs::ChunkMeta);
@@ -777,10 +928,26 @@ static qs_status build_device_plan(qs_state *h) {
     std::vector<qs::ROp> ops;
     std::vector<cplx> pool;
     h->passes.clear();
+    const bool permute = env_int("QOMPSIM_PERMUTE_CHUNKS", 1) != 0;
     for (uint32_t s = 0; s < h->stages.size(); ++s) {
         for (uint32_t gi : h->stages[s])
             if (gi >= h->cgates.size()) return fail(h, QS_ERR_ARG, "stage refers to a gate index out of range");
-        auto pl = plan_passes(h->stages[s], h->cgates, C, jmax, jmin, C, (int)h->B);
+        std::vector<CGate> sg;
+        HostPerm P((int)(h->n - h->C));
+        stage_relabel(h->cgates, h->stages[s], C, permute, &sg, &P);
+        if (sg.empty()) {  // only chunk permutations: one header pass does the stage
+            qs_state::DevPass dp{};
+            dp.stage = s;
+            dp.kind = 1;
+            dp.first = dp.final = true;
+            dp.perm = P.device();
+            if (std::getenv("QOMPSIM_DEBUG_PLAN")) printf("stage %u: header permutation only\n", s);
+            h->passes.push_back(dp);
+            continue;
+        }
+        std::vector<uint32_t> ids(sg.size());
+        for (size_t i = 0; i < ids.size(); ++i) ids[i] = (uint32_t)i;
+        auto pl = plan_passes(ids, sg, C, jmax, jmin, C, (int)h->B);
         for (size_t p = 0; p < pl.size(); ++p) {
             qs_state::DevPass dp{};
             dp.stage = s;
@@ -791,7 +958,9 @@ static qs_status build_device_plan(qs_state *h) {
             dp.ngates = (uint32_t)pl[p].gates.size();
             dp.first = p == 0;
             dp.final = p + 1 == pl.size();
-            for (uint32_t gi : pl[p].gates) kg.push_back(to_kgate(h->cgates[gi], pl[p].tile, C));
+            dp.kind = 0;
+            dp.perm = dp.final ? P.device() : identity_perm();
+            for (uint32_t gi : pl[p].gates) kg.push_back(to_kgate(sg[gi], pl[p].tile, C));
             const int RB = C + dp.j >= RBmain ? RBmain : 3;  // small tiles use 8-amplitude groups
             dp.rb = RB;
             auto swp = plan_sweeps(kg, dp.gate_off, kg.size(), C + dp.j, RB);
@@ -947,6 +1116,43 @@ qs_status qs_plan_stages(const qs_gate *gates, size_t count, uint32_t n, uint32_
     return QS_OK;
 }
 
+qs_status qs_stage_chunk_permutation(const qs_gate *gates, size_t count, uint32_t n, uint32_t chunk_log2,
+                                     int reference_controls, qs_gate *out, size_t *out_count, int32_t *perm_dst,
+                                     uint64_t *perm_flip) {
+    if ((count && !gates) || !out_count || !perm_flip) return fail(nullptr, QS_ERR_ARG, "NULL argument");
+    if (n > 40 || chunk_log2 > n) return fail(nullptr, QS_ERR_ARG, "bad geometry");
+    std::vector<CGate> cg(count);
+    std::vector<uint32_t> ids(count);
+    for (size_t i = 0; i < count; ++i) {
+        std::string err;
+        if (!canonicalize(gates[i], reference_controls != 0, n, &cg[i], &err)) return fail(nullptr, QS_ERR_ARG, err);
+        ids[i] = (uint32_t)i;
+    }
+    std::vector<CGate> sg;
+    HostPerm P((int)(n - chunk_log2));
+    stage_relabel(cg, ids, (int)chunk_log2, true, &sg, &P);
+    *out_count = sg.size();
+    if (out) {
+        for (size_t i = 0; i < sg.size(); ++i) {
+            qs_gate g;
+            std::memset(&g, 0, sizeof(g));
+            std::snprintf(g.name, sizeof(g.name), "DenseMatrix");
+            g.ntargets = (uint32_t)sg[i].nq;
+            const int dim = 1 << sg[i].nq;
+            for (int k = 0; k < sg[i].nq; ++k) g.targets[k] = (uint32_t)sg[i].q[k];
+            for (int k = 0; k < dim * dim; ++k) {
+                g.matrix[2 * k] = sg[i].m[k].real();
+                g.matrix[2 * k + 1] = sg[i].m[k].imag();
+            }
+            out[i] = g;
+        }
+    }
+    if (perm_dst)
+        for (size_t b = 0; b < P.dst.size(); ++b) perm_dst[b] = P.dst[b];
+    *perm_flip = P.x;
+    return QS_OK;
+}
+
 qs_status qs_get_plan_info(qs_state *h, uint32_t *nstages, uint32_t *nblocks) {
     if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
     if (nstages) *nstages = (uint32_t)h->stages.size();
@@ -982,13 +1188,37 @@ qs_status qs_apply_circuit(qs_state *h) {
     CUDA_TRY(h, qs::launch_sum_mask_bytes(h->mask, h->block_bytes, h->nb, h->history_dev, s));
     CUDA_TRY(h, cudaEventRecord(h->ev[0], s));
     size_t pi = 0;
+    bool tile_passes = false;
     for (uint32_t st = 0; st < h->stages.size(); ++st) {
         const uint32_t *b2g = h->b2g_dev + (size_t)st * h->nb;
         CUDA_TRY(h, qs::launch_stage_begin(b2g, h->mask, h->nb, h->group_active, h->num_groups[st], h->block_nz,
                                            h->block_acc, h->history_dev + h->stages.size() + 1 + st, s));
         for (; pi < h->passes.size() && h->passes[pi].stage == st; ++pi) {
             const auto &dp = h->passes[pi];
+            if (dp.kind == 1) {
+                qs::PermPassArgs pa{};
+                pa.B = (int)h->B;
+                pa.C = C;
+                pa.nchunks = h->nchunks;
+                pa.meta_in = h->meta[h->mcur];
+                pa.meta_out = h->meta[h->mcur ^ 1];
+                pa.block_to_group = b2g;
+                pa.group_active = h->group_active;
+                pa.mask = h->mask;
+                pa.first_pass = dp.first;
+                pa.final_pass = dp.final;
+                pa.block_nz = h->block_nz;
+                pa.block_bytes = h->block_acc;
+                pa.stats = h->counters + 6;
+                pa.perm = dp.perm;
+                if (!h->pass_ev.empty()) CUDA_TRY(h, cudaEventRecord(h->pass_ev[2 * pi], s));
+                CUDA_TRY(h, qs::launch_perm_pass(pa, s));
+                if (!h->pass_ev.empty()) CUDA_TRY(h, cudaEventRecord(h->pass_ev[2 * pi + 1], s));
+                h->mcur ^= 1;
+                continue;
+            }
             const int out = h->cur ^ 1;
+            tile_passes = true;
             CUDA_TRY(h, cudaMemsetAsync(h->counters + out, 0, sizeof(unsigned long long), s));
             qs::PassArgs a{};
             a.n = (int)h->n;
@@ -1003,10 +1233,11 @@ qs_status qs_apply_circuit(qs_state *h) {
             a.nsweeps = (int)dp.nsweeps;
             a.rb = dp.rb;
             a.codec = h->codec;
-            a.meta_in = h->meta[h->cur];
+            a.meta_in = h->meta[h->mcur];
             a.arena_in = h->arena[h->cur];
-            a.meta_out = h->meta[out];
+            a.meta_out = h->meta[h->mcur ^ 1];
             a.arena_out = h->arena[out];
+            a.perm = dp.perm;
             a.bump = h->counters + out;
             a.capacity = h->capacity;
             a.block_to_group = b2g;
@@ -1023,6 +1254,7 @@ qs_status qs_apply_circuit(qs_state *h) {
             CUDA_TRY(h, qs::launch_pass(h->f64, a, h->tile_log2, s));
             if (!h->pass_ev.empty()) CUDA_TRY(h, cudaEventRecord(h->pass_ev[2 * pi + 1], s));
             h->cur = out;
+            h->mcur ^= 1;
         }
         CUDA_TRY(h, qs::launch_stage_end(b2g, h->group_active, h->nb, h->block_nz, h->block_acc, h->mask,
                                          h->block_bytes, h->history_dev + st + 1, s));
@@ -1042,16 +1274,18 @@ qs_status qs_apply_circuit(qs_state *h) {
         return fail(h, QS_ERR_CAPACITY,
                     "compressed store overflowed its arena (" + std::to_string(h->capacity) +
                         " bytes); the state is invalid.  Set QOMPSIM_ARENA_BYTES larger.");
-    if (!h->passes.empty()) h->arena_used = ctr[h->cur];
+    if (tile_passes) h->arena_used = ctr[h->cur];
     const size_t ns = h->stages.size();
     h->history.assign(hist.begin(), hist.begin() + ns + 1);
     uint64_t updates = 0;
     for (size_t st = 0; st < ns; ++st) updates += (uint64_t)h->stages[st].size() * hist[ns + 1 + st] << h->B;
-    double pass_ms = 0;
+    double pass_ms = 0, perm_ms = 0;
+    uint64_t perm_passes = 0;
+    for (size_t p = 0; p < h->passes.size(); ++p) perm_passes += h->passes[p].kind == 1 ? 1 : 0;
     for (size_t p = 0; p < h->pass_ev.size() / 2; ++p) {
         float t = 0;
         CUDA_TRY(h, cudaEventElapsedTime(&t, h->pass_ev[2 * p], h->pass_ev[2 * p + 1]));
-        pass_ms += t;
+        (h->passes[p].kind == 1 ? perm_ms : pass_ms) += t;
     }
     h->times[1] += ms / 1000.0;
     h->st.stages = h->stages.size();
@@ -1066,6 +1300,9 @@ qs_status qs_apply_circuit(qs_state *h) {
     h->st.linear_exp = h->codec.L;
     h->st.chunk_log2 = (int32_t)h->C;
     h->st.tile_log2 = h->tile_log2;
+    h->st.perm_passes = perm_passes;
+    h->st.perm_bytes = ctr[6];
+    h->st.perm_ms = perm_ms;
     if (!h->quiet()) {
         printf("Total SV bytes: %s\n", format_size(hist[0]).c_str());
         for (size_t st = 0; st < ns; ++st)
@@ -1078,7 +1315,7 @@ qs_status qs_apply_circuit(qs_state *h) {
 qs_status qs_norm_squared(qs_state *h, double *out) {
     if (!h || !out) return fail(h, QS_ERR_ARG, "NULL argument");
     CUDA_TRY(h, cudaMemsetAsync(h->dscratch, 0, sizeof(double), h->stream));
-    CUDA_TRY(h, qs::launch_norm(h->f64, h->meta[h->cur], h->arena[h->cur], h->mask, (int)h->B, (int)h->C, h->codec,
+    CUDA_TRY(h, qs::launch_norm(h->f64, h->meta[h->mcur], h->arena[h->cur], h->mask, (int)h->B, (int)h->C, h->codec,
                                 h->nchunks, h->dscratch, h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(out, h->dscratch, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
@@ -1102,7 +1339,7 @@ qs_status qs_get_vector(qs_state *h, double *out, int renormalize) {
     qs_status rs = QS_OK;
     for (uint64_t c0 = 0; c0 < h->nchunks; c0 += nslab) {
         const uint64_t cnt = std::min<uint64_t>(nslab, h->nchunks - c0);
-        cudaError_t e = qs::launch_readout(h->f64, h->meta[h->cur], h->arena[h->cur], h->mask, (int)h->B, (int)h->C,
+        cudaError_t e = qs::launch_readout(h->f64, h->meta[h->mcur], h->arena[h->cur], h->mask, (int)h->B, (int)h->C,
                                            h->codec, c0, cnt, dbuf, scale, h->stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(out + c0 * chunk_amps * 2, dbuf, cnt * chunk_amps * 2 * sizeof(double),
@@ -1185,7 +1422,7 @@ qs_status qs_load_vector(qs_state *h, const double *vec) {
         cudaError_t e = cudaMemcpyAsync(dbuf, vec + c0 * chunk_amps * 2, cnt * chunk_amps * 2 * sizeof(double),
                                         cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess)
-            e = qs::launch_encode(h->f64, dbuf, (int)h->B, (int)h->C, h->codec, c0, cnt, h->meta[h->cur],
+            e = qs::launch_encode(h->f64, dbuf, (int)h->B, (int)h->C, h->codec, c0, cnt, h->meta[h->mcur],
                                   h->arena[h->cur], h->counters + h->cur, h->capacity, h->block_nz, h->block_acc,
                                   h->error_dev, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -1307,7 +1544,7 @@ qs_status qs_expectation_pauli(qs_state *h, const uint64_t *x_masks, const uint6
             a.j = (int)tv.size();
             for (int k = 0; k < a.j; ++k) a.tq[k] = tv[k] - C;
             a.n_tiles = uint64_t(1) << (h->n - C - a.j);
-            a.meta = h->meta[h->cur];
+            a.meta = h->meta[h->mcur];
             a.arena = h->arena[h->cur];
             a.mask = h->mask;
             a.codec = h->codec;
@@ -1357,7 +1594,7 @@ qs_status qs_checkpoint(qs_state *h, uint32_t slot) {
         c.arena_cap = cap;
     }
     cudaStream_t s = h->stream;
-    CUDA_TRY(h, cudaMemcpyAsync(c.meta, h->meta[h->cur], meta_bytes, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(h, cudaMemcpyAsync(c.meta, h->meta[h->mcur], meta_bytes, cudaMemcpyDeviceToDevice, s));
     if (h->arena_used)
         CUDA_TRY(h, cudaMemcpyAsync(c.arena, h->arena[h->cur], h->arena_used, cudaMemcpyDeviceToDevice, s));
     CUDA_TRY(h, cudaMemcpyAsync(c.mask, h->mask, h->nb, cudaMemcpyDeviceToDevice, s));
@@ -1373,7 +1610,7 @@ qs_status qs_restore(qs_state *h, uint32_t slot) {
     if (slot >= h->ckpt.size() || !h->ckpt[slot].meta) return fail(h, QS_ERR_STATE, "no checkpoint in this slot");
     auto &c = h->ckpt[slot];
     cudaStream_t s = h->stream;
-    CUDA_TRY(h, cudaMemcpyAsync(h->meta[h->cur], c.meta, h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(h, cudaMemcpyAsync(h->meta[h->mcur], c.meta, h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyDeviceToDevice, s));
     if (c.used) CUDA_TRY(h, cudaMemcpyAsync(h->arena[h->cur], c.arena, c.used, cudaMemcpyDeviceToDevice, s));
     CUDA_TRY(h, cudaMemcpyAsync(h->mask, c.mask, h->nb, cudaMemcpyDeviceToDevice, s));
     CUDA_TRY(h, cudaMemcpyAsync(h->block_bytes, c.block_bytes, h->nb * sizeof(unsigned long long),
@@ -1418,7 +1655,7 @@ qs_status qs_export_store(qs_state *h, void *buf, uint64_t cap, uint64_t *size) 
     p += nbpad;
     CUDA_TRY(h, cudaMemcpyAsync(p, h->block_bytes, h->nb * 8, cudaMemcpyDeviceToHost, s));
     p += h->nb * 8;
-    CUDA_TRY(h, cudaMemcpyAsync(p, h->meta[h->cur], h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(h, cudaMemcpyAsync(p, h->meta[h->mcur], h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyDeviceToHost, s));
     p += h->nchunks * sizeof(qs::ChunkMeta);
     if (h->arena_used) CUDA_TRY(h, cudaMemcpyAsync(p, h->arena[h->cur], h->arena_used, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(h, cudaStreamSynchronize(s));
@@ -1447,7 +1684,7 @@ qs_status qs_import_store(qs_state *h, const void *buf, uint64_t size) {
     std::vector<uint64_t> bb(h->nb);
     std::memcpy(bb.data(), p, h->nb * 8);
     p += h->nb * 8;
-    CUDA_TRY(h, cudaMemcpyAsync(h->meta[h->cur], p, h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(h, cudaMemcpyAsync(h->meta[h->mcur], p, h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyHostToDevice, s));
     p += h->nchunks * sizeof(qs::ChunkMeta);
     if (hd.arena_bytes) CUDA_TRY(h, cudaMemcpyAsync(h->arena[h->cur], p, hd.arena_bytes, cudaMemcpyHostToDevice, s));
     CUDA_TRY(h, cudaStreamSynchronize(s));

@@ -81,6 +81,18 @@ struct CodecParams {
     int32_t L;      // absolute step 2^-L in the linear region
 };
 
+// A permutation of chunk indices (the amplitude-index bits >= C) made of bit
+// moves and bit flips: SWAP and X gates on qubits >= C move whole chunks, so
+// they are applied by rewriting chunk headers, never by decoding payloads.
+//   perm(c) = ((c & keep) | sum_k bit(c, src[k]) << dst[k]) ^ flip
+constexpr int kMaxPermBits = 40;
+struct ChunkPerm {
+    uint64_t keep;          // bits that stay in place (all ones: identity)
+    uint64_t flip;          // bits flipped after the moves
+    int32_t nmove;
+    int8_t src[kMaxPermBits], dst[kMaxPermBits];
+};
+
 // One fused pass over the compressed store.
 struct PassArgs {
     int32_t n, B, C, j;                 // qubits, block log2, chunk log2, tile qubits above C
@@ -106,6 +118,24 @@ struct PassArgs {
     unsigned long long *block_bytes;    // final pass: stored bytes of block
     int32_t *error;                     // 1 = arena overflow
     unsigned long long *stats;          // [0] bytes read [1] bytes written [2] tiles
+    ChunkPerm perm;                     // chunk c of the pass is stored as chunk perm(c)
+};
+
+// A pass that only permutes chunk headers: meta_out[perm(c)] = meta_in[c]
+// for the chunks of active groups (the payload arena is shared).
+struct PermPassArgs {
+    int32_t B, C;
+    uint64_t nchunks;
+    const ChunkMeta *meta_in;
+    ChunkMeta *meta_out;
+    const uint32_t *block_to_group;
+    const uint8_t *group_active;
+    const uint8_t *mask;
+    int32_t first_pass, final_pass;
+    uint32_t *block_nz;
+    unsigned long long *block_bytes;
+    unsigned long long *stats;
+    ChunkPerm perm;
 };
 
 // One fused pass over a dense state vector (in place).
@@ -178,6 +208,7 @@ cudaError_t launch_expect(bool f64, const ExpectArgs &a, cudaStream_t stream);
 cudaError_t launch_dense_expect(bool f64, const void *state, int n, const PauliTerm *terms, int nterms, double *out,
                                 cudaStream_t stream);
 cudaError_t launch_pass(bool f64, const PassArgs &a, int tile_log2, cudaStream_t stream);
+cudaError_t launch_perm_pass(const PermPassArgs &a, cudaStream_t stream);
 cudaError_t launch_dense_pass(bool f64, const DensePassArgs &a, int tile_log2, cudaStream_t stream);
 cudaError_t launch_pergate(bool f64, void *state, int n, const KGate *gate_dev, cudaStream_t stream);
 

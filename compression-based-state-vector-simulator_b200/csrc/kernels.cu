@@ -415,6 +415,12 @@ __device__ __forceinline__ void pack_chunk(const int32_t *codes, int per_lane, i
     if (nbits > 0) __stcs(dst + r * 32 + lane, (uint32_t)buf);
 }
 
+__device__ __forceinline__ uint64_t apply_perm(const ChunkPerm &p, uint64_t c) {
+    uint64_t o = c & p.keep;
+    for (int k = 0; k < p.nmove; ++k) o |= ((c >> p.src[k]) & 1ull) << p.dst[k];
+    return o ^ p.flip;
+}
+
 __device__ __forceinline__ size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 size_t pass_smem_bytes(bool f64, int nb, int j) {
@@ -522,7 +528,7 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
 
         // ---- pack and store
         for (int c = warp; c < nchunks; c += nwarps) {
-            const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
+            const uint64_t chunk = apply_perm(a.perm, chunk_base | deposit_bits((uint32_t)c, s_tq, j));
             const int32_t *codes = reinterpret_cast<const int32_t *>(reinterpret_cast<R *>(tile) + (size_t)c * ncomp);
             const unsigned long long off = s_tile_off + s_off[c];
             const uint32_t w = s_width[c];
@@ -546,6 +552,49 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
     if (threadIdx.x == 0) {
         if (wr) atomicAdd(&a.stats[1], wr);
         if (ntiles) atomicAdd(&a.stats[2], ntiles);
+    }
+}
+
+// ------------------------------------------------------------ header permutation pass
+__global__ void perm_pass_kernel(const PermPassArgs a) {
+    const int blk_shift = a.B - a.C;
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long moved = 0;
+    // every lane of a warp runs the same iterations, so the per-block sums
+    // below can use warp-wide match and reduce
+    for (uint64_t c0 = warp0 * 32; c0 < a.nchunks; c0 += nwarps * 32) {
+        const uint64_t c = c0 + lane;
+        bool live = c < a.nchunks;
+        const uint64_t blk = c >> blk_shift;
+        if (live) live = a.group_active[a.block_to_group[blk]] != 0;
+        uint64_t ob = ~0ull;
+        uint32_t bytes = 0, nz = 0;
+        if (live) {
+            ChunkMeta md{0, 0, 0};
+            if (!a.first_pass || a.mask[blk]) md = a.meta_in[c];
+            const uint64_t oc = apply_perm(a.perm, c);
+            a.meta_out[oc] = md;
+            ++moved;
+            ob = oc >> blk_shift;
+            bytes = (uint32_t)(payload_bytes(a.C, md.width) + sizeof(ChunkMeta));
+            nz = (md.width != 0 || md.base != 0) ? 1u : 0u;
+        }
+        if (a.final_pass) {
+            const unsigned grp = __match_any_sync(0xffffffffu, ob);
+            const uint32_t gbytes = __reduce_add_sync(grp, bytes);
+            const uint32_t gnz = __reduce_or_sync(grp, nz);
+            if (live && lane == __ffs(grp) - 1) {
+                if (gnz) atomicOr(&a.block_nz[ob], 1u);
+                atomicAdd(&a.block_bytes[ob], (unsigned long long)gbytes);
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) moved += __shfl_xor_sync(0xffffffffu, moved, o);
+    if (lane == 0 && moved) {
+        atomicAdd(&a.stats[0], moved * sizeof(ChunkMeta));
+        atomicAdd(&a.stats[1], moved * sizeof(ChunkMeta));
     }
 }
 
@@ -1121,6 +1170,12 @@ static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
 cudaError_t launch_pass(bool f64, const PassArgs &a, int, cudaStream_t s) {
     if (f64) return a.rb == kRegBitsF64 ? launch_pass_t<double, kRegBitsF64>(a, s) : launch_pass_t<double, 3>(a, s);
     return a.rb == kRegBitsF32 ? launch_pass_t<float, kRegBitsF32>(a, s) : launch_pass_t<float, 3>(a, s);
+}
+
+cudaError_t launch_perm_pass(const PermPassArgs &a, cudaStream_t s) {
+    const unsigned grid = grid_for(a.nchunks, 256, 16);
+    perm_pass_kernel<<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
 }
 
 template <typename R, int RB>

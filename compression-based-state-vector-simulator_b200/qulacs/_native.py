@@ -70,6 +70,9 @@ class qs_stats(ct.Structure):
         ("tile_log2", ct.c_int32),
         ("sweeps", ct.c_uint64),
         ("ops", ct.c_uint64),
+        ("perm_passes", ct.c_uint64),
+        ("perm_bytes", ct.c_uint64),
+        ("perm_ms", ct.c_double),
     ]
 
 
@@ -91,6 +94,9 @@ SIGNATURES = [
                                       ct.POINTER(_U32), ct.POINTER(_U32)]),
     ("qs_plan_stages", ct.c_int, [ct.POINTER(qs_gate), ct.c_size_t, _U32, _U32, _U32, ct.POINTER(ct.c_size_t),
                                   ct.POINTER(_U32), ct.POINTER(_U32), ct.POINTER(_U32), ct.POINTER(_U32)]),
+    ("qs_stage_chunk_permutation", ct.c_int, [ct.POINTER(qs_gate), ct.c_size_t, _U32, _U32, ct.c_int,
+                                              ct.POINTER(qs_gate), ct.POINTER(ct.c_size_t),
+                                              ct.POINTER(ct.c_int32), ct.POINTER(_U64)]),
     ("qs_get_plan_info", ct.c_int, [_P, ct.POINTER(_U32), ct.POINTER(_U32)]),
     ("qs_get_stage", ct.c_int, [_P, _U32, ct.POINTER(_U32), _U32, ct.POINTER(_U32),
                                 ct.POINTER(_U32), ct.POINTER(_U32)]),

@@ -83,12 +83,12 @@ typedef struct qs_dense qs_dense;
 /* Codec / engine statistics of the last qs_apply_circuit. */
 typedef struct qs_stats {
     uint64_t stages;             /* reference stages executed                          */
-    uint64_t passes;             /* fused device passes (a stage needs >= 1)           */
-    uint64_t tiles;              /* tiles processed (all passes)                       */
-    uint64_t bytes_read;         /* compressed payload + chunk headers read (all passes) */
-    uint64_t bytes_written;      /* compressed payload + chunk headers written          */
+    uint64_t passes;             /* device passes, tile passes + perm_passes (>= 1 per stage) */
+    uint64_t tiles;              /* tiles processed (tile passes)                      */
+    uint64_t bytes_read;         /* compressed payload + chunk headers read (tile passes) */
+    uint64_t bytes_written;      /* compressed payload + chunk headers written (tile passes) */
     uint64_t amp_gate_updates;   /* sum over stages of gates(s) * amplitudes in active groups(s) */
-    double kernel_ms;            /* device time of the fused passes alone (QS_FLAG_PROFILE),
+    double kernel_ms;            /* device time of the fused tile passes alone (QS_FLAG_PROFILE),
                                     else equal to apply_ms                             */
     double apply_ms;             /* device time of qs_apply_circuit end to end          */
     int32_t mantissa_bits;       /* quantiser parameter m (relative step 2^-m)          */
@@ -97,6 +97,10 @@ typedef struct qs_stats {
     int32_t tile_log2;           /* largest tile = 2^tile_log2 amplitudes               */
     uint64_t sweeps;             /* register sweeps over all passes (plan)              */
     uint64_t ops;                /* gate op records over all passes (plan)              */
+    uint64_t perm_passes;        /* passes that only permute chunk headers (SWAP / X on
+                                    qubits >= chunk_log2, applied without decoding)     */
+    uint64_t perm_bytes;         /* chunk-header bytes read + written by those passes   */
+    double perm_ms;              /* their device time (QS_FLAG_PROFILE), else 0         */
 } qs_stats;
 
 /* ---------------------------------------------------------------- errors */
@@ -149,6 +153,24 @@ qs_status qs_register_stages(qs_state *h, const uint32_t *stage_sizes, size_t ns
 qs_status qs_plan_stages(const qs_gate *gates, size_t count, uint32_t n, uint32_t block_size,
                          uint32_t inner_size, size_t *nstages, uint32_t *stage_sizes,
                          uint32_t *stage_gate_ids, uint32_t *block_to_group, uint32_t *num_groups);
+
+/* Planner introspection (host only; no reference counterpart): the gates of
+ * ONE stage as the engine applies them.  SWAP and X gates (and other
+ * bit-moving 0/1 permutations) whose qubits are all >= chunk_log2 move whole
+ * chunks; the engine folds them into a chunk-index permutation sigma that the
+ * stage's last pass applies when it stores the chunks (a stage made only of
+ * such gates becomes a pass over chunk headers alone), and relabels every
+ * later gate of the stage through sigma.  out (may be NULL; room for `count`)
+ * receives the remaining gates as "DenseMatrix" gates without controls,
+ * targets ascending, and *out_count their number; perm_dst (may be NULL;
+ * n - chunk_log2 entries) gets the destination of each chunk-index bit and
+ * *perm_flip the bits flipped after the moves:
+ *   sigma(c) = perm_flip ^ sum_b bit(c, b) << perm_dst[b],
+ *   stored amplitude i  ==  true amplitude ((sigma(i >> chunk_log2) << chunk_log2) | (i & (2^chunk_log2 - 1))).
+ * The engine does this unless QOMPSIM_PERMUTE_CHUNKS=0. */
+qs_status qs_stage_chunk_permutation(const qs_gate *gates, size_t count, uint32_t n, uint32_t chunk_log2,
+                                     int reference_controls, qs_gate *out, size_t *out_count,
+                                     int32_t *perm_dst, uint64_t *perm_flip);
 
 /* Planner results: number of stages and blocks; one stage's gate ids,
  * block->group map (nblocks entries, may be NULL) and group count. */

@@ -92,3 +92,30 @@ def random_circuit(n: int, ngates: int, seed: int, controlled: bool = True):
             g.add_control_qubit(b, int(rng.integers(0, 2)))
             c.add_gate(g)
     return c
+
+
+def perm_heavy_circuit(n, C, ngates, seed):
+    """Random gates with many SWAP / X / CNOT gates on qubits >= C."""
+    import qulacs
+    from qulacs import gate as G
+    rng = np.random.default_rng(seed)
+    base = random_circuit(n, ngates, seed)
+    c = qulacs.QuantumCircuit(n)
+    hi = list(range(C, n))
+    for g in base._gates:
+        c.add_gate(g)
+        r = rng.integers(0, 4)
+        a, b = (int(x) for x in rng.choice(hi, size=2, replace=False))
+        if r == 0:
+            c.add_SWAP_gate(a, b)
+        elif r == 1:
+            c.add_X_gate(a)
+        elif r == 2:
+            c.add_CNOT_gate(a, b)      # a permutation, but not a bit move: stays a gate
+        else:
+            m = np.zeros((4, 4))
+            f = [int(x) for x in rng.permutation(4)]
+            for col, row in enumerate(f):
+                m[row, col] = 1.0
+            c.add_gate(G.DenseMatrix([a, b], m))
+    return c

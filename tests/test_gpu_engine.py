@@ -225,6 +225,59 @@ def test_compressed_random_circuits_vs_csim(qulacs_mod, n, seed):
         assert np.array_equal(cq.get_zero_mask(), o.mask())
 
 
+def _permute_chunks_run(qulacs, c, B, I, on, monkeypatch, **kw):
+    monkeypatch.setenv("QOMPSIM_PERMUTE_CHUNKS", "1" if on else "0")
+    cq = _compressed(qulacs, c, B, I, **kw)
+    return cq, cq.get_vector(renormalize=False), cq.get_zero_mask(), cq.get_SV_bytes_history(), cq.get_stats()
+
+
+def test_chunk_permutation_stage_bit_identical(qulacs_mod, monkeypatch):
+    """Stages made only of SWAP / X gates on qubits >= C run as header-only
+    passes: the stored state, masks and byte history equal those of decoding,
+    permuting and re-encoding every chunk."""
+    import qulacs
+    n, B = 14, 8
+    c = qulacs.QuantumCircuit(n)
+    for q in range(n):
+        c.add_H_gate(q)
+    for q in range(n - 1):
+        c.add_RZ_gate(q, 0.3 + q)
+        c.add_CNOT_gate(q, q + 1)
+    c.add_SWAP_gate(9, 13)
+    c.add_X_gate(12)
+    c.add_SWAP_gate(8, 10)
+    c.add_SWAP_gate(11, 12)
+    c.add_X_gate(11)
+    c.add_RY_gate(2, 0.7)
+    a = _permute_chunks_run(qulacs_mod, c, B, 2, True, monkeypatch)
+    b = _permute_chunks_run(qulacs_mod, c, B, 2, False, monkeypatch)
+    assert a[4]["perm_passes"] >= 1 and b[4]["perm_passes"] == 0
+    assert np.array_equal(a[1], b[1])
+    assert np.array_equal(a[2], b[2])
+    assert list(a[3]) == list(b[3])
+    ref = csim_ref.run_circuit(n, c._gates)
+    assert helpers.fidelity(ref, a[0].get_vector()) > 0.999
+
+
+@pytest.mark.parametrize("n,B,seed", [(12, 8, 21), (12, 6, 22), (15, 9, 23)])
+def test_chunk_permutation_random_circuits(qulacs_mod, monkeypatch, n, B, seed):
+    """Random circuits dense in SWAP / X / permutation gates on high qubits:
+    folded into chunk permutations, against csim and against the unfolded
+    plan (tight codec bounds: both agree to the codec's error)."""
+    C = min(8, B)
+    c = helpers.perm_heavy_circuit(n, C, 60, seed)
+    ref = csim_ref.run_circuit(n, c._gates)
+    kw = dict(eps_rel=2.0 ** -22, eps_abs=1e-13)
+    a = _permute_chunks_run(qulacs_mod, c, B, 3, True, monkeypatch, **kw)
+    b = _permute_chunks_run(qulacs_mod, c, B, 3, False, monkeypatch, **kw)
+    assert np.abs(a[1] - ref).max() < 1e-5
+    assert np.abs(a[1] - b[1]).max() < 1e-5
+    assert np.array_equal(a[2], b[2])
+    L = oc.params(True, 2.0 ** -22, 1e-13)[1]
+    o, _ = _oracle_masks(c, n, B, 3, zero_test=("code", L))
+    assert np.array_equal(a[2], o.mask())
+
+
 @pytest.mark.parametrize("key", ["ghz_10", "qft_8", "hea_9", "qaoa_9", "ising_8", "qsvm_8", "hadamard_8"])
 def test_exact_zero_test_flag(qulacs_mod, key):
     """QS_FLAG_EXACT_ZERO_TEST: the reference GPU build's exact test gives the

@@ -167,3 +167,61 @@ def test_three_qubit_gate_rejected_before_device():
 def test_check_build_for_mpi_false():
     import qulacs
     assert qulacs.check_build_for_mpi() is False
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+def test_stage_chunk_permutation_keeps_the_state(seed):
+    """Folding SWAP / X on qubits >= C into a chunk permutation and relabelling
+    the later gates gives the same state (csim kernels, FP64) once the
+    permutation is applied to the stored amplitudes."""
+    from qulacs import _native
+    from qulacs import gate as G
+    L = _native.load_library()
+    n, C = 9, 3
+    c = helpers.perm_heavy_circuit(n, C, 40, seed)
+    gates = c._gates
+    arr = _native.make_gate_array(gates)
+    out = (_native.qs_gate * len(gates))()
+    cnt = ct.c_size_t()
+    dst = (ct.c_int32 * (n - C))()
+    flip = ct.c_uint64()
+    assert L.qs_stage_chunk_permutation(arr, len(gates), n, C, 0, out, ct.byref(cnt), dst, ct.byref(flip)) == 0
+    assert cnt.value < len(gates)            # something was folded
+    rel = []
+    for k in range(cnt.value):
+        g = out[k]
+        d = 1 << g.ntargets
+        m = np.array(g.matrix[:2 * d * d]).view(np.complex128).reshape(d, d)
+        rel.append(G.DenseMatrix([g.targets[i] for i in range(g.ntargets)], m))
+    stored = csim_ref.run_circuit(n, rel)
+    idx = np.arange(1 << n, dtype=np.int64)
+    ch = idx >> C
+    sig = np.full_like(ch, flip.value)
+    for b in range(n - C):
+        sig ^= ((ch >> b) & 1) << dst[b]
+    true = np.empty_like(stored)
+    true[(sig << C) | (idx & ((1 << C) - 1))] = stored
+    ref = csim_ref.run_circuit(n, gates)
+    assert np.max(np.abs(true - ref)) < 1e-12
+    assert sorted(dst[b] for b in range(n - C)) == list(range(n - C))
+
+
+def test_stage_chunk_permutation_leaves_low_qubits_alone():
+    import qulacs
+    from qulacs import _native
+    L = _native.load_library()
+    c = qulacs.QuantumCircuit(6)
+    c.add_SWAP_gate(0, 5)     # touches a chunk bit: a real gate
+    c.add_X_gate(1)
+    c.add_SWAP_gate(3, 5)     # folded
+    c.add_X_gate(4)           # folded
+    c.add_H_gate(3)           # relabelled to qubit 5
+    arr = _native.make_gate_array(c._gates)
+    out = (_native.qs_gate * 5)()
+    cnt = ct.c_size_t()
+    dst = (ct.c_int32 * 4)()
+    flip = ct.c_uint64()
+    assert L.qs_stage_chunk_permutation(arr, 5, 6, 2, 0, out, ct.byref(cnt), dst, ct.byref(flip)) == 0
+    assert cnt.value == 3
+    assert [out[k].targets[0] for k in range(3)] == [0, 1, 5]
+    assert list(dst) == [0, 3, 2, 1] and flip.value == 1 << 2
