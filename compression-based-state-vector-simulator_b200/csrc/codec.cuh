@@ -177,6 +177,141 @@ __host__ __device__ inline double dequantize_f64(int32_t q, CodecParams p) {
 __host__ __device__ inline float dequantize(int32_t q, CodecParams p, float) { return dequantize_f32(q, p); }
 __host__ __device__ inline double dequantize(int32_t q, CodecParams p, double) { return dequantize_f64(q, p); }
 
+// ---------------------------------------------------------------- fast paths
+// The same maps with 32-bit integer work only and no branches, for the hot
+// kernels.  For doubles they need m <= kFastMantissaF64: then the log-region
+// rounding bit and the kept mantissa bits all lie in the high word of the
+// double, so the low word never contributes; for m above that the kernels
+// call quantize()/dequantize_f64().  Bit-identical to the statements above
+// (the CPU oracle checks the device codes).
+constexpr int kFastMantissaF64 = 19;
+
+__host__ __device__ inline uint32_t hi_word(double x) {
+#ifdef __CUDA_ARCH__
+    return (uint32_t)__double2hiint(x);
+#else
+    uint64_t b;
+    std::memcpy(&b, &x, 8);
+    return (uint32_t)(b >> 32);
+#endif
+}
+__host__ __device__ inline uint32_t lo_word(double x) {
+#ifdef __CUDA_ARCH__
+    return (uint32_t)__double2loint(x);
+#else
+    uint64_t b;
+    std::memcpy(&b, &x, 8);
+    return (uint32_t)b;
+#endif
+}
+__host__ __device__ inline double from_words(uint32_t hi, uint32_t lo) {
+#ifdef __CUDA_ARCH__
+    return __hiloint2double((int)hi, (int)lo);
+#else
+    const uint64_t b = ((uint64_t)hi << 32) | lo;
+    double x;
+    std::memcpy(&x, &b, 8);
+    return x;
+#endif
+}
+__host__ __device__ inline uint32_t f32_bits(float x) {
+#ifdef __CUDA_ARCH__
+    return __float_as_uint(x);
+#else
+    uint32_t b;
+    std::memcpy(&b, &x, 4);
+    return b;
+#endif
+}
+__host__ __device__ inline float f32_from(uint32_t b) {
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(b);
+#else
+    float x;
+    std::memcpy(&x, &b, 4);
+    return x;
+#endif
+}
+
+// m <= kFastMantissaF64.
+__host__ __device__ inline int32_t quantize_fast(double x, CodecParams p) {
+    const uint32_t hi = hi_word(x), ahi = hi & 0x7fffffffu;
+    const int e0 = p.m - p.L;
+    const uint32_t thr = uint32_t(e0 + 1023) << 20;
+    // linear region: rint(|x| 2^L) appears in the low word of fma(|x|, 2^L, 2^52)
+    const double a = from_words(ahi, lo_word(x));
+    const double scale = from_words(uint32_t(p.L + 1023) << 20, 0u);
+#ifdef __CUDA_ARCH__
+    const double r = __fma_rn(a, scale, 4503599627370496.0);
+#else
+    const double r = std::fma(a, scale, 4503599627370496.0);
+#endif
+    const uint32_t c_lin = lo_word(r);
+    // log region: round the high word to m mantissa bits (the rounding bit is
+    // bit 19 - m of the high word)
+    const int shh = 20 - p.m;
+    const uint32_t c_log = ((ahi + (1u << (shh - 1))) >> shh) - (uint32_t(e0 + 1023) << p.m) + (1u << p.m);
+    uint32_t c = ahi < thr ? c_lin : c_log;
+    if (ahi >= thr && c > (uint32_t)kCodeLimit) c = (uint32_t)kCodeLimit;
+    const uint32_t sgn = (uint32_t)((int32_t)hi >> 31);
+    return (int32_t)((c ^ sgn) - sgn);
+}
+
+// m <= kFastMantissaF64.
+__host__ __device__ inline double dequantize_fast(int32_t q, CodecParams p) {
+    const uint32_t sgn = (uint32_t)(q >> 31);
+    const uint32_t c = ((uint32_t)q ^ sgn) - sgn;
+    // linear region: c in the low word of 2^(52-L) (1 + c 2^-52), minus 2^(52-L)
+    const uint32_t ehi = uint32_t(1075 - p.L) << 20;
+    const double lin = from_words(ehi, c) - from_words(ehi, 0u);
+    // log region: the code is the high word of the value, shifted
+    const int e0 = p.m - p.L;
+    const uint32_t lhi = (c + (uint32_t(e0 + 1023) << p.m) - (1u << p.m)) << (20 - p.m);
+    const double a = c <= (1u << p.m) ? lin : from_words(lhi, 0u);
+    return from_words(hi_word(a) | (sgn & 0x80000000u), lo_word(a));
+}
+
+__host__ __device__ inline int32_t quantize_fast(float x, CodecParams p) {
+    const uint32_t bits = f32_bits(x), abits = bits & 0x7fffffffu;
+    const int e0 = p.m - p.L;
+    const uint32_t thr = uint32_t(e0 + 127) << 23;
+    const float scale = f32_from(uint32_t(p.L + 127) << 23);
+#ifdef __CUDA_ARCH__
+    const float r = __fmaf_rn(f32_from(abits), scale, 8388608.0f);
+#else
+    const float r = std::fma(f32_from(abits), scale, 8388608.0f);
+#endif
+    const uint32_t c_lin = f32_bits(r) - 0x4b000000u;
+    const int sh = 23 - p.m;
+    const uint32_t half = sh > 0 ? (1u << (sh - 1)) : 0u;
+    const uint32_t c_log = ((abits + half) >> sh) - (uint32_t(e0 + 127) << p.m) + (1u << p.m);
+    uint32_t c = abits < thr ? c_lin : c_log;
+    if (abits >= thr && c > (uint32_t)kCodeLimit) c = (uint32_t)kCodeLimit;
+    const uint32_t sgn = (uint32_t)((int32_t)bits >> 31);
+    return (int32_t)((c ^ sgn) - sgn);
+}
+
+__host__ __device__ inline float dequantize_fast_f32(int32_t q, CodecParams p) {
+    const uint32_t sgn = (uint32_t)(q >> 31);
+    const uint32_t c = ((uint32_t)q ^ sgn) - sgn;
+    const uint32_t eb = uint32_t(150 - p.L) << 23;
+    const float lin = f32_from(eb + c) - f32_from(eb);
+    const int e0 = p.m - p.L;
+    const uint32_t lb = (c + (uint32_t(e0 + 127) << p.m) - (1u << p.m)) << (23 - p.m);
+    const float a = c <= (1u << p.m) ? lin : f32_from(lb);
+    return f32_from(f32_bits(a) | (sgn & 0x80000000u));
+}
+
+// Dispatch on the precision and on the mantissa width (uniform per launch).
+__host__ __device__ inline int32_t quantize_hot(double x, CodecParams p) {
+    return p.m <= kFastMantissaF64 ? quantize_fast(x, p) : quantize(x, p);
+}
+__host__ __device__ inline int32_t quantize_hot(float x, CodecParams p) { return quantize_fast(x, p); }
+__host__ __device__ inline double dequantize_hot(int32_t q, CodecParams p, double) {
+    return p.m <= kFastMantissaF64 ? dequantize_fast(q, p) : dequantize_f64(q, p);
+}
+__host__ __device__ inline float dequantize_hot(int32_t q, CodecParams p, float) { return dequantize_fast_f32(q, p); }
+
 // Quantiser parameters from the error bounds; false when eps_rel is out of
 // range.  L is clamped so that 2^L, 2^-L and 2^e0 are normal numbers.
 inline bool codec_params(bool f64, double eps_rel, double eps_abs, CodecParams *out) {

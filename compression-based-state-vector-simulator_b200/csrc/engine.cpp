@@ -343,8 +343,20 @@ std::vector<qs::Sweep> plan_sweeps(const std::vector<qs::KGate> &kg, size_t g0, 
 // Resolve the gates [g0, g1) of a pass against their sweeps into op records
 // and sub-matrix variants (appended to *ops and *pool).  Sweep gate ranges are
 // relative to g0; op k of the pass is gate g0 + k.
+// A register op before its final encoding: kind, register bits, selector
+// sources (< 64: tile bit, >= 64: outer qubit + 64) and its variants in the
+// pool (variant v at mat + v * vstride).
+enum RawKind : uint8_t { RK_SCALAR = 0, RK_D2 = 1, RK_M2 = 2, RK_D4 = 3, RK_M4 = 4 };
+struct RawOp {
+    uint8_t kind = RK_SCALAR;
+    uint8_t k0 = 0, k1 = 0;
+    uint8_t nsel = 0;
+    uint8_t sel[qs::kMaxSel] = {0, 0, 0, 0};
+    uint32_t mat = 0, vstride = 0;
+};
+
 void build_ops(const std::vector<qs::KGate> &kg, size_t g0, const std::vector<qs::Sweep> &sweeps, int RB,
-               std::vector<qs::ROp> *ops, std::vector<cplx> *pool) {
+               std::vector<RawOp> *ops, std::vector<cplx> *pool) {
     for (const auto &sw : sweeps) {
         for (int gi = sw.g0; gi < sw.g1; ++gi) {
             const qs::KGate &g = kg[g0 + gi];
@@ -367,7 +379,7 @@ void build_ops(const std::vector<qs::KGate> &kg, size_t g0, const std::vector<qs
             std::vector<int> regs;
             for (int i = 0; i < g.nq; ++i)
                 if (reg[i] >= 0) regs.push_back(i);
-            qs::ROp op{};
+            RawOp op{};
             op.nsel = (uint8_t)fixed.size();
             for (size_t j = 0; j < fixed.size(); ++j) op.sel[j] = (uint8_t)src[fixed[j]];
             op.mat = (uint32_t)pool->size();
@@ -388,20 +400,20 @@ void build_ops(const std::vector<qs::KGate> &kg, size_t g0, const std::vector<qs
                     for (int y = 0; y < rd; ++y)
                         if (x != y && M(full(x, v), full(y, v)) != cplx(0, 0)) diag = false;
             if (regs.empty()) {
-                op.kind = qs::OP_SCALAR;
+                op.kind = RK_SCALAR;
                 op.vstride = 1;
                 for (int v = 0; v < nvar; ++v) pool->push_back(M(full(0, v), full(0, v)));
             } else if (regs.size() == 1) {
                 op.k0 = (uint8_t)reg[regs[0]];
                 if (diag) {
-                    op.kind = qs::OP_D2;
+                    op.kind = RK_D2;
                     op.vstride = 2;
                     for (int v = 0; v < nvar; ++v) {
                         pool->push_back(M(full(0, v), full(0, v)));
                         pool->push_back(M(full(1, v), full(1, v)));
                     }
                 } else {
-                    op.kind = qs::OP_M2;
+                    op.kind = RK_M2;
                     op.vstride = 4;
                     for (int v = 0; v < nvar; ++v)
                         for (int x = 0; x < 2; ++x)
@@ -411,11 +423,11 @@ void build_ops(const std::vector<qs::KGate> &kg, size_t g0, const std::vector<qs
                 op.k0 = (uint8_t)reg[0];
                 op.k1 = (uint8_t)reg[1];
                 if (diag) {
-                    op.kind = qs::OP_D4;
+                    op.kind = RK_D4;
                     op.vstride = 4;
                     for (int x = 0; x < 4; ++x) pool->push_back(M(x, x));
                 } else {
-                    op.kind = qs::OP_M4;
+                    op.kind = RK_M4;
                     op.vstride = 16;
                     for (int x = 0; x < 16; ++x) pool->push_back(M(x / 4, x % 4));
                 }
@@ -430,9 +442,9 @@ void build_ops(const std::vector<qs::KGate> &kg, size_t g0, const std::vector<qs
 // range over the union of the selector bits (at most kMaxSel).  The merged
 // op's variant v multiplies the factors of every member at its own variant
 // (v restricted to the member's selector bits).  Applied per sweep.
-void merge_diagonal_ops(const std::vector<qs::Sweep> &sweeps, size_t op0, std::vector<qs::ROp> *ops,
+void merge_diagonal_ops(const std::vector<qs::Sweep> &sweeps, size_t op0, std::vector<RawOp> *ops,
                         std::vector<cplx> *pool, std::vector<qs::Sweep> *out_sweeps) {
-    std::vector<qs::ROp> out;
+    std::vector<RawOp> out;
     std::vector<cplx> outpool;
     out_sweeps->clear();
     for (const auto &sw : sweeps) {
@@ -441,10 +453,10 @@ void merge_diagonal_ops(const std::vector<qs::Sweep> &sweeps, size_t op0, std::v
         size_t i = op0 + sw.g0;
         const size_t end = op0 + sw.g1;
         while (i < end) {
-            const qs::ROp &a = (*ops)[i];
-            auto is_diag1 = [](const qs::ROp &o) { return o.kind == qs::OP_SCALAR || o.kind == qs::OP_D2; };
+            const RawOp &a = (*ops)[i];
+            auto is_diag1 = [](const RawOp &o) { return o.kind == RK_SCALAR || o.kind == RK_D2; };
             if (!is_diag1(a)) {
-                qs::ROp c = a;
+                RawOp c = a;
                 c.mat = (uint32_t)outpool.size();
                 const int nvar = 1 << a.nsel;
                 for (int v = 0; v < nvar; ++v)
@@ -454,22 +466,22 @@ void merge_diagonal_ops(const std::vector<qs::Sweep> &sweeps, size_t op0, std::v
                 continue;
             }
             // grow a run [i, j) of diagonal ops on one register bit (or scalars)
-            int k = a.kind == qs::OP_D2 ? a.k0 : -1;
+            int k = a.kind == RK_D2 ? a.k0 : -1;
             std::vector<int> sels(a.sel, a.sel + a.nsel);
             size_t j = i + 1;
             while (j < end && is_diag1((*ops)[j])) {
-                const qs::ROp &b = (*ops)[j];
-                if (b.kind == qs::OP_D2 && k >= 0 && b.k0 != k) break;
+                const RawOp &b = (*ops)[j];
+                if (b.kind == RK_D2 && k >= 0 && b.k0 != k) break;
                 std::vector<int> u = sels;
                 for (int t = 0; t < b.nsel; ++t)
                     if (std::find(u.begin(), u.end(), (int)b.sel[t]) == u.end()) u.push_back(b.sel[t]);
                 if ((int)u.size() > qs::kMaxSel) break;
                 sels = u;
-                if (b.kind == qs::OP_D2) k = b.k0;
+                if (b.kind == RK_D2) k = b.k0;
                 ++j;
             }
-            qs::ROp m{};
-            m.kind = k >= 0 ? qs::OP_D2 : qs::OP_SCALAR;
+            RawOp m{};
+            m.kind = k >= 0 ? RK_D2 : RK_SCALAR;
             m.k0 = (uint8_t)(k >= 0 ? k : 0);
             m.nsel = (uint8_t)sels.size();
             for (size_t t = 0; t < sels.size(); ++t) m.sel[t] = (uint8_t)sels[t];
@@ -479,13 +491,13 @@ void merge_diagonal_ops(const std::vector<qs::Sweep> &sweeps, size_t op0, std::v
             for (int v = 0; v < nvar; ++v) {
                 cplx f0 = 1.0, f1 = 1.0;
                 for (size_t t = i; t < j; ++t) {
-                    const qs::ROp &b = (*ops)[t];
+                    const RawOp &b = (*ops)[t];
                     int bv = 0;
                     for (int q = 0; q < b.nsel; ++q) {
                         const int pos = (int)(std::find(sels.begin(), sels.end(), (int)b.sel[q]) - sels.begin());
                         bv |= ((v >> pos) & 1) << q;
                     }
-                    if (b.kind == qs::OP_SCALAR) {
+                    if (b.kind == RK_SCALAR) {
                         const cplx z = (*pool)[b.mat + bv];
                         f0 *= z;
                         f1 *= z;
@@ -511,6 +523,105 @@ void merge_diagonal_ops(const std::vector<qs::Sweep> &sweeps, size_t op0, std::v
     pool->insert(pool->end(), outpool.begin(), outpool.end());
 }
 
+// Final encoding of one pass's raw ops (codes in internal.h): selector
+// sources become bit positions of the group word W (tile bit p -> p, outer
+// qubit q -> nb + its index in *outer), register bit pairs are put in
+// ascending order, and the variants are laid out for the code.  Diagonals
+// whose bit-0 factor is exactly 1 in every variant touch only the bit-1
+// amplitudes; exact X and SWAP matrices become register moves.  Appends to
+// ops/pool; false when the pass needs more than kMaxOuterSel outer qubits.
+bool finalize_ops(const std::vector<RawOp> &raw, const std::vector<cplx> &rpool, int nb, std::vector<int> *outer,
+                  std::vector<qs::ROp> *ops, std::vector<cplx> *pool) {
+    const cplx one(1.0, 0.0), zero(0.0, 0.0);
+    for (const RawOp &r : raw) {
+        qs::ROp o;
+        std::memset(&o, 0, sizeof(o));
+        o.nsel = r.nsel;
+        for (int j = 0; j < qs::kMaxSel; ++j) o.sel[j] = qs::kSelNone;
+        for (int j = 0; j < r.nsel; ++j) {
+            const int src = r.sel[j];
+            if (src < 64) {
+                o.sel[j] = (uint8_t)src;
+                continue;
+            }
+            auto it = std::find(outer->begin(), outer->end(), src - 64);
+            if (it == outer->end()) {
+                if ((int)outer->size() >= qs::kMaxOuterSel) return false;
+                outer->push_back(src - 64);
+                it = outer->end() - 1;
+            }
+            o.sel[j] = (uint8_t)(nb + (it - outer->begin()));
+        }
+        const int nvar = 1 << r.nsel;
+        auto E = [&](int v, int e) { return rpool[r.mat + (size_t)v * r.vstride + e]; };
+        o.mat = (uint32_t)pool->size();
+        const int a = std::min(r.k0, r.k1), b = std::max(r.k0, r.k1);
+        const bool flip = r.k0 > r.k1;  // canonical index: bit 0 <-> the lower register bit
+        auto canon = [&](int x) { return flip ? (((x & 1) << 1) | (x >> 1)) : x; };
+        switch (r.kind) {
+            case RK_SCALAR:
+                o.code = qs::OPC_SCALAR;
+                o.vstride = 1;
+                for (int v = 0; v < nvar; ++v) pool->push_back(E(v, 0));
+                break;
+            case RK_D2: {
+                bool unit = true;
+                for (int v = 0; v < nvar; ++v) unit = unit && E(v, 0) == one;
+                o.code = (uint8_t)((unit ? qs::OPC_D2H : qs::OPC_D2) + r.k0);
+                o.vstride = unit ? 1 : 2;
+                for (int v = 0; v < nvar; ++v) {
+                    if (!unit) pool->push_back(E(v, 0));
+                    pool->push_back(E(v, 1));
+                }
+                break;
+            }
+            case RK_M2:
+                if (r.nsel == 0 && E(0, 0) == zero && E(0, 1) == one && E(0, 2) == one && E(0, 3) == zero) {
+                    o.code = (uint8_t)(qs::OPC_X + r.k0);
+                    o.vstride = 0;
+                } else {
+                    o.code = (uint8_t)(qs::OPC_M2 + r.k0);
+                    o.vstride = 4;
+                    for (int v = 0; v < nvar; ++v)
+                        for (int e = 0; e < 4; ++e) pool->push_back(E(v, e));
+                }
+                break;
+            case RK_D4: {
+                bool unit = true;
+                for (int v = 0; v < nvar; ++v) unit = unit && E(v, canon(0)) == one;
+                o.code = (uint8_t)((unit ? qs::OPC_D4H : qs::OPC_D4) + a * 8 + b);
+                o.vstride = unit ? 3 : 4;
+                for (int v = 0; v < nvar; ++v)
+                    for (int y = unit ? 1 : 0; y < 4; ++y) pool->push_back(E(v, canon(y)));
+                break;
+            }
+            default: {  // RK_M4
+                std::vector<cplx> m(16 * (size_t)nvar);
+                for (int v = 0; v < nvar; ++v)
+                    for (int y = 0; y < 4; ++y)
+                        for (int x = 0; x < 4; ++x) m[16 * v + 4 * y + x] = E(v, 4 * canon(y) + canon(x));
+                bool is_swap = r.nsel == 0;
+                for (int y = 0; y < 4 && is_swap; ++y)
+                    for (int x = 0; x < 4; ++x) {
+                        const int t = (y == 1) ? 2 : (y == 2) ? 1 : y;
+                        if (m[4 * y + x] != (x == t ? one : zero)) is_swap = false;
+                    }
+                if (is_swap) {
+                    o.code = (uint8_t)(qs::OPC_SWAP + a * 8 + b);
+                    o.vstride = 0;
+                } else {
+                    o.code = (uint8_t)(qs::OPC_M4 + a * 8 + b);
+                    o.vstride = 16;
+                    pool->insert(pool->end(), m.begin(), m.end());
+                }
+                break;
+            }
+        }
+        ops->push_back(o);
+    }
+    return true;
+}
+
 template <typename Real>
 std::vector<Real> pool_as(const std::vector<cplx> &pool) {
     std::vector<Real> out(2 * pool.size());
@@ -533,21 +644,32 @@ struct PassPlan {
 std::vector<PassPlan> plan_passes(const std::vector<uint32_t> &gate_ids, const std::vector<CGate> &cg, int C,
                                   int jmax, int jmin, int pad_lo, int pad_hi) {
     std::vector<PassPlan> out;
-    std::set<int> cur;
+    std::set<int> cur, sel;  // mixing qubits >= C; non-mixing qubits >= C (selector candidates)
     PassPlan p;
+    auto outside = [](const std::set<int> &a, const std::set<int> &t) {
+        int k = 0;
+        for (int q : a) k += t.count(q) ? 0 : 1;
+        return k;
+    };
     for (uint32_t gi : gate_ids) {
-        std::set<int> need = cur;
-        for (int b = 0; b < cg[gi].nq; ++b)
-            if (cg[gi].mix[b] && cg[gi].q[b] >= C) need.insert(cg[gi].q[b]);
-        if ((int)need.size() > jmax) {
+        std::set<int> need = cur, nsel = sel;
+        for (int b = 0; b < cg[gi].nq; ++b) {
+            if (cg[gi].q[b] < C) continue;
+            (cg[gi].mix[b] ? need : nsel).insert(cg[gi].q[b]);
+        }
+        if ((int)need.size() > jmax || outside(nsel, need) > qs::kMaxOuterSel) {
             p.tile.assign(cur.begin(), cur.end());
             out.push_back(p);
             p = PassPlan();
             cur.clear();
-            for (int b = 0; b < cg[gi].nq; ++b)
-                if (cg[gi].mix[b] && cg[gi].q[b] >= C) cur.insert(cg[gi].q[b]);
+            sel.clear();
+            for (int b = 0; b < cg[gi].nq; ++b) {
+                if (cg[gi].q[b] < C) continue;
+                (cg[gi].mix[b] ? cur : sel).insert(cg[gi].q[b]);
+            }
         } else {
             cur = need;
+            sel = nsel;
         }
         p.gates.push_back(gi);
     }
@@ -615,6 +737,8 @@ struct qs_state {
         uint32_t sweep_off, nsweeps;
         uint32_t op_off;
         int rb;
+        int nouter;
+        int8_t outer_q[qs::kMaxOuterSel];
         bool first, final;
         int kind;             // 0: tile pass, 1: chunk-header permutation only
         qs::ChunkPerm perm;   // where the pass stores each chunk
@@ -921,8 +1045,7 @@ static void make_block_groups(qs_state *h) {
 static qs_status build_device_plan(qs_state *h) {
     const int C = (int)h->C;
     const int jmax = std::min(h->tile_log2 - C, qs::kMaxTileQubits);
-    const int RBmain = h->f64 ? qs::kRegBitsF64 : qs::kRegBitsF32;
-    const int jmin = std::min(jmax, std::max(3, RBmain - C));
+    const int jmin = std::min(jmax, std::max(3, qs::kRegBits - C));
     std::vector<qs::KGate> kg;
     std::vector<qs::Sweep> sw;
     std::vector<qs::ROp> ops;
@@ -961,19 +1084,38 @@ static qs_status build_device_plan(qs_state *h) {
             dp.kind = 0;
             dp.perm = dp.final ? P.device() : identity_perm();
             for (uint32_t gi : pl[p].gates) kg.push_back(to_kgate(sg[gi], pl[p].tile, C));
-            const int RB = C + dp.j >= RBmain ? RBmain : 3;  // small tiles use 8-amplitude groups
+            const int RB = qs::kRegBits;
             dp.rb = RB;
             auto swp = plan_sweeps(kg, dp.gate_off, kg.size(), C + dp.j, RB);
             const size_t op0 = ops.size();
-            build_ops(kg, dp.gate_off, swp, RB, &ops, &pool);
+            std::vector<RawOp> raw;
+            std::vector<cplx> rpool;
+            build_ops(kg, dp.gate_off, swp, RB, &raw, &rpool);
             std::vector<qs::Sweep> merged;
-            merge_diagonal_ops(swp, op0, &ops, &pool, &merged);
+            merge_diagonal_ops(swp, 0, &raw, &rpool, &merged);
             swp.swap(merged);
+            std::vector<int> outer;
+            if (!finalize_ops(raw, rpool, C + dp.j, &outer, &ops, &pool))
+                return fail(h, QS_ERR_ARG, "a pass needs more outer selector qubits than the planner allows");
+            dp.nouter = (int)outer.size();
+            for (size_t i = 0; i < outer.size(); ++i) dp.outer_q[i] = (int8_t)outer[i];
             dp.op_off = (uint32_t)op0;
             dp.sweep_off = (uint32_t)sw.size();
             if (std::getenv("QOMPSIM_DEBUG_PLAN")) {
-                printf("stage %u pass %zu: j=%d gates=%u sweeps=%zu ops=%zu tile=[", s, p, dp.j, dp.ngates, swp.size(),
-                       ops.size() - op0);
+                int kinds[5] = {0, 0, 0, 0, 0}, sel = 0, half = 0, moves = 0;
+                for (size_t o = op0; o < ops.size(); ++o) {
+                    const int c = ops[o].code;
+                    const int kind = c == qs::OPC_SCALAR ? 0 : c < qs::OPC_M2 ? 1 : c < qs::OPC_D4 ? 2
+                                   : c < qs::OPC_M4 ? 3 : 4;
+                    ++kinds[kind];
+                    sel += ops[o].nsel;
+                    half += (c >= qs::OPC_D2H && c < qs::OPC_M2) || (c >= qs::OPC_D4H && c < qs::OPC_M4);
+                    moves += (c >= qs::OPC_X && c < qs::OPC_D4) || c >= qs::OPC_SWAP;
+                }
+                printf("stage %u pass %zu: j=%d gates=%u sweeps=%zu ops=%zu (scalar %d d2 %d m2 %d d4 %d m4 %d, "
+                       "half-diagonal %d, moves %d, selectors %d, outer %d)%s tile=[", s, p, dp.j, dp.ngates,
+                       swp.size(), ops.size() - op0, kinds[0], kinds[1], kinds[2], kinds[3], kinds[4], half, moves,
+                       sel, dp.nouter, dp.final && !P.identity() ? " +perm" : "");
                 for (int t : pl[p].tile) printf(" %d", t);
                 printf(" ]\n");
             }
@@ -1232,6 +1374,8 @@ qs_status qs_apply_circuit(qs_state *h) {
             a.sweeps = h->sweeps_dev + dp.sweep_off;
             a.nsweeps = (int)dp.nsweeps;
             a.rb = dp.rb;
+            a.nouter = dp.nouter;
+            for (int k = 0; k < qs::kMaxOuterSel; ++k) a.outer_q[k] = dp.outer_q[k];
             a.codec = h->codec;
             a.meta_in = h->meta[h->mcur];
             a.arena_in = h->arena[h->cur];
@@ -1824,8 +1968,8 @@ qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) 
     const int tl = env_int("QOMPSIM_DENSE_TILE_LOG2", h->f64 ? 12 : 13);
     const int tile_log2 = std::min<int>((int)h->n, std::min<int>(tl, C + qs::kMaxTileQubits));
     const int jmax = tile_log2 - C;
-    const int RBmain = h->f64 ? qs::kRegBitsF64 : qs::kRegBitsF32;
-    if ((int)h->n < 3) return qs_dense_apply_gates_pergate(h, gates, count);
+    const int RB = qs::kRegBits;
+    if ((int)h->n < RB) return qs_dense_apply_gates_pergate(h, gates, count);
     std::vector<uint32_t> ids(count);
     for (size_t i = 0; i < count; ++i) ids[i] = (uint32_t)i;
     auto pl = plan_passes(ids, cg, C, jmax, std::min(jmax, 3), C, (int)h->n);
@@ -1835,22 +1979,26 @@ qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) 
     std::vector<cplx> pool;
     std::vector<std::pair<size_t, size_t>> sweep_ranges;
     std::vector<size_t> op_offsets;
-    std::vector<int> pass_rb;
+    std::vector<std::vector<int>> outers;
     for (auto &p : pl) {
         // a tile must hold at least the RB register bits
         std::set<int> t(p.tile.begin(), p.tile.end());
-        for (int q = C; q < (int)h->n && C + (int)t.size() < RBmain; ++q) t.insert(q);
+        for (int q = C; q < (int)h->n && C + (int)t.size() < RB; ++q) t.insert(q);
         p.tile.assign(t.begin(), t.end());
-        const int RB = C + (int)t.size() >= RBmain ? RBmain : 3;
-        pass_rb.push_back(RB);
         const size_t g0 = kg.size();
         for (uint32_t gi : p.gates) kg.push_back(to_kgate(cg[gi], p.tile, C));
         auto swp = plan_sweeps(kg, g0, kg.size(), C + (int)p.tile.size(), RB);
         const size_t op0 = ops.size();
-        build_ops(kg, g0, swp, RB, &ops, &pool);
+        std::vector<RawOp> raw;
+        std::vector<cplx> rpool;
+        build_ops(kg, g0, swp, RB, &raw, &rpool);
         std::vector<qs::Sweep> merged;
-        merge_diagonal_ops(swp, op0, &ops, &pool, &merged);
+        merge_diagonal_ops(swp, 0, &raw, &rpool, &merged);
         swp.swap(merged);
+        std::vector<int> outer;
+        if (!finalize_ops(raw, rpool, C + (int)p.tile.size(), &outer, &ops, &pool))
+            return dfail(h, QS_ERR_ARG, "a pass needs more outer selector qubits than the planner allows");
+        outers.push_back(outer);
         op_offsets.push_back(op0);
         sweep_ranges.push_back({sw.size(), swp.size()});
         sw.insert(sw.end(), swp.begin(), swp.end());
@@ -1901,7 +2049,9 @@ qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) 
         a.pool = h->pool;
         a.sweeps = h->sw + sweep_ranges[pi].first;
         a.nsweeps = (int)sweep_ranges[pi].second;
-        a.rb = pass_rb[pi];
+        a.rb = RB;
+        a.nouter = (int)outers[pi].size();
+        for (size_t k = 0; k < outers[pi].size(); ++k) a.outer_q[k] = (int8_t)outers[pi][k];
         a.state = h->state;
         off += p.gates.size();
         CUDA_TRY(h, qs::launch_dense_pass(h->f64, a, tile_log2, h->stream));

@@ -16,7 +16,9 @@ constexpr int kMaxPerLane = (2 << kMaxChunkLog2) / 32;
 // Largest tile: 2^14 amplitudes; at most kMaxTileQubits qubits above the chunk.
 constexpr int kMaxTileLog2 = 14;
 constexpr int kMaxTileQubits = 10;
-constexpr int kPassThreads = 256;
+// Threads of the per-chunk codec kernels (readout, norm, encode, codec tests):
+// one warp per chunk, four warps per CTA.
+constexpr int kPassThreads = 128;
 
 // Header of one encoded chunk (16 bytes).  offset is a byte offset into the
 // payload arena; the payload is 128 * rows bytes (see codec.cuh).
@@ -42,37 +44,55 @@ struct KGate {
     double m[32];
 };
 
-// Register blocking: a sweep applies gates g0..g1-1 of a pass in one pass
+// Register blocking: a sweep applies ops g0..g1-1 of a pass in one pass
 // over the tile in shared memory.  Each thread holds 2^RB amplitudes whose
 // tile indices differ in the sweep's RB tile bits `sbits` (ascending); every
-// gate of the sweep mixes amplitudes only along those bits (diagonal action
-// on any other bit is allowed).  RB = 3 for complex128, 4 for complex64.
-constexpr int kRegBitsF64 = 3;
-constexpr int kRegBitsF32 = 4;
-constexpr int kMaxRegBits = 5;
+// op of the sweep mixes amplitudes only along those bits (diagonal action on
+// any other bit is allowed).  RB = 4 for both precisions: 16 amplitudes per
+// group keep every op's arithmetic independent across the group, which is
+// what hides the latency of the op stream.
+constexpr int kRegBits = 4;
+constexpr int kRegBitsF64 = kRegBits;
+constexpr int kRegBitsF32 = kRegBits;
+constexpr int kMaxRegBits = kRegBits;
 struct Sweep {
     int32_t g0, g1;
     int32_t sbits[6];
 };
-// Threads of the fused pass kernels (compressed and dense): 4 warps, three
-// CTAs per SM, so that a thread can hold 2^RB amplitudes in registers.
+// Threads of the fused pass kernels (compressed and dense): 4 warps per CTA.
 constexpr int kSweepThreads = 128;
 
-// A gate resolved against its sweep (host-built).  Register bits k0/k1 index
-// the sweep bits; the gate's other qubits are fixed for a register group and
-// select one of 2^nsel pre-computed sub-matrix variants: selector source
-// sel[j] < 64 is a tile bit (its value comes from the group), sel[j] >= 64 is
-// qubit sel[j]-64 outside the tile (its value comes from the tile).
-enum : uint8_t { OP_SCALAR = 0, OP_D2 = 1, OP_M2 = 2, OP_D4 = 3, OP_M4 = 4 };
+// One register op (host-built, 16 bytes).  `code` names the action and the
+// register bits it acts on; the gate's other qubits are fixed for a register
+// group and select one of 2^nsel pre-computed variants: sel[j] is a bit
+// position in the group word W = (tile index of the group's element 0) |
+// (outer selector bits << tile bits), unused slots hold 31 (always 0 in W).
+//   OPC_SCALAR           z *= m[0]                (lazy: one factor per group)
+//   OPC_D2  + k          diag(m0, m1) on bit k
+//   OPC_D2H + k          diag(1,  m0) on bit k    (only the bit-1 half)
+//   OPC_M2  + k          2x2 matrix m0..m3 on bit k
+//   OPC_X   + k          swap the halves of bit k (Pauli X, no arithmetic)
+//   OPC_D4  + (a*8+b)    diag(m0..m3) on bits a < b (matrix bit 0 <-> a)
+//   OPC_D4H + (a*8+b)    diag(1, m0, m1, m2) on bits a < b
+//   OPC_M4  + (a*8+b)    4x4 matrix m0..m15 on bits a < b
+//   OPC_SWAP + (a*8+b)   exchange bits a and b (no arithmetic)
+enum : uint8_t {
+    OPC_SCALAR = 0, OPC_D2 = 8, OPC_D2H = 16, OPC_M2 = 24, OPC_X = 32,
+    OPC_D4 = 64, OPC_D4H = 96, OPC_M4 = 128, OPC_SWAP = 160
+};
 constexpr int kMaxSel = 4;
+constexpr uint8_t kSelNone = 31;
 struct ROp {
-    uint8_t kind;
-    uint8_t k0, k1;      // register bits; for D4/M4 k0 <-> matrix bit 0
+    uint8_t code;
     uint8_t nsel;        // 0..kMaxSel selector bits
     uint8_t sel[kMaxSel];
+    uint8_t pad[2];
     uint32_t mat;        // pool index of variant 0 (complex entries)
-    uint32_t vstride;    // complex entries per variant: 1, 2, 4 or 16
+    uint32_t vstride;    // complex entries per variant
 };
+// Outer qubits (outside the tile) that select variants: at most this many per
+// pass, so that tile bits + outer bits stay below bit 31 of W.
+constexpr int kMaxOuterSel = 16;
 static_assert(sizeof(ROp) == 16, "ROp is one 16-byte load");
 static_assert(sizeof(KGate) == 288, "KGate layout");
 
@@ -102,7 +122,7 @@ struct PassArgs {
     const void *pool;                   // double2 (complex128) or float2 (complex64)
     const Sweep *sweeps;
     int32_t nsweeps;
-    int32_t rb;                         // register bits of the sweeps (3 or the dtype's RB)
+    int32_t rb;                         // register bits of the sweeps (kRegBits)
     CodecParams codec;
     const ChunkMeta *meta_in;
     const uint32_t *arena_in;
@@ -119,6 +139,8 @@ struct PassArgs {
     int32_t *error;                     // 1 = arena overflow
     unsigned long long *stats;          // [0] bytes read [1] bytes written [2] tiles
     ChunkPerm perm;                     // chunk c of the pass is stored as chunk perm(c)
+    int32_t nouter;                     // outer selector qubits of the pass
+    int8_t outer_q[kMaxOuterSel];       // their global qubit indices (bit nb + i of W)
 };
 
 // A pass that only permutes chunk headers: meta_out[perm(c)] = meta_in[c]
@@ -149,6 +171,8 @@ struct DensePassArgs {
     int32_t nsweeps;
     int32_t rb;
     void *state;
+    int32_t nouter;
+    int8_t outer_q[kMaxOuterSel];
 };
 
 // A Pauli string as the expectation kernels read it: P|x> = i^ny (-1)^{|x & z|} |x ^ x_flip>.

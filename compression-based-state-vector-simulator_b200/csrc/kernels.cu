@@ -141,112 +141,123 @@ __device__ __forceinline__ void r_diag4(T (&v)[NS], T d0, T d1, T d2, T d3) {
 }
 
 template <typename T>
-__device__ __forceinline__ bool is_one(T c) { return c.x == 1 && c.y == 0; }
-
-template <typename T>
 __device__ __forceinline__ T c_one() { T r; r.x = 1; r.y = 0; return r; }
 
-// Pending diagonal factors of a register group: the amplitude with register
-// index s still has to be multiplied by z * prod_k (bit k of s ? d1[k] : d0[k]).
-// Diagonal gates accumulate here (one complex product per gate and group);
-// a mixing gate on bit k first applies the factors of bit k.
-template <int RB, typename T>
-struct Pending {
-    T z, d0[RB], d1[RB];
-    __device__ __forceinline__ void reset() {
-        z = c_one<T>();
+template <int NS, int K, typename T>
+__device__ __forceinline__ void r_half2(T (&v)[NS], T d1) {
 #pragma unroll
-        for (int k = 0; k < RB; ++k) d0[k] = d1[k] = c_one<T>();
-    }
-};
-
-template <int RB, typename T>
-__device__ __forceinline__ void pend_d2(Pending<RB, T> &p, int k, T a, T b) {
-#define QS_PD(K)                                         \
-    case K:                                              \
-        if constexpr (K < RB) {                          \
-            p.d0[K] = cmul(p.d0[K], a);                  \
-            p.d1[K] = cmul(p.d1[K], b);                  \
-        }                                                \
-        break;
-    switch (k) { QS_PD(0) QS_PD(1) QS_PD(2) QS_PD(3) QS_PD(4) default: break; }
-#undef QS_PD
+    for (int s = 0; s < NS; ++s)
+        if ((s >> K) & 1) v[s] = cmul(d1, v[s]);
 }
 
-template <int RB, typename T>
-__device__ __forceinline__ void flush_bit(T (&v)[1 << RB], Pending<RB, T> &p, int k) {
-    constexpr int NS = 1 << RB;
-#define QS_FB(K)                                                          \
-    case K:                                                               \
-        if constexpr (K < RB) {                                           \
-            if (!is_one(p.d0[K]) || !is_one(p.d1[K])) {                   \
-                r_diag2<NS, K>(v, p.d0[K], p.d1[K]);                      \
-                p.d0[K] = p.d1[K] = c_one<T>();                           \
-            }                                                             \
-        }                                                                 \
-        break;
-    switch (k) { QS_FB(0) QS_FB(1) QS_FB(2) QS_FB(3) QS_FB(4) default: break; }
-#undef QS_FB
-}
-
-template <int RB, typename T>
-__device__ __forceinline__ void flush_all(T (&v)[1 << RB], Pending<RB, T> &p) {
-    constexpr int NS = 1 << RB;
-    if (!is_one(p.z)) {  // fold the scalar into bit 0
-        p.d0[0] = cmul(p.d0[0], p.z);
-        p.d1[0] = cmul(p.d1[0], p.z);
-        p.z = c_one<T>();
-    }
+template <int NS, int KA, int KB, typename T>
+__device__ __forceinline__ void r_half4(T (&v)[NS], T d1, T d2, T d3) {
 #pragma unroll
-    for (int k = 0; k < RB; ++k) {
-        if (!is_one(p.d0[k]) || !is_one(p.d1[k])) {
-#pragma unroll
-            for (int s = 0; s < NS; ++s) v[s] = cmul(((s >> k) & 1) ? p.d1[k] : p.d0[k], v[s]);
-            p.d0[k] = p.d1[k] = c_one<T>();
-        }
+    for (int s = 0; s < NS; ++s) {
+        const int k = ((s >> KA) & 1) | (((s >> KB) & 1) << 1);
+        if (k) v[s] = cmul(k == 1 ? d1 : (k == 2 ? d2 : d3), v[s]);
     }
 }
 
-template <int RB, typename T>
-__device__ __forceinline__ void d_m2(T (&v)[1 << RB], int k, const T *m) {
-    constexpr int NS = 1 << RB;
-#define QS_CASE2(K)                                               \
-    case K:                                                       \
-        if constexpr (K < RB) r_2x2<NS, K>(v, m[0], m[1], m[2], m[3]); \
-        break;
-    switch (k) { QS_CASE2(0) QS_CASE2(1) QS_CASE2(2) QS_CASE2(3) QS_CASE2(4) default: break; }
-#undef QS_CASE2
+template <int NS, int K, typename T>
+__device__ __forceinline__ void r_x(T (&v)[NS]) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        if ((s >> K) & 1) continue;
+        const T t = v[s];
+        v[s] = v[s | (1 << K)];
+        v[s | (1 << K)] = t;
+    }
 }
 
+template <int NS, int KA, int KB, typename T>
+__device__ __forceinline__ void r_swap(T (&v)[NS]) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        if (((s >> KA) & 1) || ((s >> KB) & 1)) continue;
+        const T t = v[s | (1 << KA)];
+        v[s | (1 << KA)] = v[s | (1 << KB)];
+        v[s | (1 << KB)] = t;
+    }
+}
+
+// One register op on a group (codes in internal.h).  z collects the group's
+// scalar factors and is applied when the group is stored.
 template <int RB, typename T>
-__device__ __forceinline__ void d_44(T (&v)[1 << RB], int ka, int kb, bool diag, const T *m) {
+__device__ __forceinline__ void apply_rop(T (&v)[1 << RB], T &z, int code, const T *__restrict__ m) {
     constexpr int NS = 1 << RB;
-#define QS_CASE4(A, B)                                                            \
-    case (A) * 8 + (B):                                                           \
-        if constexpr ((A) < RB && (B) < RB && (A) != (B)) {                       \
-            if (diag) r_diag4<NS, A, B>(v, m[0], m[1], m[2], m[3]);               \
-            else r_4x4<NS, A, B>(v, m);                                           \
-        }                                                                         \
+#define QS_K(BASE, K, ...) \
+    case BASE + K:         \
+        if constexpr (K < RB) { __VA_ARGS__; } \
         break;
-    switch (ka * 8 + kb) {
-        QS_CASE4(0, 1) QS_CASE4(0, 2) QS_CASE4(0, 3) QS_CASE4(0, 4) QS_CASE4(1, 0) QS_CASE4(1, 2)
-        QS_CASE4(1, 3) QS_CASE4(1, 4) QS_CASE4(2, 0) QS_CASE4(2, 1) QS_CASE4(2, 3) QS_CASE4(2, 4)
-        QS_CASE4(3, 0) QS_CASE4(3, 1) QS_CASE4(3, 2) QS_CASE4(3, 4) QS_CASE4(4, 0) QS_CASE4(4, 1)
-        QS_CASE4(4, 2) QS_CASE4(4, 3)
+#define QS_P(BASE, A, B, ...) \
+    case BASE + (A) * 8 + (B): \
+        if constexpr ((A) < RB && (B) < RB) { __VA_ARGS__; } \
+        break;
+#define QS_ALLK(BASE, F) F(BASE, 0) F(BASE, 1) F(BASE, 2) F(BASE, 3) F(BASE, 4)
+#define QS_ALLP(BASE, F) F(BASE, 0, 1) F(BASE, 0, 2) F(BASE, 0, 3) F(BASE, 0, 4) F(BASE, 1, 2) \
+    F(BASE, 1, 3) F(BASE, 1, 4) F(BASE, 2, 3) F(BASE, 2, 4) F(BASE, 3, 4)
+#define QS_D2(B, K) QS_K(B, K, r_diag2<NS, K>(v, m[0], m[1]))
+#define QS_D2H(B, K) QS_K(B, K, r_half2<NS, K>(v, m[0]))
+#define QS_M2(B, K) QS_K(B, K, r_2x2<NS, K>(v, m[0], m[1], m[2], m[3]))
+#define QS_X(B, K) QS_K(B, K, r_x<NS, K>(v))
+#define QS_D4(B, A, C) QS_P(B, A, C, r_diag4<NS, A, C>(v, m[0], m[1], m[2], m[3]))
+#define QS_D4H(B, A, C) QS_P(B, A, C, r_half4<NS, A, C>(v, m[0], m[1], m[2]))
+#define QS_M4(B, A, C) QS_P(B, A, C, r_4x4<NS, A, C>(v, m))
+#define QS_SW(B, A, C) QS_P(B, A, C, r_swap<NS, A, C>(v))
+    switch (code) {
+        case OPC_SCALAR: z = cmul(z, m[0]); break;
+        QS_ALLK(OPC_D2, QS_D2)
+        QS_ALLK(OPC_D2H, QS_D2H)
+        QS_ALLK(OPC_M2, QS_M2)
+        QS_ALLK(OPC_X, QS_X)
+        QS_ALLP(OPC_D4, QS_D4)
+        QS_ALLP(OPC_D4H, QS_D4H)
+        QS_ALLP(OPC_M4, QS_M4)
+        QS_ALLP(OPC_SWAP, QS_SW)
         default: break;
     }
-#undef QS_CASE4
+#undef QS_K
+#undef QS_P
+#undef QS_ALLK
+#undef QS_ALLP
+#undef QS_D2
+#undef QS_D2H
+#undef QS_M2
+#undef QS_X
+#undef QS_D4
+#undef QS_D4H
+#undef QS_M4
+#undef QS_SW
 }
 
-// Apply every sweep of a pass to a tile of 2^nb elements whose element 0 is
-// global amplitude base_amp.
+// Variant index of an op for a group with word W (selector bits of W).
+__device__ __forceinline__ uint32_t rop_variant(const ROp &o, uint32_t W) {
+    uint32_t var = 0;
+    if (o.nsel) {
+#pragma unroll
+        for (int j = 0; j < kMaxSel; ++j) var |= ((W >> o.sel[j]) & 1u) << j;
+    }
+    return var;
+}
+
+// Outer selector word of a tile whose element 0 is global amplitude base_amp.
+__device__ __forceinline__ uint32_t outer_word(uint64_t base_amp, const int8_t *outer_q, int nouter) {
+    uint32_t w = 0;
+    for (int i = 0; i < nouter; ++i) w |= (uint32_t)((base_amp >> outer_q[i]) & 1u) << i;
+    return w;
+}
+
+// Apply every sweep of a pass to a tile of 2^nb elements.  ow is the tile's
+// outer selector word.
 template <typename R, int RB>
 __device__ void tile_sweeps(typename Cplx<R>::T *tile, int nb, int swm, const Sweep *__restrict__ sweeps,
                             int nsweeps, const ROp *__restrict__ ops, const typename Cplx<R>::T *__restrict__ pool,
-                            uint64_t base_amp) {
+                            uint32_t ow) {
     using T = typename Cplx<R>::T;
     constexpr int NS = 1 << RB;
     const int groups = 1 << (nb - RB);
+    const uint32_t wo = ow << nb;
     for (int w = 0; w < nsweeps; ++w) {
         const Sweep sw = sweeps[w];
         int sb[RB];
@@ -267,42 +278,19 @@ __device__ void tile_sweeps(typename Cplx<R>::T *tile, int nb, int swm, const Sw
                 const int t = sb[k];
                 base = ((base >> t) << (t + 1)) | (base & ((1 << t) - 1));
             }
+            const uint32_t W = (uint32_t)base | wo;
             T v[NS];
 #pragma unroll
             for (int s = 0; s < NS; ++s) v[s] = tile[swz<R>(base | off[s], swm)];
-            Pending<RB, T> pend;
-            pend.reset();
-            ROp nxt{};
-            if (sw.g0 < sw.g1) nxt = ops[sw.g0];
+            T z = c_one<T>();
             for (int k = sw.g0; k < sw.g1; ++k) {
-                const ROp o = nxt;
-                if (k + 1 < sw.g1) nxt = ops[k + 1];
-                int var = 0;
-#pragma unroll
-                for (int jj = 0; jj < kMaxSel; ++jj) {
-                    if (jj < o.nsel) {
-                        const int src = o.sel[jj];
-                        const int bit = src < 64 ? (base >> src) & 1 : (int)((base_amp >> (src - 64)) & 1);
-                        var |= bit << jj;
-                    }
-                }
-                const T *m = pool + o.mat + (uint32_t)var * o.vstride;
-                switch (o.kind) {
-                    case OP_SCALAR: pend.z = cmul(pend.z, m[0]); break;
-                    case OP_D2: pend_d2<RB>(pend, o.k0, m[0], m[1]); break;
-                    case OP_M2:
-                        flush_bit<RB>(v, pend, o.k0);
-                        d_m2<RB>(v, o.k0, m);
-                        break;
-                    case OP_D4: d_44<RB>(v, o.k0, o.k1, true, m); break;
-                    default:
-                        flush_bit<RB>(v, pend, o.k0);
-                        flush_bit<RB>(v, pend, o.k1);
-                        d_44<RB>(v, o.k0, o.k1, false, m);
-                        break;
-                }
+                const ROp o = ops[k];
+                apply_rop<RB>(v, z, o.code, pool + o.mat + rop_variant(o, W) * o.vstride);
             }
-            flush_all<RB>(v, pend);
+            if (z.x != R(1) || z.y != R(0)) {
+#pragma unroll
+                for (int s = 0; s < NS; ++s) v[s] = cmul(z, v[s]);
+            }
 #pragma unroll
             for (int s = 0; s < NS; ++s) tile[swz<R>(base | off[s], swm)] = v[s];
         }
@@ -323,13 +311,17 @@ struct TileSlot {
     __device__ __forceinline__ int operator()(int c) const { return 2 * swz<R>(elem0 + (c >> 1), swm) + (c & 1); }
 };
 
+// Words of the per-warp staging area of decode_chunk: one row more than a
+// chunk can use, so that the look-ahead word of the last row stays inside.
+constexpr int kStageWords = (kMaxPerLane + 1) * 32;
+
 template <typename R, typename Slot = LinearSlot>
 __device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena, const ChunkMeta md,
                                              int per_lane, CodecParams p, R *comp, uint32_t *wstage,
                                              int lane, Slot slot = Slot()) {
     const uint32_t w = md.width;
     if (w == 0) {
-        const R v = dequantize(md.base, p, R());
+        const R v = dequantize_hot(md.base, p, R());
         for (int i = 0; i < per_lane; ++i) comp[slot(lane + 32 * i)] = v;
         return;
     }
@@ -342,19 +334,16 @@ __device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena,
 #pragma unroll
     for (int r = 0; r < kMaxPerLane; ++r)
         if (r < (int)rows) wstage[r * 32 + lane] = tmp[r];
-    uint64_t buf = 0;
-    uint32_t nbits = 0, r = 0;
-    const uint64_t mask = (w == 32) ? 0xffffffffull : ((1ull << w) - 1);
-    for (int i = 0; i < per_lane; ++i) {
-        if (nbits < w) {
-            buf |= (uint64_t)wstage[r * 32 + lane] << nbits;
-            ++r;
-            nbits += 32;
+    // element i of this lane's stream starts at bit i*w: every element is
+    // extracted independently (one funnel shift); a lane reads only its own words
+    const uint32_t mask = (w >= 32) ? 0xffffffffu : ((1u << w) - 1u);
+#pragma unroll
+    for (int i = 0; i < kMaxPerLane; ++i) {
+        if (i < per_lane) {
+            const uint32_t bit = (uint32_t)i * w, r = bit >> 5;
+            const uint32_t u = __funnelshift_r(wstage[r * 32 + lane], wstage[(r + 1) * 32 + lane], bit & 31) & mask;
+            comp[slot(lane + 32 * i)] = dequantize_hot((int32_t)((uint32_t)md.base + u), p, R());
         }
-        const uint32_t u = (uint32_t)(buf & mask);
-        buf >>= w;
-        nbits -= w;
-        comp[slot(lane + 32 * i)] = dequantize((int32_t)((uint32_t)md.base + u), p, R());
     }
 }
 
@@ -376,7 +365,7 @@ __device__ __forceinline__ void quantize_chunk(R *comp, int per_lane, CodecParam
 #pragma unroll
     for (int i = 0; i < kMaxPerLane; ++i) {
         if (i < per_lane) {
-            const int32_t q = quantize(v[i], p);
+            const int32_t q = quantize_hot(v[i], p);
             codes[lane + 32 * i] = q;
             lo = min(lo, q);
             hi = max(hi, q);
@@ -421,11 +410,9 @@ __device__ __forceinline__ uint64_t apply_perm(const ChunkPerm &p, uint64_t c) {
     return o ^ p.flip;
 }
 
-__device__ __forceinline__ size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-
 size_t pass_smem_bytes(bool f64, int nb, int j) {
     const size_t tile = (f64 ? 16 : 8) << nb;
-    const size_t stage = (size_t)(kSweepThreads / 32) * kMaxPerLane * 32 * 4;
+    const size_t stage = (size_t)(kSweepThreads / 32) * kStageWords * 4;
     const size_t tables = ((size_t)3 * 4 << j) + 8;
     const size_t offs = (size_t)8 << j;
     return tile + stage + ((tables + 7) / 8) * 8 + offs;
@@ -439,7 +426,9 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
     __shared__ unsigned long long s_tile_off;
     __shared__ int s_flag;
     __shared__ int32_t s_tq[kMaxTileQubits];
+    __shared__ int8_t s_oq[kMaxOuterSel];
     if (threadIdx.x < kMaxTileQubits) s_tq[threadIdx.x] = a.tq[threadIdx.x];
+    if (threadIdx.x < kMaxOuterSel) s_oq[threadIdx.x] = a.outer_q[threadIdx.x];
     __syncthreads();
 
     const int C = a.C, j = a.j, nb = C + j;
@@ -452,8 +441,8 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
 
     T *tile = reinterpret_cast<T *>(smem);
     uint32_t *stage_all = reinterpret_cast<uint32_t *>(smem + (sizeof(T) << nb));
-    uint32_t *wstage = stage_all + warp * (kMaxPerLane * 32);
-    int32_t *s_base = reinterpret_cast<int32_t *>(stage_all + nwarps * (kMaxPerLane * 32));
+    uint32_t *wstage = stage_all + warp * kStageWords;
+    int32_t *s_base = reinterpret_cast<int32_t *>(stage_all + nwarps * kStageWords);
     uint32_t *s_width = reinterpret_cast<uint32_t *>(s_base + nchunks);
     uint32_t *s_nz = s_width + nchunks;
     unsigned long long *s_off = reinterpret_cast<unsigned long long *>(
@@ -487,8 +476,8 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
         __syncthreads();
 
         // ---- gates
-        const uint64_t base_amp = chunk_base << C;
-        tile_sweeps<R, RB>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool), base_amp);
+        tile_sweeps<R, RB>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool),
+                           outer_word(chunk_base << C, s_oq, a.nouter));
 
         // ---- quantise (codes replace values in shared memory)
         for (int c = warp; c < nchunks; c += nwarps) {
@@ -506,22 +495,36 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
         }
         __syncthreads();
 
-        // ---- reserve the tile's output bytes with one atomic
-        if (threadIdx.x == 0) {
-            unsigned long long total = 0;
-            for (int c = 0; c < nchunks; ++c) {
-                s_off[c] = total;
-                total += payload_bytes(C, s_width[c]);
+        // ---- reserve the tile's output bytes with one atomic: warp 0 scans
+        // the chunk sizes (each lane a run of consecutive chunks)
+        if (warp == 0) {
+            const int per = (nchunks + 31) >> 5;
+            const int c0 = lane * per;
+            unsigned long long mine = 0;
+            for (int c = c0; c < c0 + per && c < nchunks; ++c) mine += payload_bytes(C, s_width[c]);
+            unsigned long long incl = mine;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
             }
-            const unsigned long long off = atomicAdd(a.bump, total);
-            if (off + total > a.capacity) {
-                atomicExch(a.error, 1);
-                s_flag = 1;
-            } else {
-                s_flag = 0;
+            unsigned long long run = incl - mine;
+            for (int c = c0; c < c0 + per && c < nchunks; ++c) {
+                s_off[c] = run;
+                run += payload_bytes(C, s_width[c]);
             }
-            s_tile_off = off;
-            wr += total + (unsigned long long)nchunks * sizeof(ChunkMeta);
+            const unsigned long long total = __shfl_sync(0xffffffffu, incl, 31);
+            if (lane == 0) {
+                const unsigned long long off = atomicAdd(a.bump, total);
+                if (off + total > a.capacity) {
+                    atomicExch(a.error, 1);
+                    s_flag = 1;
+                } else {
+                    s_flag = 0;
+                }
+                s_tile_off = off;
+                wr += total + (unsigned long long)nchunks * sizeof(ChunkMeta);
+            }
         }
         __syncthreads();
         if (s_flag) break;
@@ -610,7 +613,9 @@ __global__ void __launch_bounds__(kSweepThreads, 3) dense_pass_kernel(const Dens
     const int cmask = (1 << C) - 1;
     const int swm = swizzle_mask<R>(C);
     __shared__ int32_t s_tq[kMaxTileQubits];
+    __shared__ int8_t s_oq[kMaxOuterSel];
     if (threadIdx.x < kMaxTileQubits) s_tq[threadIdx.x] = a.tq[threadIdx.x];
+    if (threadIdx.x < kMaxOuterSel) s_oq[threadIdx.x] = a.outer_q[threadIdx.x];
     __syncthreads();
     for (uint64_t tile_id = blockIdx.x; tile_id < a.n_tiles; tile_id += gridDim.x) {
         const uint64_t chunk_base = insert_zero_bits(tile_id, s_tq, j);
@@ -620,7 +625,7 @@ __global__ void __launch_bounds__(kSweepThreads, 3) dense_pass_kernel(const Dens
         }
         __syncthreads();
         tile_sweeps<R, RB>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool),
-                           chunk_base << C);
+                           outer_word(chunk_base << C, s_oq, a.nouter));
         for (int e = threadIdx.x; e < size; e += blockDim.x) {
             const uint64_t amp = ((chunk_base | deposit_bits((uint32_t)(e >> C), s_tq, j)) << C) | (uint64_t)(e & cmask);
             st[amp] = tile[swz<R>(e, swm)];
@@ -738,7 +743,7 @@ __global__ void sum_mask_bytes_kernel(const uint8_t *mask, const unsigned long l
 template <typename R>
 __global__ void readout_kernel(const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B, int C,
                                CodecParams p, uint64_t chunk0, uint64_t nchunks, double *out, double scale) {
-    __shared__ uint32_t stage[kPassThreads / 32][kMaxPerLane * 32];
+    __shared__ uint32_t stage[kPassThreads / 32][kStageWords];
     __shared__ R vals[kPassThreads / 32][2 << kMaxChunkLog2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ncomp = 2 << C, per_lane = ncomp >> 5;
@@ -760,7 +765,7 @@ __global__ void readout_kernel(const ChunkMeta *meta, const uint32_t *arena, con
 template <typename R>
 __global__ void norm_kernel(const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B, int C,
                             CodecParams p, uint64_t nchunks, double *out) {
-    __shared__ uint32_t stage[kPassThreads / 32][kMaxPerLane * 32];
+    __shared__ uint32_t stage[kPassThreads / 32][kStageWords];
     __shared__ R vals[kPassThreads / 32][2 << kMaxChunkLog2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ncomp = 2 << C, per_lane = ncomp >> 5;
@@ -826,7 +831,7 @@ __global__ void encode_kernel(const double *vals, int B, int C, CodecParams p, u
 template <typename R>
 __global__ void codec_test_kernel(const R *vals, int C, CodecParams p, uint64_t nchunks, uint32_t *words,
                                   int32_t *bases, uint32_t *widths, R *decoded) {
-    __shared__ uint32_t stage[kPassThreads / 32][kMaxPerLane * 32];
+    __shared__ uint32_t stage[kPassThreads / 32][kStageWords];
     __shared__ R buf[kPassThreads / 32][2 << kMaxChunkLog2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ncomp = 2 << C, per_lane = ncomp >> 5;
@@ -906,7 +911,7 @@ __global__ void __launch_bounds__(kExpectThreads) expect_kernel(const ExpectArgs
     const int blk_shift = a.B - C;
     const int swm = swizzle_mask<R>(C);
     T *tile = reinterpret_cast<T *>(smem);
-    uint32_t *wstage = reinterpret_cast<uint32_t *>(smem + (sizeof(T) << nb)) + warp * (kMaxPerLane * 32);
+    uint32_t *wstage = reinterpret_cast<uint32_t *>(smem + (sizeof(T) << nb)) + warp * kStageWords;
     for (int i = threadIdx.x; i < 2 * a.nterms; i += blockDim.x) s_acc[i] = 0.0;
     if (threadIdx.x < kMaxTileQubits) s_tq[threadIdx.x] = a.tq[threadIdx.x];
     __syncthreads();
@@ -1168,8 +1173,8 @@ static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
 }
 
 cudaError_t launch_pass(bool f64, const PassArgs &a, int, cudaStream_t s) {
-    if (f64) return a.rb == kRegBitsF64 ? launch_pass_t<double, kRegBitsF64>(a, s) : launch_pass_t<double, 3>(a, s);
-    return a.rb == kRegBitsF32 ? launch_pass_t<float, kRegBitsF32>(a, s) : launch_pass_t<float, 3>(a, s);
+    if (a.rb != kRegBits || a.C + a.j < kRegBits) return cudaErrorInvalidValue;
+    return f64 ? launch_pass_t<double, kRegBits>(a, s) : launch_pass_t<float, kRegBits>(a, s);
 }
 
 cudaError_t launch_perm_pass(const PermPassArgs &a, cudaStream_t s) {
@@ -1196,8 +1201,8 @@ static cudaError_t launch_dense_pass_t(const DensePassArgs &a, cudaStream_t s) {
 }
 
 cudaError_t launch_dense_pass(bool f64, const DensePassArgs &a, int, cudaStream_t s) {
-    if (f64) return a.rb == kRegBitsF64 ? launch_dense_pass_t<double, kRegBitsF64>(a, s) : launch_dense_pass_t<double, 3>(a, s);
-    return a.rb == kRegBitsF32 ? launch_dense_pass_t<float, kRegBitsF32>(a, s) : launch_dense_pass_t<float, 3>(a, s);
+    if (a.rb != kRegBits || a.C + a.j < kRegBits) return cudaErrorInvalidValue;
+    return f64 ? launch_dense_pass_t<double, kRegBits>(a, s) : launch_dense_pass_t<float, kRegBits>(a, s);
 }
 
 cudaError_t launch_pergate(bool f64, void *state, int n, const KGate *g, cudaStream_t s) {
@@ -1334,7 +1339,7 @@ template <typename R>
 static cudaError_t launch_expect_t(const ExpectArgs &a, cudaStream_t s) {
     if (a.nterms > kMaxTermsPerLaunch) return cudaErrorInvalidValue;
     const int nb = a.C + a.j;
-    const size_t smem = ((size_t)(2 * sizeof(R)) << nb) + (size_t)(kExpectThreads / 32) * kMaxPerLane * 32 * 4;
+    const size_t smem = ((size_t)(2 * sizeof(R)) << nb) + (size_t)(kExpectThreads / 32) * kStageWords * 4;
     cudaError_t e = cudaFuncSetAttribute(expect_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
