@@ -232,6 +232,63 @@ def run_reference(args, spec):
 
 
 # ----------------------------------------------------------------- our arm
+def complex64_leg(spec, circuit, updates_per_step, torch, steps: int = 3):
+    """The same fused gate list through the complex64 compressed pipeline
+    (FP32 gate arithmetic and stored amplitudes, FP64 reductions)."""
+    import qulacs
+    from qulacs import _native
+    cq = qulacs.CompressedQuantumState(spec["n"], spec["block_size"], dtype="complex64", eps_rel=spec["eps_rel"],
+                                       eps_abs=spec["eps_abs"], flags=_native.QS_FLAG_QUIET)
+    cq.partition_and_register_circuit(circuit, spec["inner_size"], 0)
+    for _ in range(3):
+        cq.set_computational_basis(0)
+        cq.apply_circuit()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        cq.set_computational_basis(0)
+        cq.apply_circuit()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    out = {"ms_per_step": ms, "value": updates_per_step / (ms * 1e-3), "unit": UNIT, "steps": steps,
+           "max_sv_bytes": cq.get_max_SV_bytes()}
+    del cq
+    return out
+
+
+def adjoint_leg(torch, n: int = 24, depth: int = 8, reps: int = 3):
+    """Hardware-efficient ansatz n=24, depth 8 (RY RZ per qubit + CNOT ladder,
+    384 parameters), H = sum Z_i Z_i+1 + 0.5 sum X_i: wall time of the energy
+    alone and of energy + adjoint gradient through the public API, each call
+    synchronised."""
+    import qulacs
+    from qompsim import circuits as C
+    from qulacs.torch import energy, energy_and_gradient
+    circ = C.hea(n, depth, seed=0, parametric=True)
+    obs = qulacs.Observable(n)
+    for coef, pauli, qubits in C.hea_observable_terms(n):
+        obs.add_operator(coef, " ".join(f"{p} {q}" for p, q in zip(pauli, qubits)))
+    res = {"workload": f"hea: n={n} depth={depth}, {circ.get_parameter_count()} parameters"}
+    for dtype in ("complex64", "complex128"):
+        energy_and_gradient(circ, obs, dtype)
+        energy(circ, obs, dtype)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            energy(circ, obs, dtype)
+        torch.cuda.synchronize()
+        fwd = (time.perf_counter() - t0) / reps
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            energy_and_gradient(circ, obs, dtype)
+        torch.cuda.synchronize()
+        grad = (time.perf_counter() - t0) / reps
+        res[dtype] = {"energy_ms": fwd * 1e3, "energy_and_gradient_ms": grad * 1e3, "ratio": grad / fwd}
+    return res
+
+
 def run_ours(args, spec):
     import numpy as np
     import torch
@@ -326,6 +383,18 @@ def run_ours(args, spec):
         dense = legs
         dense["compressed_speedup_vs_pergate_c128"] = legs["pergate_c128"]["ms_per_step"] / (ms / args.steps)
 
+    # ---- the same circuit in the complex64 pipeline, and the adjoint gradient of the
+    # hardware-efficient ansatz against its forward pass (rank 0, N=1 only)
+    extra = {}
+    max_sv = cq.get_max_SV_bytes()
+    if rank == 0 and world == 1 and not args.no_legs:
+        del cq  # frees the complex128 store's arena for the complex64 state
+        extra["complex64"] = complex64_leg(spec, circuit, updates_per_step, torch)
+        if dense is not None:
+            extra["complex64"]["speedup_vs_pergate_c128"] = (dense["pergate_c128"]["ms_per_step"]
+                                                             / extra["complex64"]["ms_per_step"])
+        extra["adjoint"] = adjoint_leg(torch)
+
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -351,7 +420,7 @@ def run_ours(args, spec):
                        "gates": circuit.get_gate_count(), "amp_gate_updates_per_step": updates_per_step,
                        "parallelism": f"replicas x{world}",
                        "l2": "compressed store larger than L2 (126 MB); no flush between steps",
-                       "max_sv_bytes": cq.get_max_SV_bytes()},
+                       "max_sv_bytes": max_sv},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
@@ -368,6 +437,7 @@ def run_ours(args, spec):
             "cpu_baseline": cpu,
             "uncompressed": dense,
         }
+        out.update(extra)
         print(json.dumps(out))
     if pg is not None:
         pg.destroy_process_group()
@@ -382,6 +452,7 @@ def main():
     ap.add_argument("--workload", default="qft30")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-dense", action="store_true", help="skip the uncompressed per-gate comparison leg")
+    ap.add_argument("--no-legs", action="store_true", help="skip the complex64 and adjoint-gradient legs")
     args = ap.parse_args()
     spec = workload_spec(args.workload)
     if args.impl == "reference":

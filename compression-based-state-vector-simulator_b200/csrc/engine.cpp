@@ -699,10 +699,13 @@ int env_int(const char *name, int dflt) {
 
 }  // namespace
 
+// A failed call also leaves its error as the thread's last CUDA error; it is
+// cleared here so that the next launch check does not report it again.
 #define CUDA_TRY(h, expr)                                                               \
     do {                                                                                \
         cudaError_t e__ = (expr);                                                       \
         if (e__ != cudaSuccess) {                                                       \
+            (void)cudaGetLastError();                                                   \
             (h)->err = std::string(#expr) + ": " + cudaGetErrorString(e__);             \
             return QS_ERR_CUDA;                                                         \
         }                                                                               \
@@ -752,7 +755,7 @@ struct qs_state {
     qs::ChunkMeta *meta[2] = {nullptr, nullptr};
     uint32_t *arena[2] = {nullptr, nullptr};
     uint64_t capacity = 0;
-    unsigned long long *counters = nullptr;  // [0..1] bump, [2..4] stats, [5] init scratch, [6] header-pass bytes
+    unsigned long long *counters = nullptr;  // [0..1] bump, [2..4] stats, [5] init scratch, [6] header-pass bytes, [7] diagonal-pass total
     uint8_t *mask = nullptr;
     uint32_t *block_nz = nullptr;
     unsigned long long *block_bytes = nullptr, *block_acc = nullptr;
@@ -1601,8 +1604,30 @@ qs_status qs_load_vector(qs_state *h, const double *vec) {
 // ---- Pauli expectation values
 // Terms are batched so that each batch's flip qubits at or above the chunk
 // size fit in one tile; each batch is one read-only pass.
+static bool same_geometry(const qs_state *a, const qs_state *b) {
+    return a->n == b->n && a->B == b->B && a->C == b->C && a->f64 == b->f64 && a->codec.m == b->codec.m &&
+           a->codec.L == b->codec.L;
+}
+
+// Pauli sums over the ket store h, with bra store `bra` (NULL: the ket).
+static qs_status pauli_sums(qs_state *h, const qs_state *bra, const uint64_t *x_masks, const uint64_t *z_masks,
+                            size_t nterms, double *out);
+
 qs_status qs_expectation_pauli(qs_state *h, const uint64_t *x_masks, const uint64_t *z_masks, size_t nterms,
                                double *out) {
+    return pauli_sums(h, nullptr, x_masks, z_masks, nterms, out);
+}
+
+qs_status qs_transition_pauli(const qs_state *bra, qs_state *ket, const uint64_t *x_masks, const uint64_t *z_masks,
+                              size_t nterms, double *out) {
+    if (!bra || !ket) return fail(ket, QS_ERR_ARG, "NULL handle");
+    if (!same_geometry(bra, ket)) return fail(ket, QS_ERR_ARG, "bra and ket differ in qubits, block, chunk, dtype or codec");
+    if (bra->stream != ket->stream) CUDA_TRY(ket, cudaStreamSynchronize(bra->stream));
+    return pauli_sums(ket, bra, x_masks, z_masks, nterms, out);
+}
+
+static qs_status pauli_sums(qs_state *h, const qs_state *bra, const uint64_t *x_masks, const uint64_t *z_masks,
+                            size_t nterms, double *out) {
     if (!h || (nterms && (!x_masks || !z_masks || !out))) return fail(h, QS_ERR_ARG, "NULL argument");
     const int C = (int)h->C;
     const int jmax = std::min(h->tile_log2 - C, qs::kMaxTileQubits);
@@ -1695,6 +1720,11 @@ qs_status qs_expectation_pauli(qs_state *h, const uint64_t *x_masks, const uint6
             a.terms = bdev;
             a.nterms = (int)bt.size();
             a.out = bout;
+            if (bra) {
+                a.meta_bra = bra->meta[bra->mcur];
+                a.arena_bra = bra->arena[bra->cur];
+                a.mask_bra = bra->mask;
+            }
             e = qs::launch_expect(h->f64, a, h->stream);
         }
         std::vector<double> hb(2 * bt.size());
@@ -1708,10 +1738,128 @@ qs_status qs_expectation_pauli(qs_state *h, const uint64_t *x_masks, const uint6
         if (bdev) cudaFree(bdev);
         if (bout) cudaFree(bout);
     }
-    if (e != cudaSuccess) rs = fail(h, QS_ERR_CUDA, std::string("expectation: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        rs = fail(h, QS_ERR_CUDA, std::string("expectation: ") + cudaGetErrorString(e));
+    }
     if (dout) cudaFree(dout);
     if (dterms) cudaFree(dterms);
     return rs;
+}
+
+// ---- out := (sum_t c_t Z^{z_t}) in, one tile pass from in's store into out's
+qs_status qs_apply_diagonal_pauli_sum(qs_state *out, const qs_state *in, const uint64_t *z_masks,
+                                      const double *coefs, size_t nterms) {
+    if (!out || !in) return fail(out, QS_ERR_ARG, "NULL handle");
+    if (out == in) return fail(out, QS_ERR_ARG, "out and in must be different states");
+    if (nterms && (!z_masks || !coefs)) return fail(out, QS_ERR_ARG, "NULL argument");
+    if (nterms > (size_t)qs::kMaxDiagTerms)
+        return fail(out, QS_ERR_ARG, "at most " + std::to_string(qs::kMaxDiagTerms) + " terms");
+    if (!same_geometry(out, in)) return fail(out, QS_ERR_ARG, "in and out differ in qubits, block, chunk, dtype or codec");
+    const uint64_t full = out->n >= 64 ? ~0ull : ((1ull << out->n) - 1);
+    for (size_t t = 0; t < nterms; ++t)
+        if (z_masks[t] & ~full) return fail(out, QS_ERR_ARG, "Pauli term acts outside the register");
+    if (in->stream != out->stream) CUDA_TRY(out, cudaStreamSynchronize(in->stream));
+    cudaStream_t s = out->stream;
+    const int C = (int)out->C;
+    const int jmax = std::min(out->tile_log2 - C, qs::kMaxTileQubits);
+    const int j = std::max(0, std::min<int>({jmax, 3, (int)out->n - C}));
+    std::vector<int> tv;
+    for (int q = C; q < C + j; ++q) tv.push_back(q);
+    if (C + j < qs::kRegBits) return fail(out, QS_ERR_ARG, "state too small for a tile pass");
+    std::vector<qs::PauliTerm> terms(nterms);
+    for (size_t t = 0; t < nterms; ++t) {
+        qs::PauliTerm pt{};
+        for (int q = 0; q < (int)out->n; ++q) {
+            if (!((z_masks[t] >> q) & 1)) continue;
+            if (q < C + j) pt.zt |= 1u << q;  // tile qubits are the lowest C + j
+            else pt.zo |= 1ull << q;
+        }
+        pt.zg = z_masks[t];
+        terms[t] = pt;
+    }
+    qs::PauliTerm *dterms = nullptr;
+    double *dcoef = nullptr;
+    uint32_t *ident = nullptr;
+    auto cleanup = [&]() {
+        if (dterms) cudaFree(dterms);
+        if (dcoef) cudaFree(dcoef);
+        if (ident) cudaFree(ident);
+    };
+    cudaError_t e = cudaMalloc(&dterms, std::max<size_t>(1, nterms) * sizeof(qs::PauliTerm));
+    if (e == cudaSuccess) e = cudaMalloc(&dcoef, std::max<size_t>(1, 2 * nterms) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&ident, out->nb * sizeof(uint32_t));
+    std::vector<uint32_t> hid(out->nb);
+    for (uint32_t b = 0; b < out->nb; ++b) hid[b] = b;
+    if (e == cudaSuccess && nterms)
+        e = cudaMemcpyAsync(dterms, terms.data(), nterms * sizeof(qs::PauliTerm), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && nterms)
+        e = cudaMemcpyAsync(dcoef, coefs, 2 * nterms * sizeof(double), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ident, hid.data(), hid.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    const int o = out->cur ^ 1;
+    if (e == cudaSuccess) e = cudaMemsetAsync(out->counters, 0, 8 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(out->error_dev, 0, sizeof(int32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(out->block_nz, 0, out->nb * sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(out->block_acc, 0, out->nb * sizeof(unsigned long long), s);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        cleanup();
+        return fail(out, QS_ERR_CUDA, std::string("diagonal Pauli sum: ") + cudaGetErrorString(e));
+    }
+    qs::PassArgs a{};
+    a.n = (int)out->n;
+    a.B = (int)out->B;
+    a.C = C;
+    a.j = j;
+    for (int k = 0; k < j; ++k) a.tq[k] = tv[k] - C;
+    a.n_tiles = uint64_t(1) << (out->n - C - j);
+    a.nsweeps = 0;
+    a.rb = qs::kRegBits;
+    a.codec = out->codec;
+    a.meta_in = in->meta[in->mcur];
+    a.arena_in = in->arena[in->cur];
+    a.meta_out = out->meta[out->mcur ^ 1];
+    a.arena_out = out->arena[o];
+    a.bump = out->counters + o;
+    a.capacity = out->capacity;
+    a.block_to_group = ident;
+    a.group_active = in->mask;  // stored blocks of `in` are processed, the others stay zero
+    a.mask = in->mask;
+    a.first_pass = 1;
+    a.final_pass = 1;
+    a.exact_zero = (out->flags & QS_FLAG_EXACT_ZERO_TEST) ? 1 : 0;
+    a.block_nz = out->block_nz;
+    a.block_bytes = out->block_acc;
+    a.error = out->error_dev;
+    a.stats = out->counters + 2;
+    a.perm = identity_perm();
+    a.diag.terms = dterms;
+    a.diag.coefs = dcoef;
+    a.diag.nterms = (int)nterms;
+    e = qs::launch_pass(out->f64, a, out->tile_log2, s);
+    // out keeps in's zero-block mask; its block bytes are the new ones
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out->mask, in->mask, out->nb, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess)
+        e = qs::launch_stage_end(ident, in->mask, out->nb, out->block_nz, out->block_acc, out->mask, out->block_bytes,
+                                 out->counters + 7, s);  // counters were zeroed above
+    int32_t errflag = 0;
+    unsigned long long ctr[8] = {0}, total = 0;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaMemcpy(&errflag, out->error_dev, sizeof(errflag), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(ctr, out->counters, sizeof(ctr), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) total = ctr[7];
+    cleanup();
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return fail(out, QS_ERR_CUDA, std::string("diagonal Pauli sum: ") + cudaGetErrorString(e));
+    }
+    if (errflag)
+        return fail(out, QS_ERR_CAPACITY, "compressed store overflowed its arena; the state is invalid");
+    out->cur = o;
+    out->mcur ^= 1;
+    out->arena_used = ctr[o];
+    out->history.assign(1, total);
+    return QS_OK;
 }
 
 // ---- device checkpoints of the compressed store

@@ -113,6 +113,17 @@ struct ChunkPerm {
     int8_t src[kMaxPermBits], dst[kMaxPermBits];
 };
 
+// Diagonal Pauli sum applied inside a tile pass: each element x of a tile is
+// multiplied by h(x) = sum_t c_t (-1)^{|x & z_t|}; zt is the tile-local mask
+// and zo the mask of qubits outside the tile (PauliTerm fields).
+constexpr int kMaxDiagTerms = 256;
+struct PauliTerm;
+struct DiagSum {
+    const PauliTerm *terms;   // xt = xg = 0
+    const double *coefs;      // complex, interleaved
+    int32_t nterms;
+};
+
 // One fused pass over the compressed store.
 struct PassArgs {
     int32_t n, B, C, j;                 // qubits, block log2, chunk log2, tile qubits above C
@@ -141,6 +152,7 @@ struct PassArgs {
     ChunkPerm perm;                     // chunk c of the pass is stored as chunk perm(c)
     int32_t nouter;                     // outer selector qubits of the pass
     int8_t outer_q[kMaxOuterSel];       // their global qubit indices (bit nb + i of W)
+    DiagSum diag;                       // nterms > 0: multiply by a diagonal Pauli sum after the sweeps
 };
 
 // A pass that only permutes chunk headers: meta_out[perm(c)] = meta_in[c]
@@ -197,6 +209,11 @@ struct ExpectArgs {
     const PauliTerm *terms;
     int32_t nterms;
     double *out;
+    // optional bra store of the same geometry: S_t = sum_x conj(bra_{x ^ xflip})
+    // (-1)^{|x & z|} ket_x (transition amplitudes); NULL meta_bra: bra = ket
+    const ChunkMeta *meta_bra;
+    const uint32_t *arena_bra;
+    const uint8_t *mask_bra;
 };
 
 // Backward (adjoint) pass over two uncompressed states psi and lam: gates are

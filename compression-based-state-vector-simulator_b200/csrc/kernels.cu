@@ -418,6 +418,38 @@ size_t pass_smem_bytes(bool f64, int nb, int j) {
     return tile + stage + ((tables + 7) / 8) * 8 + offs;
 }
 
+// ------------------------------------------------------------ diagonal Pauli sum
+// tile[e] *= sum_t c_t (-1)^{|e & zt_t| + |base_amp & zo_t|}: the outer sign
+// of each term is folded into its coefficient once per tile (s_dc, 2 doubles
+// per term, written and read by the whole CTA between barriers).
+template <typename R>
+__device__ void tile_diag_sum(typename Cplx<R>::T *tile, int nb, int swm, const DiagSum &d, uint64_t base_amp,
+                              double *s_dc) {
+    using T = typename Cplx<R>::T;
+    for (int t = threadIdx.x; t < d.nterms; t += blockDim.x) {
+        const double sg = (__popcll(base_amp & d.terms[t].zo) & 1) ? -1.0 : 1.0;
+        s_dc[2 * t] = sg * d.coefs[2 * t];
+        s_dc[2 * t + 1] = sg * d.coefs[2 * t + 1];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < (1 << nb); e += blockDim.x) {
+        double hr = 0.0, hi = 0.0;
+        for (int t = 0; t < d.nterms; ++t) {
+            const double sg = (__popc((uint32_t)e & d.terms[t].zt) & 1) ? -1.0 : 1.0;
+            hr = fma(sg, s_dc[2 * t], hr);
+            hi = fma(sg, s_dc[2 * t + 1], hi);
+        }
+        T &v = tile[swz<R>(e, swm)];
+        const double vr = (double)v.x, vi = (double)v.y;
+        v.x = (R)(hr * vr - hi * vi);
+        v.y = (R)(hr * vi + hi * vr);
+    }
+    __syncthreads();
+}
+
+static_assert((kSweepThreads / 32) * kStageWords * 4 >= 2 * kMaxDiagTerms * sizeof(double),
+              "the pass kernel's decode staging holds the diagonal-sum coefficients");
+
 // ------------------------------------------------------------ pass kernel
 template <typename R, int RB>
 __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a) {
@@ -478,6 +510,9 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
         // ---- gates
         tile_sweeps<R, RB>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool),
                            outer_word(chunk_base << C, s_oq, a.nouter));
+        // the decode staging area is free here: it holds the tile's term coefficients
+        if (a.diag.nterms)
+            tile_diag_sum<R>(tile, nb, swm, a.diag, chunk_base << C, reinterpret_cast<double *>(stage_all));
 
         // ---- quantise (codes replace values in shared memory)
         for (int c = warp; c < nchunks; c += nwarps) {
@@ -910,26 +945,38 @@ __global__ void __launch_bounds__(kExpectThreads) expect_kernel(const ExpectArgs
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int blk_shift = a.B - C;
     const int swm = swizzle_mask<R>(C);
+    const bool two = a.meta_bra != nullptr;
     T *tile = reinterpret_cast<T *>(smem);
-    uint32_t *wstage = reinterpret_cast<uint32_t *>(smem + (sizeof(T) << nb)) + warp * kStageWords;
+    T *btile = two ? tile + ((size_t)1 << nb) : tile;  // bra tile (the ket tile itself without a bra store)
+    uint32_t *wstage = reinterpret_cast<uint32_t *>(smem + ((two ? 2 * sizeof(T) : sizeof(T)) << nb)) + warp * kStageWords;
     for (int i = threadIdx.x; i < 2 * a.nterms; i += blockDim.x) s_acc[i] = 0.0;
     if (threadIdx.x < kMaxTileQubits) s_tq[threadIdx.x] = a.tq[threadIdx.x];
     __syncthreads();
     const int size = 1 << nb;
     for (uint64_t tile_id = blockIdx.x; tile_id < a.n_tiles; tile_id += gridDim.x) {
         const uint64_t chunk_base = insert_zero_bits(tile_id, s_tq, j);
-        bool any = false;
-        for (int c = 0; c < nchunks; ++c) any |= a.mask[(chunk_base | deposit_bits((uint32_t)c, s_tq, j)) >> blk_shift] != 0;
-        if (!any) continue;  // uniform: every thread reads the same mask bytes
-        for (int c = warp; c < nchunks; c += nwarps) {
-            const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
-            R *comp = reinterpret_cast<R *>(tile) + (size_t)c * ncomp;
-            if (!a.mask[chunk >> blk_shift]) {
-                for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = R(0);
-                continue;
+        bool any = false, anyb = false;
+        for (int c = 0; c < nchunks; ++c) {
+            const uint64_t blk = (chunk_base | deposit_bits((uint32_t)c, s_tq, j)) >> blk_shift;
+            any |= a.mask[blk] != 0;
+            anyb |= two && a.mask_bra[blk] != 0;
+        }
+        if (!any || (two && !anyb)) continue;  // uniform: every thread reads the same mask bytes
+        for (int side = 0; side < (two ? 2 : 1); ++side) {
+            const ChunkMeta *meta = side ? a.meta_bra : a.meta;
+            const uint32_t *arena = side ? a.arena_bra : a.arena;
+            const uint8_t *mask = side ? a.mask_bra : a.mask;
+            T *dst = side ? btile : tile;
+            for (int c = warp; c < nchunks; c += nwarps) {
+                const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
+                R *comp = reinterpret_cast<R *>(dst) + (size_t)c * ncomp;
+                if (!mask[chunk >> blk_shift]) {
+                    for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = R(0);
+                    continue;
+                }
+                decode_chunk<R>(arena, meta[chunk], per_lane, a.codec, reinterpret_cast<R *>(dst), wstage, lane,
+                                TileSlot<R>{c << C, swm});
             }
-            decode_chunk<R>(a.arena, a.meta[chunk], per_lane, a.codec, reinterpret_cast<R *>(tile), wstage, lane,
-                            TileSlot<R>{c << C, swm});
         }
         __syncthreads();
         const uint64_t base_amp = chunk_base << C;
@@ -939,7 +986,7 @@ __global__ void __launch_bounds__(kExpectThreads) expect_kernel(const ExpectArgs
             double re = 0.0, im = 0.0;
             for (int x = threadIdx.x; x < size; x += blockDim.x) {
                 const T ax = tile[swz<R>(x, swm)];
-                const T by = tile[swz<R>(x ^ (int)pt.xt, swm)];
+                const T by = btile[swz<R>(x ^ (int)pt.xt, swm)];
                 // conj(by) * ax
                 double pr = (double)by.x * (double)ax.x + (double)by.y * (double)ax.y;
                 double pi = (double)by.x * (double)ax.y - (double)by.y * (double)ax.x;
@@ -1173,7 +1220,7 @@ static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
 }
 
 cudaError_t launch_pass(bool f64, const PassArgs &a, int, cudaStream_t s) {
-    if (a.rb != kRegBits || a.C + a.j < kRegBits) return cudaErrorInvalidValue;
+    if (a.rb != kRegBits || a.C + a.j < kRegBits || a.diag.nterms > kMaxDiagTerms) return cudaErrorInvalidValue;
     return f64 ? launch_pass_t<double, kRegBits>(a, s) : launch_pass_t<float, kRegBits>(a, s);
 }
 
@@ -1339,7 +1386,8 @@ template <typename R>
 static cudaError_t launch_expect_t(const ExpectArgs &a, cudaStream_t s) {
     if (a.nterms > kMaxTermsPerLaunch) return cudaErrorInvalidValue;
     const int nb = a.C + a.j;
-    const size_t smem = ((size_t)(2 * sizeof(R)) << nb) + (size_t)(kExpectThreads / 32) * kStageWords * 4;
+    const size_t tiles = a.meta_bra ? 2 : 1;
+    const size_t smem = tiles * ((size_t)(2 * sizeof(R)) << nb) + (size_t)(kExpectThreads / 32) * kStageWords * 4;
     cudaError_t e = cudaFuncSetAttribute(expect_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;

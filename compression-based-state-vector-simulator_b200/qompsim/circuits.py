@@ -157,6 +157,9 @@ WORKLOADS = {
                   eps_rel=1e-3, eps_abs=1e-7),
     "qft26": dict(builder=lambda: qft_basis(26, seed=0), n=26, block_size=20, inner_size=4, dtype="complex128",
                   eps_rel=1e-3, eps_abs=1e-7),
+    # the QFT workload in the complex64 pipeline (FP32 gate arithmetic, FP64 reductions)
+    "qft30c64": dict(builder=lambda: qft_basis(30, seed=0), n=30, block_size=20, inner_size=4, dtype="complex64",
+                     eps_rel=1e-3, eps_abs=1e-7),
     "brickwork32": dict(builder=lambda: brickwork(32, 20, seed=0), n=32, block_size=22, inner_size=4,
                         dtype="complex64", eps_rel=1e-3, eps_abs=1e-7),
     "hea24": dict(builder=lambda: hea(24, 8, seed=0), n=24, block_size=18, inner_size=4, dtype="complex64",

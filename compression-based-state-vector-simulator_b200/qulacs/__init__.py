@@ -520,6 +520,27 @@ class CompressedQuantumState:
         self._check(_n.lib().qs_get_stats(self._h, _n.ct.byref(st)))
         return {name: getattr(st, name) for name, _ in st._fields_}
 
+    def transition_pauli_sums(self, bra: "CompressedQuantumState", xs, zs) -> np.ndarray:
+        """sum_x conj(bra[x ^ x_t]) (-1)^{|x & z_t|} self[x] for every term
+        (qs_transition_pauli; no normalisation)."""
+        n = len(xs)
+        xa = np.ascontiguousarray(np.asarray(xs, dtype=np.uint64))
+        za = np.ascontiguousarray(np.asarray(zs, dtype=np.uint64))
+        out = np.zeros(2 * max(1, n), dtype=np.float64)
+        self._check(_n.lib().qs_transition_pauli(bra._h, self._h, xa.ctypes.data_as(_n.ct.POINTER(_n.ct.c_uint64)),
+                                                 za.ctypes.data_as(_n.ct.POINTER(_n.ct.c_uint64)), n,
+                                                 out.ctypes.data_as(_n.ct.POINTER(_n.ct.c_double))))
+        return out[0:2 * n:2] + 1j * out[1:2 * n:2]
+
+    def load_diagonal_pauli_sum(self, source: "CompressedQuantumState", zs, coefs) -> None:
+        """self := (sum_t coefs[t] Z^{zs[t]}) source (qs_apply_diagonal_pauli_sum)."""
+        za = np.ascontiguousarray(np.asarray(zs, dtype=np.uint64))
+        ca = np.ascontiguousarray(np.asarray(coefs, dtype=np.complex128))
+        self._check(_n.lib().qs_apply_diagonal_pauli_sum(self._h, source._h,
+                                                         za.ctypes.data_as(_n.ct.POINTER(_n.ct.c_uint64)),
+                                                         ca.view(np.float64).ctypes.data_as(_n.ct.POINTER(_n.ct.c_double)),
+                                                         len(za)))
+
     def checkpoint(self, slot: int = 0) -> None:
         """Copy the compressed store into device checkpoint `slot`."""
         self._check(_n.lib().qs_checkpoint(self._h, int(slot)))

@@ -104,6 +104,8 @@ SIGNATURES = [
     ("qs_get_vector", ct.c_int, [_P, ct.POINTER(_D), ct.c_int]),
     ("qs_norm_squared", ct.c_int, [_P, ct.POINTER(_D)]),
     ("qs_expectation_pauli", ct.c_int, [_P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
+    ("qs_transition_pauli", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
+    ("qs_apply_diagonal_pauli_sum", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_D), ct.c_size_t]),
     ("qs_dense_expectation_pauli", ct.c_int, [_P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
     ("qs_dense_copy", ct.c_int, [_P, _P]),
     ("qs_dense_apply_pauli_sum", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_U64), ct.POINTER(_D), ct.c_size_t]),

@@ -91,6 +91,122 @@ def energy_and_gradient(circuit, observable: Observable, dtype="complex128"):
     return float(energy), grads
 
 
+def _support(g):
+    return set(g.get_target_index_list()) | set(g.get_control_index_list())
+
+
+def _is_diagonal(g) -> bool:
+    m = np.asarray(g.get_matrix())
+    return not np.any(m - np.diag(np.diag(m)))
+
+
+def _commute(a, b) -> bool:
+    """Sufficient test: disjoint qubits, or both diagonal."""
+    return not (_support(a) & _support(b)) or (_is_diagonal(a) and _is_diagonal(b))
+
+
+def commuting_groups(circuit):
+    """Maximal runs of consecutive parametric gates that commute pairwise, as
+    (start, end) gate-index ranges, last group first."""
+    gates = circuit._gates
+    pset = set(getattr(circuit, "_param_pos", []))
+    out = []
+    i = len(gates) - 1
+    while i >= 0:
+        if i in pset:
+            grp = [i]
+            j = i - 1
+            while j >= 0 and j in pset and all(_commute(gates[j], gates[m]) for m in grp):
+                grp.append(j)
+                j -= 1
+            out.append((j + 1, i + 1))
+            i = j
+        else:
+            i -= 1
+    return out
+
+
+def compressed_energy_and_gradient(circuit, observable: Observable, block_size: int, inner_size: int = 4,
+                                   dtype="complex128", eps_rel: float = 1e-3, eps_abs: float = 1e-7,
+                                   checkpoints: bool = False, flags: Optional[int] = None):
+    """(E, dE/dtheta) with both states compressed, for a diagonal observable
+    (Z strings only) and circuits whose parametric gates come in groups that
+    commute (QAOA cost and mixer layers, layers of single-qubit rotations).
+
+    Forward: psi = U |0> on a CompressedQuantumState.  lambda = H psi by one
+    fused diagonal pass.  Backward, group by group from the end: at the group
+    boundary every gate k of the group has dE/dtheta_k = -Im <lambda|P_k|psi>
+    / <psi|psi> (the group's other gates commute with P_k, so the boundary
+    states serve all of them), evaluated by one transition-sum pass over the
+    two compressed stores; then the inverse gates back to the previous group
+    are applied to psi and lambda as compressed circuits.  With checkpoints,
+    psi is stored in device checkpoints at every group boundary during the
+    forward pass and restored in the backward pass instead of being
+    uncomputed, so its compression error does not accumulate twice."""
+    import qulacs
+    from . import CompressedQuantumState
+    n = circuit.get_qubit_count()
+    xs, zs, nys, coefs = observable.term_masks()
+    if any(xs):
+        raise ValueError("the compressed adjoint needs a diagonal observable (Z strings only)")
+    gates = list(circuit._gates)
+    param_pos = list(getattr(circuit, "_param_pos", []))
+    slot_of = {pos: i for i, pos in enumerate(param_pos)}
+    groups = commuting_groups(circuit)
+    if flags is None:
+        flags = _n.QS_FLAG_QUIET
+
+    def state():
+        return CompressedQuantumState(n, block_size, dtype=dtype, eps_rel=eps_rel, eps_abs=eps_abs, flags=flags)
+
+    def run(st, gate_list):
+        if not gate_list:
+            return
+        c = qulacs.QuantumCircuit(n)
+        for g in gate_list:
+            c.add_gate(g)
+        st.partition_and_register_circuit(c, inner_size, 0)
+        st.apply_circuit()
+
+    psi = state()
+    if checkpoints:
+        bounds = sorted(e for _, e in groups)
+        pos = 0
+        for k, e in enumerate(bounds):
+            run(psi, gates[pos:e])
+            psi.checkpoint(k)
+            pos = e
+        run(psi, gates[pos:])
+        slot_at = {e: k for k, e in enumerate(bounds)}
+    else:
+        run(psi, gates)
+    sums = psi._pauli_sums(list(xs) + [0], list(zs) + [0])
+    norm2 = sums[-1].real
+    energy_value = float(np.real(sum(c * (1j ** ny) * v for c, ny, v in zip(coefs, nys, sums[:-1])) / norm2))
+    lam = state()
+    lam.load_diagonal_pauli_sum(psi, zs, [c * (1j ** ny) for c, ny in zip(coefs, nys)])
+    grads = np.zeros(len(param_pos))
+    pos = len(gates)
+    for start, end in groups:
+        back = [g.get_inverse() for g in reversed(gates[end:pos])]
+        run(lam, back)
+        if checkpoints:
+            psi.restore(slot_at[end])
+        else:
+            run(psi, back)
+        idx = list(range(start, end))
+        masks = [gates[i].generator_masks() for i in idx]
+        # <lambda| P |psi>: bra lambda, ket psi
+        s = psi.transition_pauli_sums(lam, [m[0] for m in masks], [m[1] for m in masks])
+        for i, (xm, zm, ny), v in zip(idx, masks, s):
+            grads[slot_of[i]] = -np.imag((1j ** ny) * v) / norm2
+        pos = end
+    if checkpoints:
+        for k in range(len(groups)):
+            psi.free_checkpoint(k)
+    return energy_value, grads
+
+
 def energy(circuit, observable: Observable, dtype="complex128") -> float:
     psi = QuantumState(circuit.get_qubit_count(), dtype=dtype)
     circuit.update_quantum_state(psi)

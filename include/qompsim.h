@@ -204,6 +204,26 @@ qs_status qs_norm_squared(qs_state *h, double *out);
 qs_status qs_expectation_pauli(qs_state *h, const uint64_t *x_masks, const uint64_t *z_masks, size_t nterms,
                                double *out);
 
+/* Transition sums between two compressed states of the same geometry (qubits,
+ * block, chunk, dtype, error bounds): out[2t] + i out[2t+1] =
+ * sum_x conj(bra[x ^ x_t]) (-1)^{popcount(x & z_t)} ket[x], FP64
+ * accumulation, no normalisation.  The adjoint sweep's <lambda|P|psi> on
+ * compressed states; the reference has no counterpart (its gradients run on
+ * uncompressed states, src/vqcsim/parametric_circuit.cpp:180-306). */
+qs_status qs_transition_pauli(const qs_state *bra, qs_state *ket, const uint64_t *x_masks,
+                              const uint64_t *z_masks, size_t nterms, double *out);
+
+/* out := (sum_t c_t Z^{z_masks[t]}) in for a diagonal observable (Z strings
+ * only; coefs complex interleaved, at most 256 terms): one fused pass that
+ * decodes in's store, multiplies every amplitude by h(x) = sum_t c_t
+ * (-1)^{popcount(x & z_t)} and encodes into out's store (previous contents
+ * of out are replaced; out keeps in's zero-block mask).  in and out are
+ * distinct states of the same geometry.  This is Observable::apply_to_state
+ * (src/cppsim/observable.cpp) restricted to diagonal terms, on compressed
+ * states, for the adjoint sweep's lambda = H psi. */
+qs_status qs_apply_diagonal_pauli_sum(qs_state *out, const qs_state *in, const uint64_t *z_masks,
+                                      const double *coefs, size_t nterms);
+
 /* Zero-block mask: out[b] = 1 when block b is stored (the reference's
  * block_pointers[b] != nullptr, compressed_state.hpp:18-19, 319-325). */
 qs_status qs_get_zero_mask(qs_state *h, uint8_t *out);

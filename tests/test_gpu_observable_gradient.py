@@ -158,3 +158,88 @@ def test_adjoint_gradient_qaoa_torch(qulacs_mod):
         fd[j] = (energy(builder(xp)[0], obs) - energy(builder(xm)[0], obs)) / (2 * h)
     assert np.max(np.abs(params.grad.numpy() - fd)) < 1e-6
     assert abs(float(e.detach()) - energy(builder(x0)[0], obs)) < 1e-12
+
+
+# ------------------------------------------------------------------ compressed adjoint
+def _qaoa_param(qulacs, n, p, seed):
+    from qompsim import circuits as C
+    edges = C.regular_graph_edges(n, 3, seed=seed)
+    gam, bet = C.qaoa_params(p, seed=seed)
+    c = qulacs.ParametricQuantumCircuit(n)
+    for q in range(n):
+        c.add_H_gate(q)
+    for layer in range(p):
+        for a, b in edges:
+            c.add_parametric_multi_Pauli_rotation_gate([a, b], [3, 3], gam[layer])
+        for q in range(n):
+            c.add_parametric_RX_gate(q, bet[layer])
+    obs = qulacs.Observable(n)
+    for a, b in edges:
+        obs.add_operator(0.5, f"Z {a} Z {b}")
+    return c, obs
+
+
+def test_compressed_transition_and_diagonal_sum(qulacs_mod):
+    """qs_transition_pauli and qs_apply_diagonal_pauli_sum against numpy on
+    the states' own decoded vectors."""
+    from qulacs import _native
+    n, B = 11, 6
+    c1 = helpers.optimized(helpers.random_circuit(n, 60, seed=5), B)
+    c2 = helpers.optimized(helpers.random_circuit(n, 60, seed=6), B)
+    kw = dict(eps_rel=2.0 ** -20, eps_abs=1e-12, flags=_native.QS_FLAG_QUIET)
+    a = qulacs_mod.CompressedQuantumState(n, B, **kw)
+    a.partition_and_register_circuit(c1, 2, 0)
+    a.apply_circuit()
+    b = qulacs_mod.CompressedQuantumState(n, B, **kw)
+    b.partition_and_register_circuit(c2, 2, 0)
+    b.apply_circuit()
+    va, vb = a.get_vector(renormalize=False), b.get_vector(renormalize=False)
+    xs = [0, 1 << 3, (1 << 9) | 1, 0, (1 << 10) | (1 << 7)]
+    zs = [0, 0, 1 << 2, (1 << 8) | (1 << 1), 1 << 10]
+    got = a.transition_pauli_sums(b, xs, zs)   # <b| P |a>
+    x = np.arange(1 << n)
+    for t, (xm, zm) in enumerate(zip(xs, zs)):
+        sign = np.where(np.vectorize(lambda v: bin(v).count("1") & 1)(x & zm), -1.0, 1.0)
+        want = np.sum(np.conj(vb[x ^ xm]) * sign * va)
+        assert abs(got[t] - want) < 1e-10, t
+    # lambda = (0.5 Z1 Z4 - 1.2 Z10 + 0.3) psi
+    zsd = [(1 << 1) | (1 << 4), 1 << 10, 0]
+    cd = [0.5, -1.2, 0.3]
+    lam = qulacs_mod.CompressedQuantumState(n, B, **kw)
+    lam.load_diagonal_pauli_sum(a, zsd, cd)
+    h = np.zeros(1 << n)
+    for zm, cf in zip(zsd, cd):
+        h += cf * np.where(np.vectorize(lambda v: bin(v).count("1") & 1)(x & zm), -1.0, 1.0)
+    assert np.abs(lam.get_vector(renormalize=False) - h * va).max() < 1e-5
+    assert np.array_equal(lam.get_zero_mask(), a.get_zero_mask())
+
+
+@pytest.mark.parametrize("dtype,checkpoints", [("complex128", False), ("complex128", True), ("complex64", True)])
+def test_compressed_adjoint_qaoa(qulacs_mod, dtype, checkpoints):
+    """Compressed adjoint gradient of QAOA (layer groups, diagonal H) against
+    the dense adjoint and FP64 central differences."""
+    from qulacs.torch import compressed_energy_and_gradient, energy_and_gradient
+    n, p = 10, 2
+    circ, obs = _qaoa_param(qulacs_mod, n, p, seed=2)
+    tight = dtype == "complex128"
+    e, g = compressed_energy_and_gradient(circ, obs, block_size=5, inner_size=2, dtype=dtype,
+                                          eps_rel=2.0 ** -20 if tight else 2.0 ** -16,
+                                          eps_abs=1e-12 if tight else 1e-8, checkpoints=checkpoints)
+    e_ref, g_ref = energy_and_gradient(circ, obs, "complex128")
+    tol = 1e-5 if tight else 2e-3
+    assert abs(e - e_ref) < tol
+    assert np.max(np.abs(g - g_ref)) < tol
+    fd = _fd(circ, obs, "complex128")
+    assert np.max(np.abs(g - fd)) < tol + 1e-6
+
+
+def test_compressed_adjoint_default_bounds(qulacs_mod):
+    """At the reference's default error bounds (1e-3 / 1e-7) the compressed
+    adjoint stays close to the exact gradient."""
+    from qulacs.torch import compressed_energy_and_gradient, energy_and_gradient
+    circ, obs = _qaoa_param(qulacs_mod, 12, 2, seed=3)
+    e, g = compressed_energy_and_gradient(circ, obs, block_size=6, inner_size=3, dtype="complex64", checkpoints=True)
+    e_ref, g_ref = energy_and_gradient(circ, obs, "complex128")
+    scale = max(1.0, np.max(np.abs(g_ref)))
+    assert abs(e - e_ref) < 2e-2
+    assert np.max(np.abs(g - g_ref)) / scale < 5e-2
