@@ -1470,7 +1470,17 @@ qs_status qs_norm_squared(qs_state *h, double *out) {
 }
 
 qs_status qs_get_vector(qs_state *h, double *out, int renormalize) {
-    if (!h || !out) return fail(h, QS_ERR_ARG, "NULL argument");
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    return qs_get_amplitudes(h, 0, uint64_t(1) << h->n, out, renormalize);
+}
+
+qs_status qs_get_amplitudes(qs_state *h, uint64_t first, uint64_t count, double *out, int renormalize) {
+    if (!h || (count && !out)) return fail(h, QS_ERR_ARG, "NULL argument");
+    const uint64_t chunk_amps = uint64_t(1) << h->C;
+    const uint64_t dim = uint64_t(1) << h->n;
+    if (first > dim || count > dim - first) return fail(h, QS_ERR_ARG, "amplitude range outside the state");
+    if ((first | count) & (chunk_amps - 1))
+        return fail(h, QS_ERR_ARG, "first and count must be multiples of 2^chunk_log2 (qs_get_stats)");
     double scale = 1.0;
     if (renormalize) {
         double nrm = 0;
@@ -1478,21 +1488,23 @@ qs_status qs_get_vector(qs_state *h, double *out, int renormalize) {
         if (s != QS_OK) return s;
         if (nrm > 0) scale = 1.0 / std::sqrt(nrm);
     }
-    const uint64_t chunk_amps = uint64_t(1) << h->C;
+    const uint64_t cfirst = first / chunk_amps, ccount = count / chunk_amps;
+    if (!ccount) return QS_OK;
     const uint64_t slab_chunks = std::max<uint64_t>(1, (uint64_t(1) << 24) / chunk_amps);
     double *dbuf = nullptr;
-    const uint64_t nslab = std::min<uint64_t>(slab_chunks, h->nchunks);
+    const uint64_t nslab = std::min<uint64_t>(slab_chunks, ccount);
     CUDA_TRY(h, cudaMalloc(&dbuf, nslab * chunk_amps * 2 * sizeof(double)));
     qs_status rs = QS_OK;
-    for (uint64_t c0 = 0; c0 < h->nchunks; c0 += nslab) {
-        const uint64_t cnt = std::min<uint64_t>(nslab, h->nchunks - c0);
+    for (uint64_t c0 = 0; c0 < ccount; c0 += nslab) {
+        const uint64_t cnt = std::min<uint64_t>(nslab, ccount - c0);
         cudaError_t e = qs::launch_readout(h->f64, h->meta[h->mcur], h->arena[h->cur], h->mask, (int)h->B, (int)h->C,
-                                           h->codec, c0, cnt, dbuf, scale, h->stream);
+                                           h->codec, cfirst + c0, cnt, dbuf, scale, h->stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(out + c0 * chunk_amps * 2, dbuf, cnt * chunk_amps * 2 * sizeof(double),
                                 cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) {
+            (void)cudaGetLastError();
             h->err = std::string("readout: ") + cudaGetErrorString(e);
             rs = QS_ERR_CUDA;
             break;
@@ -2224,6 +2236,30 @@ qs_status qs_dense_apply_gates_pergate(qs_dense *h, const qs_gate *gates, size_t
     s = dense_upload_gates(h, kg);
     if (s != QS_OK) return s;
     for (size_t i = 0; i < kg.size(); ++i) CUDA_TRY(h, qs::launch_pergate(h->f64, h->state, (int)h->n, h->kg + i, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return QS_OK;
+}
+
+qs_status qs_dense_get_amplitudes(qs_dense *h, uint64_t first, uint64_t count, double *out) {
+    if (!h || (count && !out)) return dfail(h, QS_ERR_ARG, "NULL argument");
+    if (first > h->dim() || count > h->dim() - first) return dfail(h, QS_ERR_ARG, "amplitude range outside the state");
+    if (!count) return QS_OK;
+    if (h->f64) {
+        CUDA_TRY(h, cudaMemcpyAsync(out, static_cast<const double *>(h->state) + 2 * first, count * 16,
+                                    cudaMemcpyDeviceToHost, h->stream));
+    } else {
+        double *tmp = nullptr;
+        CUDA_TRY(h, cudaMalloc(&tmp, count * 16));
+        cudaError_t e = qs::launch_dense_to_c128(false, static_cast<const float *>(h->state) + 2 * first, count, tmp,
+                                                 h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, count * 16, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        cudaFree(tmp);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            return dfail(h, QS_ERR_CUDA, std::string("get_amplitudes: ") + cudaGetErrorString(e));
+        }
+    }
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return QS_OK;
 }

@@ -307,6 +307,13 @@ class QuantumState:
         self._check(_n.lib().qs_dense_get_vector(self._h, out.view(np.float64).ctypes.data_as(_n.ct.POINTER(_n.ct.c_double))))
         return out
 
+    def get_amplitudes(self, first: int, count: int) -> np.ndarray:
+        """Amplitudes [first, first + count) as complex128."""
+        out = np.empty(int(count), dtype=np.complex128)
+        self._check(_n.lib().qs_dense_get_amplitudes(self._h, int(first), int(count),
+                                                     out.view(np.float64).ctypes.data_as(_n.ct.POINTER(_n.ct.c_double))))
+        return out
+
     def get_squared_norm(self) -> float:
         v = _n.ct.c_double()
         self._check(_n.lib().qs_dense_norm_squared(self._h, _n.ct.byref(v)))
@@ -465,6 +472,15 @@ class CompressedQuantumState:
         out = np.empty(1 << self._n, dtype=np.complex128)
         self._check(_n.lib().qs_get_vector(self._h, out.view(np.float64).ctypes.data_as(_n.ct.POINTER(_n.ct.c_double)),
                                            1 if renormalize else 0))
+        return out
+
+    def get_amplitudes(self, first: int, count: int, renormalize: bool = True) -> np.ndarray:
+        """Amplitudes [first, first + count) of get_vector (first and count
+        multiples of the chunk size, get_stats()['chunk_log2'])."""
+        out = np.empty(int(count), dtype=np.complex128)
+        self._check(_n.lib().qs_get_amplitudes(self._h, int(first), int(count),
+                                               out.view(np.float64).ctypes.data_as(_n.ct.POINTER(_n.ct.c_double)),
+                                               1 if renormalize else 0))
         return out
 
     def get_squared_norm(self) -> float:

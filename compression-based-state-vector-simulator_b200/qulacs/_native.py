@@ -102,6 +102,7 @@ SIGNATURES = [
                                 ct.POINTER(_U32), ct.POINTER(_U32)]),
     ("qs_apply_circuit", ct.c_int, [_P]),
     ("qs_get_vector", ct.c_int, [_P, ct.POINTER(_D), ct.c_int]),
+    ("qs_get_amplitudes", ct.c_int, [_P, _U64, _U64, ct.POINTER(_D), ct.c_int]),
     ("qs_norm_squared", ct.c_int, [_P, ct.POINTER(_D)]),
     ("qs_expectation_pauli", ct.c_int, [_P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
     ("qs_transition_pauli", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
@@ -132,6 +133,7 @@ SIGNATURES = [
     ("qs_dense_apply_gates", ct.c_int, [_P, ct.POINTER(qs_gate), ct.c_size_t]),
     ("qs_dense_apply_gates_pergate", ct.c_int, [_P, ct.POINTER(qs_gate), ct.c_size_t]),
     ("qs_dense_get_vector", ct.c_int, [_P, ct.POINTER(_D)]),
+    ("qs_dense_get_amplitudes", ct.c_int, [_P, _U64, _U64, ct.POINTER(_D)]),
     ("qs_dense_set_vector", ct.c_int, [_P, ct.POINTER(_D)]),
     ("qs_dense_set_basis_state", ct.c_int, [_P, _U64]),
     ("qs_dense_norm_squared", ct.c_int, [_P, ct.POINTER(_D)]),

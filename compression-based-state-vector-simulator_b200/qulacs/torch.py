@@ -128,7 +128,8 @@ def commuting_groups(circuit):
 
 def compressed_energy_and_gradient(circuit, observable: Observable, block_size: int, inner_size: int = 4,
                                    dtype="complex128", eps_rel: float = 1e-3, eps_abs: float = 1e-7,
-                                   checkpoints: bool = False, flags: Optional[int] = None):
+                                   checkpoints: bool = False, flags: Optional[int] = None,
+                                   timings: Optional[dict] = None):
     """(E, dE/dtheta) with both states compressed, for a diagonal observable
     (Z strings only) and circuits whose parametric gates come in groups that
     commute (QAOA cost and mixer layers, layers of single-qubit rotations).
@@ -142,7 +143,11 @@ def compressed_energy_and_gradient(circuit, observable: Observable, block_size: 
     are applied to psi and lambda as compressed circuits.  With checkpoints,
     psi is stored in device checkpoints at every group boundary during the
     forward pass and restored in the backward pass instead of being
-    uncomputed, so its compression error does not accumulate twice."""
+    uncomputed, so its compression error does not accumulate twice.
+
+    timings, when given, receives the wall time (s) of each phase: forward,
+    lambda, undo (inverse gates on both states), transition (gradient sums)."""
+    import time as _time
     import qulacs
     from . import CompressedQuantumState
     n = circuit.get_qubit_count()
@@ -159,6 +164,10 @@ def compressed_energy_and_gradient(circuit, observable: Observable, block_size: 
     def state():
         return CompressedQuantumState(n, block_size, dtype=dtype, eps_rel=eps_rel, eps_abs=eps_abs, flags=flags)
 
+    tm = timings if timings is not None else {}
+    for k in ("forward", "lambda", "undo", "transition"):
+        tm.setdefault(k, 0.0)
+
     def run(st, gate_list):
         if not gate_list:
             return
@@ -167,6 +176,13 @@ def compressed_energy_and_gradient(circuit, observable: Observable, block_size: 
             c.add_gate(g)
         st.partition_and_register_circuit(c, inner_size, 0)
         st.apply_circuit()
+
+    clock = [_time.perf_counter()]
+
+    def lap(key):
+        now = _time.perf_counter()
+        tm[key] += now - clock[0]
+        clock[0] = now
 
     psi = state()
     if checkpoints:
@@ -183,8 +199,10 @@ def compressed_energy_and_gradient(circuit, observable: Observable, block_size: 
     sums = psi._pauli_sums(list(xs) + [0], list(zs) + [0])
     norm2 = sums[-1].real
     energy_value = float(np.real(sum(c * (1j ** ny) * v for c, ny, v in zip(coefs, nys, sums[:-1])) / norm2))
+    lap("forward")
     lam = state()
     lam.load_diagonal_pauli_sum(psi, zs, [c * (1j ** ny) for c, ny in zip(coefs, nys)])
+    lap("lambda")
     grads = np.zeros(len(param_pos))
     pos = len(gates)
     for start, end in groups:
@@ -194,12 +212,14 @@ def compressed_energy_and_gradient(circuit, observable: Observable, block_size: 
             psi.restore(slot_at[end])
         else:
             run(psi, back)
+        lap("undo")
         idx = list(range(start, end))
         masks = [gates[i].generator_masks() for i in idx]
         # <lambda| P |psi>: bra lambda, ket psi
         s = psi.transition_pauli_sums(lam, [m[0] for m in masks], [m[1] for m in masks])
         for i, (xm, zm, ny), v in zip(idx, masks, s):
             grads[slot_of[i]] = -np.imag((1j ** ny) * v) / norm2
+        lap("transition")
         pos = end
     if checkpoints:
         for k in range(len(groups)):
@@ -256,5 +276,31 @@ try:
 
     def circuit_energy(params, builder, observable, dtype="complex128"):
         return CircuitEnergyFunction.apply(params, builder, observable, dtype)
+
+    class CompressedCircuitFunction(_torch.autograd.Function):
+        """E(params) on the compressed state, with the compressed adjoint
+        gradient (compressed_energy_and_gradient; diagonal observables, commuting
+        parametric layers).  builder as for CircuitEnergyFunction; options are
+        the keyword arguments of compressed_energy_and_gradient (block_size,
+        inner_size, dtype, eps_rel, eps_abs, checkpoints)."""
+
+        @staticmethod
+        def forward(ctx, params, builder: Callable, observable: Observable, options: dict):
+            p = params.detach().cpu().numpy().astype(np.float64)
+            built = builder(p)
+            circuit, jac = (built if isinstance(built, tuple) else (built, None))
+            e, g = compressed_energy_and_gradient(circuit, observable, **options)
+            if jac is not None:
+                g = np.asarray(jac, dtype=np.float64).T @ g
+            ctx.save_for_backward(_torch.as_tensor(g, dtype=_torch.float64))
+            return _torch.tensor(e, dtype=_torch.float64)
+
+        @staticmethod
+        def backward(ctx, grad_out):
+            (g,) = ctx.saved_tensors
+            return grad_out * g.to(grad_out.device), None, None, None
+
+    def compressed_circuit_energy(params, builder, observable, **options):
+        return CompressedCircuitFunction.apply(params, builder, observable, options)
 except ImportError:  # torch is optional for the rest of the package
     pass

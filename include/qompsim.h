@@ -188,6 +188,12 @@ qs_status qs_apply_circuit(qs_state *h);
  * renormalize != 0 divides by the norm as the reference does. */
 qs_status qs_get_vector(qs_state *h, double *out, int renormalize);
 
+/* Amplitudes [first, first + count) of the same dense vector (2*count
+ * doubles); first and count are multiples of the chunk size 2^chunk_log2.
+ * Lets a caller stream a state larger than host memory allows at once
+ * (fidelity in slices); the reference reads only whole vectors. */
+qs_status qs_get_amplitudes(qs_state *h, uint64_t first, uint64_t count, double *out, int renormalize);
+
 /* Squared norm of the compressed state, accumulated in FP64. */
 qs_status qs_norm_squared(qs_state *h, double *out);
 
@@ -289,6 +295,8 @@ qs_status qs_dense_apply_gates_pergate(qs_dense *h, const qs_gate *gates, size_t
 
 /* QuantumState::get_vector / load (state.hpp:445-1045); 2*2^n doubles. */
 qs_status qs_dense_get_vector(qs_dense *h, double *out);
+/* Amplitudes [first, first + count) as complex128 (2*count doubles). */
+qs_status qs_dense_get_amplitudes(qs_dense *h, uint64_t first, uint64_t count, double *out);
 qs_status qs_dense_set_vector(qs_dense *h, const double *in);
 qs_status qs_dense_set_basis_state(qs_dense *h, uint64_t basis);
 qs_status qs_dense_norm_squared(qs_dense *h, double *out);

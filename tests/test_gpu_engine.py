@@ -402,3 +402,23 @@ def test_run_sim_one_rank_fidelity(qulacs_mod, capfd):
     fid = float(out.split("Fidelity:")[1].split()[0])
     assert fid > 0.999
     assert "Circuit Stages: [" in out
+
+
+def test_amplitude_slices_match_full_vectors(qulacs_mod):
+    from qulacs import _native
+    n, B = 12, 7
+    c = helpers.optimized(helpers.random_circuit(n, 50, seed=31), B)
+    cq = _compressed(qulacs_mod, c, B, 3)
+    full = cq.get_vector()
+    ch = 1 << cq.get_stats()["chunk_log2"]
+    for first, cnt in [(0, ch), (ch * 3, ch * 5), ((1 << n) - ch, ch)]:
+        assert np.array_equal(cq.get_amplitudes(first, cnt), full[first:first + cnt])
+    with pytest.raises(_native.QompsimError):
+        cq.get_amplitudes(1, ch)
+    ds = qulacs_mod.QuantumState(n, dtype="complex128")
+    c.update_quantum_state(ds)
+    dv = ds.get_vector()
+    assert np.array_equal(ds.get_amplitudes(100, 57), dv[100:157])
+    d64 = qulacs_mod.QuantumState(n, dtype="complex64")
+    c.update_quantum_state(d64)
+    assert np.array_equal(d64.get_amplitudes(64, 128), d64.get_vector()[64:192])

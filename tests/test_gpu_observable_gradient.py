@@ -243,3 +243,49 @@ def test_compressed_adjoint_default_bounds(qulacs_mod):
     scale = max(1.0, np.max(np.abs(g_ref)))
     assert abs(e - e_ref) < 2e-2
     assert np.max(np.abs(g - g_ref)) / scale < 5e-2
+
+
+def test_compressed_circuit_function_torch(qulacs_mod):
+    """torch.autograd through the compressed adjoint, QAOA with parameters
+    shared across each layer (jacobian mapping), against FP64 differences."""
+    import torch
+    from qompsim import circuits as C
+    from qulacs.torch import compressed_circuit_energy, energy
+    n, p = 10, 2
+    edges = C.regular_graph_edges(n, 3, seed=4)
+
+    def builder(params):
+        gam, bet = params[:p], params[p:]
+        c = qulacs_mod.ParametricQuantumCircuit(n)
+        for q in range(n):
+            c.add_H_gate(q)
+        rows = []
+        for layer in range(p):
+            for a, b in edges:
+                c.add_parametric_multi_Pauli_rotation_gate([a, b], [3, 3], gam[layer])
+                rows.append(layer)
+            for q in range(n):
+                c.add_parametric_RX_gate(q, bet[layer])
+                rows.append(p + layer)
+        jac = np.zeros((len(rows), 2 * p))
+        for i, col in enumerate(rows):
+            jac[i, col] = 1.0
+        return c, jac
+
+    obs = qulacs_mod.Observable(n)
+    for a, b in edges:
+        obs.add_operator(0.5, f"Z {a} Z {b}")
+    x0 = np.concatenate(C.qaoa_params(p, seed=5))
+    params = torch.tensor(x0, dtype=torch.float64, requires_grad=True)
+    e = compressed_circuit_energy(params, builder, obs, block_size=5, inner_size=2, eps_rel=2.0 ** -20,
+                                  eps_abs=1e-12, checkpoints=True)
+    e.backward()
+    h = 1e-4
+    fd = np.zeros_like(x0)
+    for j in range(x0.size):
+        xp, xm = x0.copy(), x0.copy()
+        xp[j] += h
+        xm[j] -= h
+        fd[j] = (energy(builder(xp)[0], obs) - energy(builder(xm)[0], obs)) / (2 * h)
+    assert np.max(np.abs(params.grad.numpy() - fd)) < 1e-5
+    assert abs(float(e.detach()) - energy(builder(x0)[0], obs)) < 1e-5
