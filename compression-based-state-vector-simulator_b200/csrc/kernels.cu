@@ -249,9 +249,27 @@ __device__ __forceinline__ uint32_t outer_word(uint64_t base_amp, const int8_t *
 }
 
 // Apply every sweep of a pass to a tile of 2^nb elements.  ow is the tile's
-// outer selector word.
+// outer selector word.  For complex64 they are a separate (not inlined)
+// function: it gets its own register allocation, apart from the codec phases
+// of the pass kernel, which measured faster; complex128 keeps them inlined.
 template <typename R, int RB>
-__device__ void tile_sweeps(typename Cplx<R>::T *tile, int nb, int swm, const Sweep *__restrict__ sweeps,
+__device__ __forceinline__ void tile_sweeps_body(typename Cplx<R>::T *tile, int nb, int swm,
+                                                 const Sweep *__restrict__ sweeps, int nsweeps,
+                                                 const ROp *__restrict__ ops,
+                                                 const typename Cplx<R>::T *__restrict__ pool, uint32_t ow);
+template <typename R, int RB>
+__device__ __noinline__ void tile_sweeps_call(typename Cplx<R>::T *tile, int nb, int swm, const Sweep *__restrict__ sweeps,
+                            int nsweeps, const ROp *__restrict__ ops, const typename Cplx<R>::T *__restrict__ pool,
+                            uint32_t ow) { tile_sweeps_body<R, RB>(tile, nb, swm, sweeps, nsweeps, ops, pool, ow); }
+template <typename R, int RB>
+__device__ __forceinline__ void tile_sweeps(typename Cplx<R>::T *tile, int nb, int swm, const Sweep *__restrict__ sweeps,
+                            int nsweeps, const ROp *__restrict__ ops, const typename Cplx<R>::T *__restrict__ pool,
+                            uint32_t ow) {
+    if constexpr (sizeof(R) == 4) tile_sweeps_call<R, RB>(tile, nb, swm, sweeps, nsweeps, ops, pool, ow);
+    else tile_sweeps_body<R, RB>(tile, nb, swm, sweeps, nsweeps, ops, pool, ow);
+}
+template <typename R, int RB>
+__device__ __forceinline__ void tile_sweeps_body(typename Cplx<R>::T *tile, int nb, int swm, const Sweep *__restrict__ sweeps,
                             int nsweeps, const ROp *__restrict__ ops, const typename Cplx<R>::T *__restrict__ pool,
                             uint32_t ow) {
     using T = typename Cplx<R>::T;
@@ -325,15 +343,20 @@ __device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena,
         for (int i = 0; i < per_lane; ++i) comp[slot(lane + 32 * i)] = v;
         return;
     }
-    const uint32_t rows = (uint32_t)(((uint32_t)per_lane * w + 31) >> 5);
+    const int rows = (int)(((uint32_t)per_lane * w + 31) >> 5);
     const uint32_t *src = arena + (md.offset >> 2);
-    uint32_t tmp[kMaxPerLane];
+    // payload rows into the warp's staging, half of them at a time through registers
+    constexpr int H = kMaxPerLane / 2;
 #pragma unroll
-    for (int r = 0; r < kMaxPerLane; ++r)
-        if (r < (int)rows) tmp[r] = __ldcs(src + r * 32 + lane);
+    for (int h = 0; h < 2; ++h) {
+        uint32_t tmp[H];
 #pragma unroll
-    for (int r = 0; r < kMaxPerLane; ++r)
-        if (r < (int)rows) wstage[r * 32 + lane] = tmp[r];
+        for (int r = 0; r < H; ++r)
+            if (h * H + r < rows) tmp[r] = __ldcs(src + (h * H + r) * 32 + lane);
+#pragma unroll
+        for (int r = 0; r < H; ++r)
+            if (h * H + r < rows) wstage[(h * H + r) * 32 + lane] = tmp[r];
+    }
     // element i of this lane's stream starts at bit i*w: every element is
     // extracted independently (one funnel shift); a lane reads only its own words
     const uint32_t mask = (w >= 32) ? 0xffffffffu : ((1u << w) - 1u);
@@ -348,29 +371,37 @@ __device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena,
 }
 
 // Per-warp quantisation of one chunk held in comp[]: codes overwrite the
-// chunk's own shared memory as int32 (all values are read first).  Returns
+// chunk's own shared memory as int32.  Returns
 // base/width/non-zero flag (valid in every lane).
 template <typename R, typename Slot = LinearSlot>
 __device__ __forceinline__ void quantize_chunk(R *comp, int per_lane, CodecParams p, bool exact_zero,
                                                int lane, int32_t *base_out, uint32_t *width_out,
                                                bool *nz_out, Slot slot = Slot(), int32_t *codes = nullptr) {
-    R v[kMaxPerLane];
-#pragma unroll
-    for (int i = 0; i < kMaxPerLane; ++i)
-        if (i < per_lane) v[i] = comp[slot(lane + 32 * i)];
-    __syncwarp();
     if (codes == nullptr) codes = reinterpret_cast<int32_t *>(comp);
     int32_t lo = INT_MAX, hi = INT_MIN;
     bool nz = false;
+    // four quarters, to cut the live values: the code of component c is 4
+    // bytes at offset 4c of the chunk's region and its value lies at or after
+    // that offset, so the codes of a quarter overwrite only values already read
+    constexpr int H = kMaxPerLane / 4;
 #pragma unroll
-    for (int i = 0; i < kMaxPerLane; ++i) {
-        if (i < per_lane) {
-            const int32_t q = quantize_hot(v[i], p);
-            codes[lane + 32 * i] = q;
-            lo = min(lo, q);
-            hi = max(hi, q);
-            nz |= exact_zero ? (v[i] != R(0)) : (q != 0);
+    for (int h = 0; h < 4; ++h) {
+        R v[H];
+#pragma unroll
+        for (int i = 0; i < H; ++i)
+            if (h * H + i < per_lane) v[i] = comp[slot(lane + 32 * (h * H + i))];
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+            if (h * H + i < per_lane) {
+                const int32_t q = quantize_hot(v[i], p);
+                codes[lane + 32 * (h * H + i)] = q;
+                lo = min(lo, q);
+                hi = max(hi, q);
+                nz |= exact_zero ? (v[i] != R(0)) : (q != 0);
+            }
         }
+        __syncwarp();
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
