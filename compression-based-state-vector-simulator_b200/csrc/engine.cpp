@@ -351,7 +351,7 @@ struct RawOp {
     uint8_t kind = RK_SCALAR;
     uint8_t k0 = 0, k1 = 0;
     uint8_t nsel = 0;
-    uint8_t sel[qs::kMaxSel] = {0, 0, 0, 0};
+    uint8_t sel[qs::kMaxSel] = {};
     uint32_t mat = 0, vstride = 0;
 };
 

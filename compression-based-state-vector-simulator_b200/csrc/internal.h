@@ -64,7 +64,7 @@ constexpr int kSweepThreads = 128;
 
 // One register op (host-built, 16 bytes).  `code` names the action and the
 // register bits it acts on; the gate's other qubits are fixed for a register
-// group and select one of 2^nsel pre-computed variants: sel[j] is a bit
+// group and select one of 2^nsel (nsel <= 8) pre-computed variants: sel[j] is a bit
 // position in the group word W = (tile index of the group's element 0) |
 // (outer selector bits << tile bits), unused slots hold 31 (always 0 in W).
 //   OPC_SCALAR           z *= m[0]                (lazy: one factor per group)
@@ -80,15 +80,15 @@ enum : uint8_t {
     OPC_SCALAR = 0, OPC_D2 = 8, OPC_D2H = 16, OPC_M2 = 24, OPC_X = 32,
     OPC_D4 = 64, OPC_D4H = 96, OPC_M4 = 128, OPC_SWAP = 160
 };
-constexpr int kMaxSel = 4;
+constexpr int kMaxSel = 8;
 constexpr uint8_t kSelNone = 31;
 struct ROp {
     uint8_t code;
     uint8_t nsel;        // 0..kMaxSel selector bits
+    uint8_t vstride;     // complex entries per variant (0..16)
+    uint8_t pad;
     uint8_t sel[kMaxSel];
-    uint8_t pad[2];
     uint32_t mat;        // pool index of variant 0 (complex entries)
-    uint32_t vstride;    // complex entries per variant
 };
 // Outer qubits (outside the tile) that select variants: at most this many per
 // pass, so that tile bits + outer bits stay below bit 31 of W.

@@ -236,7 +236,11 @@ __device__ __forceinline__ uint32_t rop_variant(const ROp &o, uint32_t W) {
     uint32_t var = 0;
     if (o.nsel) {
 #pragma unroll
-        for (int j = 0; j < kMaxSel; ++j) var |= ((W >> o.sel[j]) & 1u) << j;
+        for (int j = 0; j < 4; ++j) var |= ((W >> o.sel[j]) & 1u) << j;
+        if (o.nsel > 4) {
+#pragma unroll
+            for (int j = 4; j < kMaxSel; ++j) var |= ((W >> o.sel[j]) & 1u) << j;
+        }
     }
     return var;
 }
