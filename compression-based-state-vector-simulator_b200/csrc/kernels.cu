@@ -526,19 +526,41 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
         if (s_flag) break;
         ++ntiles;
 
-        // ---- decode
-        for (int c = warp; c < nchunks; c += nwarps) {
-            const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
-            const uint64_t blk = chunk >> blk_shift;
-            R *comp = reinterpret_cast<R *>(tile) + (size_t)c * ncomp;
-            if (a.first_pass && !a.mask[blk]) {
-                for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = R(0);
-                continue;
+        // ---- decode: the headers of HB of the warp's chunks are loaded
+        // together, then the chunks are unpacked one by one (complex64 takes
+        // four at a time; complex128 one, its register budget being tighter)
+        constexpr int HB = sizeof(R) == 4 ? 4 : 1;
+        for (int c0 = warp; c0 < nchunks; c0 += HB * nwarps) {
+            ChunkMeta md[HB];
+            bool zero[HB];
+#pragma unroll
+            for (int b = 0; b < HB; ++b) {
+                const int c = c0 + b * nwarps;
+                md[b].offset = 0;
+                md[b].base = 0;
+                md[b].width = 0;
+                zero[b] = true;
+                if (c < nchunks) {
+                    const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
+                    if (!a.first_pass || a.mask[chunk >> blk_shift]) {
+                        md[b] = a.meta_in[chunk];
+                        zero[b] = false;
+                    }
+                }
             }
-            const ChunkMeta md = a.meta_in[chunk];
-            decode_chunk<R>(a.arena_in, md, per_lane, a.codec, reinterpret_cast<R *>(tile), wstage, lane,
-                            TileSlot<R>{c << C, swm});
-            if (lane == 0) rd += payload_bytes(C, md.width) + sizeof(ChunkMeta);
+#pragma unroll
+            for (int b = 0; b < HB; ++b) {
+                const int c = c0 + b * nwarps;
+                if (c >= nchunks) break;
+                R *comp = reinterpret_cast<R *>(tile) + (size_t)c * ncomp;
+                if (zero[b]) {
+                    for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = R(0);
+                    continue;
+                }
+                decode_chunk<R>(a.arena_in, md[b], per_lane, a.codec, reinterpret_cast<R *>(tile), wstage, lane,
+                                TileSlot<R>{c << C, swm});
+                if (lane == 0) rd += payload_bytes(C, md[b].width) + sizeof(ChunkMeta);
+            }
         }
         __syncthreads();
 
