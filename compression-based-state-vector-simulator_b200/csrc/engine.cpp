@@ -19,6 +19,7 @@
 #include <complex>
 #include <cstdio>
 #include <cstring>
+#include <random>
 #include <set>
 #include <string>
 #include <vector>
@@ -1512,6 +1513,87 @@ qs_status qs_get_amplitudes(qs_state *h, uint64_t first, uint64_t count, double 
     }
     cudaFree(dbuf);
     return rs;
+}
+
+// Block-wise sampling of CompressedQuantumState::sampling_blockwise
+// (compressed_state.hpp:1600-1681) for one rank: the sequential FP64 block
+// masses and the within-block inverse-cdf searches run on the device
+// (launch_block_mass / launch_sample_in_block); the shot split, the uniform
+// draws and the final shuffle use the reference's generators
+// (std::mt19937_64 seeded with seed and with seed + 1, the binomial and
+// uniform distributions, std::shuffle) in its order, so the same decoded
+// amplitudes give the same samples.
+qs_status qs_sample_blockwise(qs_state *h, uint32_t n_shots, uint32_t seed, uint64_t *out) {
+    if (!h || (n_shots && !out)) return fail(h, QS_ERR_ARG, "NULL argument");
+    struct DevTmp {
+        void *p[5] = {};
+        ~DevTmp() {
+            for (void *q : p)
+                if (q) cudaFree(q);
+        }
+    } tmp;
+    double *prefix = nullptr, *bmass = nullptr, *rin = nullptr;
+    uint32_t *sblock = nullptr;
+    uint64_t *dout = nullptr;
+    CUDA_TRY(h, cudaMalloc(&prefix, h->nchunks * sizeof(double)));
+    tmp.p[0] = prefix;
+    CUDA_TRY(h, cudaMalloc(&bmass, h->nb * sizeof(double)));
+    tmp.p[1] = bmass;
+    CUDA_TRY(h, qs::launch_block_mass(h->f64, h->meta[h->mcur], h->arena[h->cur], h->mask, (int)h->B, (int)h->C,
+                                      h->codec, h->nb, prefix, bmass, h->stream));
+    std::vector<double> mass(h->nb);
+    CUDA_TRY(h, cudaMemcpyAsync(mass.data(), bmass, h->nb * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    double total = 0.0;
+    for (double m : mass) total += m;
+    if (!(total > 0.0) || !std::isfinite(total))
+        return fail(h, QS_ERR_DOMAIN,
+                    "CompressedQuantumState::sampling_blockwise: state has no finite positive probability mass");
+    std::mt19937_64 rng(seed);
+    std::vector<uint32_t> shots(mass.size(), 0);
+    uint32_t left = n_shots;
+    double rest = total;
+    for (size_t g = 0; g < mass.size() && left > 0; g++) {
+        const double pg = rest > 0 ? std::min(1.0, mass[g] / rest) : 0.0;
+        std::binomial_distribution<uint32_t> bin(left, pg);
+        const uint32_t k = (g + 1 == mass.size()) ? left : bin(rng);
+        shots[g] = k;
+        left -= k;
+        rest -= mass[g];
+    }
+    // rank 0 of the reference: its local generator is seeded with seed + 1
+    // in 32-bit arithmetic
+    std::mt19937_64 rng_local(static_cast<uint32_t>(seed + 1u));
+    std::uniform_real_distribution<double> uni(0.0, 1.0);
+    std::vector<uint32_t> hb;
+    std::vector<double> hr;
+    hb.reserve(n_shots);
+    hr.reserve(n_shots);
+    for (uint32_t b = 0; b < h->nb; b++)
+        for (uint32_t s = 0; s < shots[b]; s++) {
+            hb.push_back(b);
+            hr.push_back(uni(rng_local) * mass[b]);
+        }
+    const uint64_t ns = hb.size();
+    std::vector<uint64_t> mine(ns);
+    if (ns) {
+        CUDA_TRY(h, cudaMalloc(&sblock, ns * sizeof(uint32_t)));
+        tmp.p[2] = sblock;
+        CUDA_TRY(h, cudaMalloc(&rin, ns * sizeof(double)));
+        tmp.p[3] = rin;
+        CUDA_TRY(h, cudaMalloc(&dout, ns * sizeof(uint64_t)));
+        tmp.p[4] = dout;
+        CUDA_TRY(h, cudaMemcpyAsync(sblock, hb.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(rin, hr.data(), ns * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(h, qs::launch_sample_in_block(h->f64, h->meta[h->mcur], h->arena[h->cur], h->mask, (int)h->B,
+                                               (int)h->C, h->codec, prefix, bmass, sblock, rin, ns, dout,
+                                               h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(mine.data(), dout, ns * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    }
+    std::shuffle(mine.begin(), mine.end(), rng);
+    if (ns) std::memcpy(out, mine.data(), ns * sizeof(uint64_t));
+    return QS_OK;
 }
 
 qs_status qs_get_zero_mask(qs_state *h, uint8_t *out) {

@@ -266,6 +266,17 @@ cudaError_t launch_stage_end(const uint32_t *block_to_group, const uint8_t *grou
 cudaError_t launch_readout(bool f64, const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask,
                            int B, int C, CodecParams codec, uint64_t chunk0, uint64_t nchunks,
                            double *out, double scale, cudaStream_t stream);
+// Sequential FP64 |a|^2 sum of every block (block_mass[nblocks]) and the
+// running sum at the start of every chunk (prefix[nchunks]); 0 for zero blocks.
+cudaError_t launch_block_mass(bool f64, const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B,
+                              int C, CodecParams codec, uint32_t nblocks, double *prefix, double *block_mass,
+                              cudaStream_t stream);
+// For each shot s: the first amplitude of block shot_block[s] whose cumulative
+// |a|^2 reaches rin[s] (clamped to the block); out[s] = its global index.
+cudaError_t launch_sample_in_block(bool f64, const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask,
+                                   int B, int C, CodecParams codec, const double *prefix, const double *block_mass,
+                                   const uint32_t *shot_block, const double *rin, uint64_t nshots, uint64_t *out,
+                                   cudaStream_t stream);
 // sum |a|^2 over the stored blocks (FP64 accumulation); *out must be zeroed.
 cudaError_t launch_norm(bool f64, const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask,
                         int B, int C, CodecParams codec, uint64_t nchunks, double *out,

@@ -854,6 +854,107 @@ __global__ void readout_kernel(const ChunkMeta *meta, const uint32_t *arena, con
     }
 }
 
+// ------------------------------------------------------------ sampling
+// |a|^2 of amplitude a of a decoded chunk as x*x + y*y, rounded after each
+// operation (no fused multiply-add), so that the sums below are the ones of
+// the reference's std::norm loop (compressed_state.hpp:1615-1616).
+template <typename R>
+__device__ __forceinline__ double amp_norm(const R *vals, int a) {
+    const double x = (double)vals[2 * a], y = (double)vals[2 * a + 1];
+    return __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+}
+
+// Sequential FP64 mass of every block, one warp per block: the warp decodes
+// the block's chunks in order and lane 0 adds |a|^2 amplitude by amplitude,
+// the reference's order (compressed_state.hpp:1613-1619), so block_mass is
+// bit-identical to its `mass` for the same decoded amplitudes.  prefix[k] is
+// the running sum when chunk k of the block begins, so that the cumulative
+// distribution inside any chunk can be rebuilt exactly.  Zero blocks get 0.
+template <typename R>
+__global__ void block_mass_kernel(const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B, int C,
+                                  CodecParams p, uint32_t nblocks, double *prefix, double *block_mass) {
+    __shared__ uint32_t stage[kPassThreads / 32][kStageWords];
+    __shared__ R vals[kPassThreads / 32][2 << kMaxChunkLog2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int namps = 1 << C, per_lane = (2 << C) >> 5;
+    const uint32_t cpb = 1u << (B - C);
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t b = gw; b < nblocks; b += nw) {
+        const uint64_t k0 = b * cpb;
+        if (!mask[b]) {
+            for (uint32_t k = lane; k < cpb; k += 32) prefix[k0 + k] = 0.0;
+            if (lane == 0) block_mass[b] = 0.0;
+            continue;
+        }
+        double acc = 0.0;
+        for (uint32_t k = 0; k < cpb; ++k) {
+            decode_chunk<R>(arena, meta[k0 + k], per_lane, p, vals[warp], stage[warp], lane);
+            __syncwarp();
+            if (lane == 0) {
+                prefix[k0 + k] = acc;
+                for (int a = 0; a < namps; ++a) acc = __dadd_rn(acc, amp_norm(vals[warp], a));
+            }
+            __syncwarp();
+        }
+        if (lane == 0) block_mass[b] = acc;
+    }
+}
+
+// One shot per warp: the first amplitude j of block shot_block[s] whose
+// sequential cumulative |a|^2 reaches rin[s] (std::lower_bound over the
+// block's cdf, compressed_state.hpp:1652-1662), clamped to the block's last
+// amplitude.  The chunk is found by a binary search over the chunk-end sums
+// (prefix of the next chunk, block_mass for the last); inside it the running
+// sum restarts from prefix[chunk] and repeats the same additions.  A zero
+// block has an all-zero cdf, so its answer is j = 0.  out[s] = b * 2^B + j.
+template <typename R>
+__global__ void sample_in_block_kernel(const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B,
+                                       int C, CodecParams p, const double *prefix, const double *block_mass,
+                                       const uint32_t *shot_block, const double *rin, uint64_t nshots,
+                                       uint64_t *out) {
+    __shared__ uint32_t stage[kPassThreads / 32][kStageWords];
+    __shared__ R vals[kPassThreads / 32][2 << kMaxChunkLog2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int namps = 1 << C, per_lane = (2 << C) >> 5;
+    const uint32_t cpb = 1u << (B - C);
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t s = gw; s < nshots; s += nw) {
+        const uint64_t b = shot_block[s];
+        const uint64_t k0 = b * cpb;
+        const double r = rin[s];
+        if (!mask[b]) {
+            if (lane == 0) out[s] = b << B;
+            continue;
+        }
+        // first chunk whose end sum reaches r; the last chunk when none does
+        uint32_t lo = 0, hi = cpb - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            const double end = prefix[k0 + mid + 1];
+            if (end >= r) hi = mid;
+            else lo = mid + 1;
+        }
+        const uint32_t k = lo;
+        decode_chunk<R>(arena, meta[k0 + k], per_lane, p, vals[warp], stage[warp], lane);
+        __syncwarp();
+        if (lane == 0) {
+            double acc = prefix[k0 + k];
+            int j = namps - 1;
+            for (int a = 0; a < namps; ++a) {
+                acc = __dadd_rn(acc, amp_norm(vals[warp], a));
+                if (acc >= r) {
+                    j = a;
+                    break;
+                }
+            }
+            out[s] = (b << B) + ((uint64_t)k << C) + (uint64_t)j;
+        }
+        __syncwarp();
+    }
+}
+
 template <typename R>
 __global__ void norm_kernel(const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B, int C,
                             CodecParams p, uint64_t nchunks, double *out) {
@@ -1347,6 +1448,34 @@ cudaError_t launch_readout(bool f64, const ChunkMeta *meta, const uint32_t *aren
     const unsigned grid = grid_for(nchunks, kPassThreads / 32, 8);
     if (f64) readout_kernel<double><<<grid, kPassThreads, 0, s>>>(meta, arena, mask, B, C, p, chunk0, nchunks, out, scale);
     else readout_kernel<float><<<grid, kPassThreads, 0, s>>>(meta, arena, mask, B, C, p, chunk0, nchunks, out, scale);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_block_mass(bool f64, const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B,
+                              int C, CodecParams p, uint32_t nblocks, double *prefix, double *block_mass,
+                              cudaStream_t s) {
+    const unsigned grid = grid_for(nblocks, kPassThreads / 32, 8);
+    if (f64)
+        block_mass_kernel<double><<<grid, kPassThreads, 0, s>>>(meta, arena, mask, B, C, p, nblocks, prefix,
+                                                                block_mass);
+    else
+        block_mass_kernel<float><<<grid, kPassThreads, 0, s>>>(meta, arena, mask, B, C, p, nblocks, prefix,
+                                                               block_mass);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sample_in_block(bool f64, const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask,
+                                   int B, int C, CodecParams p, const double *prefix, const double *block_mass,
+                                   const uint32_t *shot_block, const double *rin, uint64_t nshots, uint64_t *out,
+                                   cudaStream_t s) {
+    if (!nshots) return cudaSuccess;
+    const unsigned grid = grid_for(nshots, kPassThreads / 32, 8);
+    if (f64)
+        sample_in_block_kernel<double><<<grid, kPassThreads, 0, s>>>(meta, arena, mask, B, C, p, prefix,
+                                                                     block_mass, shot_block, rin, nshots, out);
+    else
+        sample_in_block_kernel<float><<<grid, kPassThreads, 0, s>>>(meta, arena, mask, B, C, p, prefix, block_mass,
+                                                                    shot_block, rin, nshots, out);
     return cudaGetLastError();
 }
 

@@ -112,6 +112,16 @@ def eval_qft(quick):
             return np.exp(2j * np.pi * ((x * k) % (1 << n)) / (1 << n)) / math.sqrt(1 << n)
         f, e = _fidelity(cq, n, oracle)
         info.update(fidelity=f, max_abs_err=e)
+        # block-wise sampling on the device: |a|^2 = 2^-n, so the per-block
+        # counts of 10^6 shots are multinomial with equal cells
+        shots = 1_000_000
+        t0 = time.perf_counter()
+        smp = np.asarray(cq.sampling_blockwise(shots, 7), dtype=np.int64)
+        ms = (time.perf_counter() - t0) * 1e3
+        cnt = np.bincount(smp >> B, minlength=1 << (n - B))
+        e_blk = shots / cnt.size
+        info.update(sampling_ms_1e6_shots=ms,
+                    sampling_block_chi2_per_dof=float(((cnt - e_blk) ** 2 / e_blk).sum() / (cnt.size - 1)))
         out.append({"config": f"qft{n}: n={n} B={B} I={I} QFT of basis state {x}", **info})
         del cq
     return out

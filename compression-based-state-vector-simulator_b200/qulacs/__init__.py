@@ -579,16 +579,18 @@ class CompressedQuantumState:
         self._check(_n.lib().qs_import_store(self._h, buf.ctypes.data, buf.size))
 
     def sampling_blockwise(self, sampling_count: int, random_seed: int) -> List[int]:
-        """Draw basis-state samples from the renormalised state.  The
-        reference samples block by block (compressed_state.hpp:1600-1681); this
-        build reads the state back and samples by inverse CDF with a seeded
-        numpy generator -- the draws are not the reference's random stream."""
-        v = self.get_vector()
-        p = np.abs(v) ** 2
-        cdf = np.cumsum(p)
-        rng = np.random.default_rng(int(random_seed))
-        u = rng.random(int(sampling_count)) * cdf[-1]
-        return [int(x) for x in np.searchsorted(cdf, u, side="right").clip(0, v.size - 1)]
+        """Draw `sampling_count` basis-state indices block by block
+        (compressed_state.hpp:1600-1681): block masses and the searches inside
+        blocks on the device, the reference's seeded generators on the host,
+        so that equal amplitudes give the reference's samples.  Raises
+        ValueError when the state has no finite positive probability mass."""
+        n = int(sampling_count)
+        if n < 0 or n >= 1 << 32:
+            raise ValueError("sampling_count must fit an unsigned 32-bit integer")
+        out = np.empty(max(n, 1), dtype=np.uint64)
+        self._check(_n.lib().qs_sample_blockwise(self._h, n, int(random_seed) & 0xFFFFFFFF,
+                                                 out.ctypes.data_as(_n.ct.POINTER(_n.ct.c_uint64))))
+        return [int(x) for x in out[:n]]
 
     def __repr__(self):
         return f"CompressedQuantumState(qubits={self._n}, block_size={self._B})"

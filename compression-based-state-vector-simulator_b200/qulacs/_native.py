@@ -26,6 +26,7 @@ QS_ERR_TIMEOUT = 5
 QS_ERR_CORRUPT = 6
 QS_ERR_STATE = 7
 QS_ERR_NOMEM = 8
+QS_ERR_DOMAIN = 9
 
 QS_COMPLEX128 = 0
 QS_COMPLEX64 = 1
@@ -38,7 +39,7 @@ QS_FLAG_PROFILE = 0x8
 STATUS_NAMES = {
     0: "QS_OK", 1: "QS_ERR_ARG", 2: "QS_ERR_CUDA", 3: "QS_ERR_CAPACITY",
     4: "QS_ERR_UNSUPPORTED_GATE", 5: "QS_ERR_TIMEOUT", 6: "QS_ERR_CORRUPT",
-    7: "QS_ERR_STATE", 8: "QS_ERR_NOMEM",
+    7: "QS_ERR_STATE", 8: "QS_ERR_NOMEM", 9: "QS_ERR_DOMAIN",
 }
 
 
@@ -103,6 +104,7 @@ SIGNATURES = [
     ("qs_apply_circuit", ct.c_int, [_P]),
     ("qs_get_vector", ct.c_int, [_P, ct.POINTER(_D), ct.c_int]),
     ("qs_get_amplitudes", ct.c_int, [_P, _U64, _U64, ct.POINTER(_D), ct.c_int]),
+    ("qs_sample_blockwise", ct.c_int, [_P, ct.c_uint32, ct.c_uint32, ct.POINTER(_U64)]),
     ("qs_norm_squared", ct.c_int, [_P, ct.POINTER(_D)]),
     ("qs_expectation_pauli", ct.c_int, [_P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
     ("qs_transition_pauli", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
@@ -154,6 +156,11 @@ class QompsimError(RuntimeError):
         self.status = status
 
 
+class QompsimDomainError(QompsimError, ValueError):
+    """QS_ERR_DOMAIN: the reference raises std::domain_error, which its
+    bindings turn into ValueError."""
+
+
 def load_library(path: str = LIB_PATH):
     """Load libqompsim.so and declare its C signatures (no device work)."""
     global _lib
@@ -182,7 +189,8 @@ def check(status: int, handle=None, dense: bool = False) -> None:
         return
     L = lib()
     msg = (L.qs_dense_last_error(handle) if dense else L.qs_last_error(handle)) or b""
-    raise QompsimError(status, msg.decode(errors="replace"))
+    cls = QompsimDomainError if status == QS_ERR_DOMAIN else QompsimError
+    raise cls(status, msg.decode(errors="replace"))
 
 
 def make_gate_array(gates):

@@ -41,7 +41,8 @@ typedef enum qs_status {
     QS_ERR_TIMEOUT = 5,          /* reserved: a bounded device wait gave up             */
     QS_ERR_CORRUPT = 6,          /* imported store failed its length/header checks      */
     QS_ERR_STATE = 7,            /* call out of order (e.g. apply before registration)  */
-    QS_ERR_NOMEM = 8             /* host allocation failed                              */
+    QS_ERR_NOMEM = 8,            /* host allocation failed                              */
+    QS_ERR_DOMAIN = 9            /* no finite positive probability mass to sample from  */
 } qs_status;
 
 typedef enum qs_dtype {
@@ -193,6 +194,17 @@ qs_status qs_get_vector(qs_state *h, double *out, int renormalize);
  * Lets a caller stream a state larger than host memory allows at once
  * (fidelity in slices); the reference reads only whole vectors. */
 qs_status qs_get_amplitudes(qs_state *h, uint64_t first, uint64_t count, double *out, int renormalize);
+
+/* sampling_blockwise(sampling_count, random_seed) -- compressed_state.hpp:
+ * 1600-1681, one rank: n_shots basis-state indices into out[n_shots].  The
+ * per-block FP64 masses (sequential sums of x*x + y*y) and the searches
+ * inside blocks run on the device; the shot split over blocks
+ * (std::binomial_distribution on std::mt19937_64(seed)), the uniform draws
+ * (std::mt19937_64(seed + 1)) and the final std::shuffle follow the
+ * reference's order, so equal decoded amplitudes give equal samples.
+ * QS_ERR_DOMAIN when the total mass is not finite and positive (the
+ * reference's std::domain_error). */
+qs_status qs_sample_blockwise(qs_state *h, uint32_t n_shots, uint32_t seed, uint64_t *out);
 
 /* Squared norm of the compressed state, accumulated in FP64. */
 qs_status qs_norm_squared(qs_state *h, double *out);

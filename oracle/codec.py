@@ -57,6 +57,8 @@ def lib():
             f.argtypes = [P, I32, I32, ct.c_uint32, I32, I32, P, P]
         L.qsor_roundtrip_f64.argtypes = [P, ct.c_uint64, I32, I32, P]
         L.qsor_roundtrip_f32.argtypes = [P, ct.c_uint64, I32, I32, P]
+        L.qsor_sampling_blockwise.argtypes = [P, ct.c_uint32, ct.c_uint32, P, ct.c_uint32, ct.c_uint32, P]
+        L.qsor_sampling_blockwise.restype = ct.c_int
         _lib = L
     return _lib
 

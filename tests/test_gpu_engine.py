@@ -422,3 +422,47 @@ def test_amplitude_slices_match_full_vectors(qulacs_mod):
     d64 = qulacs_mod.QuantumState(n, dtype="complex64")
     c.update_quantum_state(d64)
     assert np.array_equal(d64.get_amplitudes(64, 128), d64.get_vector()[64:192])
+
+
+# ------------------------------------------------------------------ sampling
+@pytest.mark.parametrize("dtype,n,B", [("complex128", 12, 6), ("complex128", 14, 10), ("complex128", 10, 4),
+                                       ("complex64", 13, 8), ("complex64", 12, 12)])
+def test_sampling_blockwise_matches_oracle(qulacs_mod, dtype, n, B):
+    """Device block masses and in-block searches with the reference's seeded
+    generators on the host: the samples equal the oracle's, drawn from the
+    same decoded amplitudes, index for index."""
+    from oracle import sampling
+    c = helpers.optimized(helpers.random_circuit(n, 60, seed=n + B), B)
+    cq = _compressed(qulacs_mod, c, B, 3, dtype=dtype)
+    v = cq.get_vector(renormalize=False)
+    mask = cq.get_zero_mask()
+    for shots, seed in [(0, 1), (1, 2), (1000, 3), (20000, 2 ** 32 - 1)]:
+        got = cq.sampling_blockwise(shots, seed)
+        want = sampling.sampling_blockwise(v, B, shots, seed, stored=mask)
+        assert got == want, (shots, seed)
+    # the samples follow |a|^2: chi-square over the 64 heaviest amplitudes
+    got = np.asarray(cq.sampling_blockwise(200000, 17))
+    p = np.abs(v) ** 2
+    p /= p.sum()
+    top = np.argsort(p)[-64:]
+    cnt = np.bincount(got, minlength=v.size)[top]
+    e = p[top] * got.size
+    chi = float(((cnt - e) ** 2 / e).sum())
+    assert chi < 64 + 6 * math.sqrt(2 * 64), chi
+
+
+def test_sampling_blockwise_sparse_and_errors(qulacs_mod):
+    """GHZ: all mass in the first and last blocks, every sample is 0 or
+    2^n - 1.  A zero state has no mass to sample from."""
+    from oracle import sampling
+    from qompsim import circuits as C
+    n, B = 16, 8
+    cq = _compressed(qulacs_mod, C.ghz_fanout(n), B, 4)
+    mask = cq.get_zero_mask()
+    got = cq.sampling_blockwise(5000, 9)
+    assert set(got) == {0, (1 << n) - 1}
+    assert got == sampling.sampling_blockwise(cq.get_vector(renormalize=False), B, 5000, 9, stored=mask)
+    z = qulacs_mod.CompressedQuantumState(10, 5, eps_rel=1e-3, eps_abs=1e-7)
+    z.load(np.zeros(1 << 10, dtype=np.complex128))
+    with pytest.raises(ValueError):
+        z.sampling_blockwise(10, 1)
