@@ -25,6 +25,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <unistd.h>
 
 #include "../../include/qompsim.h"
 #include "codec.cuh"
@@ -756,6 +757,7 @@ struct qs_state {
     qs::ChunkMeta *meta[2] = {nullptr, nullptr};
     uint32_t *arena[2] = {nullptr, nullptr};
     uint64_t capacity = 0;
+    bool host_store = false;   // arenas in pinned, device-mapped host memory (QS_FLAG_HOST_STORE)
     unsigned long long *counters = nullptr;  // [0..1] bump, [2..4] stats, [5] init scratch, [6] header-pass bytes, [7] diagonal-pass total
     uint8_t *mask = nullptr;
     uint32_t *block_nz = nullptr;
@@ -790,7 +792,10 @@ struct qs_state {
     ~qs_state() {
         for (int i = 0; i < 2; ++i) {
             if (meta[i]) cudaFree(meta[i]);
-            if (arena[i]) cudaFree(arena[i]);
+            if (arena[i]) {
+                if (host_store) cudaFreeHost(arena[i]);
+                else cudaFree(arena[i]);
+            }
             if (ev[i]) cudaEventDestroy(ev[i]);
         }
         if (counters) cudaFree(counters);
@@ -842,7 +847,7 @@ struct qs_state {
         words[r * 32 + lane] |= (uint32_t)((uint64_t)q1 << s);
         if (s + w > 32) words[(r + 1) * 32 + lane] |= (uint32_t)((uint64_t)q1 >> (32 - s));
         qs::ChunkMeta md{0, 0, w};
-        CUDA_TRY(this, cudaMemcpyAsync(arena[cur], words.data(), words.size() * 4, cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(this, cudaMemcpyAsync(arena[cur], words.data(), words.size() * 4, cudaMemcpyDefault, stream));
         CUDA_TRY(this, cudaMemcpyAsync(meta[mcur] + chunk, &md, sizeof(md), cudaMemcpyHostToDevice, stream));
         const uint8_t one = 1;
         CUDA_TRY(this, cudaMemcpyAsync(mask + blk, &one, 1, cudaMemcpyHostToDevice, stream));
@@ -902,7 +907,9 @@ qs_status qs_create(qs_state **out, uint32_t n, uint32_t block_size, qs_dtype dt
     h->eps_rel = eps_rel;
     h->eps_abs = eps_abs;
     h->codec = cp;
+    if (env_int("QOMPSIM_HOST_STORE", 0)) flags |= QS_FLAG_HOST_STORE;
     h->flags = flags;
+    h->host_store = (flags & QS_FLAG_HOST_STORE) != 0;
     h->tile_log2 = env_int("QOMPSIM_TILE_LOG2", h->f64 ? 12 : 13);
     h->tile_log2 = std::max<int>(h->tile_log2, (int)h->C + 2);
     h->tile_log2 = std::min<int>(h->tile_log2, std::min<int>(qs::kMaxTileLog2, (int)h->C + qs::kMaxTileQubits));
@@ -923,16 +930,37 @@ qs_status qs_create(qs_state **out, uint32_t n, uint32_t block_size, qs_dtype dt
     const uint64_t worst = h->nchunks * qs::payload_bytes((int)h->C, 32);
     const uint64_t reserve = (uint64_t)1 << 30;
     uint64_t avail = free_b > 2 * meta_bytes + reserve ? free_b - 2 * meta_bytes - reserve : 0;
+    if (h->host_store) {
+        // spill tier: the two payload arenas live in pinned host memory that
+        // the passes read and write through the bus; headers, masks and
+        // counters stay in HBM.  Default size: a quarter of the host's free
+        // memory each (two arenas), at most the worst case.
+        const uint64_t host_free = (uint64_t)sysconf(_SC_AVPHYS_PAGES) * (uint64_t)sysconf(_SC_PAGESIZE);
+        avail = host_free / 2;
+    }
     const char *cap_env = std::getenv("QOMPSIM_ARENA_BYTES");
     h->capacity = cap_env ? (uint64_t)std::strtoull(cap_env, nullptr, 10) : std::min<uint64_t>(worst, avail / 2);
     h->capacity = (h->capacity + 127) / 128 * 128;
     if (h->capacity < std::min<uint64_t>(worst, 4096)) {
-        h->err = "not enough device memory for the compressed store";
+        h->err = h->host_store ? "not enough host memory for the compressed store"
+                               : "not enough device memory for the compressed store";
         return cleanup(QS_ERR_CAPACITY);
     }
     for (int i = 0; i < 2; ++i) {
         CREATE_TRY(cudaMalloc(&h->meta[i], meta_bytes));
-        CREATE_TRY(cudaMalloc(&h->arena[i], h->capacity));
+        if (h->host_store) {
+            void *hp = nullptr;
+            CREATE_TRY(cudaHostAlloc(&hp, h->capacity, cudaHostAllocMapped | cudaHostAllocPortable));
+            h->arena[i] = static_cast<uint32_t *>(hp);
+            void *dp = nullptr;
+            CREATE_TRY(cudaHostGetDevicePointer(&dp, hp, 0));
+            if (dp != hp) {
+                h->err = "mapped host arena has a different device address (no unified addressing)";
+                return cleanup(QS_ERR_CUDA);
+            }
+        } else {
+            CREATE_TRY(cudaMalloc(&h->arena[i], h->capacity));
+        }
         CREATE_TRY(cudaMemset(h->meta[i], 0, meta_bytes));
         CREATE_TRY(cudaEventCreate(&h->ev[i]));
     }
@@ -1636,6 +1664,8 @@ qs_status qs_get_total_times(qs_state *h, double out[10]) {
 qs_status qs_get_stats(qs_state *h, qs_stats *out) {
     if (!h || !out) return fail(h, QS_ERR_ARG, "NULL argument");
     *out = h->st;
+    out->arena_capacity = h->capacity;
+    out->host_store = h->host_store ? 1 : 0;
     return QS_OK;
 }
 
@@ -1982,7 +2012,7 @@ qs_status qs_checkpoint(qs_state *h, uint32_t slot) {
     cudaStream_t s = h->stream;
     CUDA_TRY(h, cudaMemcpyAsync(c.meta, h->meta[h->mcur], meta_bytes, cudaMemcpyDeviceToDevice, s));
     if (h->arena_used)
-        CUDA_TRY(h, cudaMemcpyAsync(c.arena, h->arena[h->cur], h->arena_used, cudaMemcpyDeviceToDevice, s));
+        CUDA_TRY(h, cudaMemcpyAsync(c.arena, h->arena[h->cur], h->arena_used, cudaMemcpyDefault, s));
     CUDA_TRY(h, cudaMemcpyAsync(c.mask, h->mask, h->nb, cudaMemcpyDeviceToDevice, s));
     CUDA_TRY(h, cudaMemcpyAsync(c.block_bytes, h->block_bytes, h->nb * sizeof(unsigned long long),
                                 cudaMemcpyDeviceToDevice, s));
@@ -1997,7 +2027,7 @@ qs_status qs_restore(qs_state *h, uint32_t slot) {
     auto &c = h->ckpt[slot];
     cudaStream_t s = h->stream;
     CUDA_TRY(h, cudaMemcpyAsync(h->meta[h->mcur], c.meta, h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyDeviceToDevice, s));
-    if (c.used) CUDA_TRY(h, cudaMemcpyAsync(h->arena[h->cur], c.arena, c.used, cudaMemcpyDeviceToDevice, s));
+    if (c.used) CUDA_TRY(h, cudaMemcpyAsync(h->arena[h->cur], c.arena, c.used, cudaMemcpyDefault, s));
     CUDA_TRY(h, cudaMemcpyAsync(h->mask, c.mask, h->nb, cudaMemcpyDeviceToDevice, s));
     CUDA_TRY(h, cudaMemcpyAsync(h->block_bytes, c.block_bytes, h->nb * sizeof(unsigned long long),
                                 cudaMemcpyDeviceToDevice, s));
@@ -2043,7 +2073,7 @@ qs_status qs_export_store(qs_state *h, void *buf, uint64_t cap, uint64_t *size) 
     p += h->nb * 8;
     CUDA_TRY(h, cudaMemcpyAsync(p, h->meta[h->mcur], h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyDeviceToHost, s));
     p += h->nchunks * sizeof(qs::ChunkMeta);
-    if (h->arena_used) CUDA_TRY(h, cudaMemcpyAsync(p, h->arena[h->cur], h->arena_used, cudaMemcpyDeviceToHost, s));
+    if (h->arena_used) CUDA_TRY(h, cudaMemcpyAsync(p, h->arena[h->cur], h->arena_used, cudaMemcpyDefault, s));
     CUDA_TRY(h, cudaStreamSynchronize(s));
     h->times[8] += 0;  // d2h time is measured by callers with their own events
     return QS_OK;
@@ -2072,7 +2102,7 @@ qs_status qs_import_store(qs_state *h, const void *buf, uint64_t size) {
     p += h->nb * 8;
     CUDA_TRY(h, cudaMemcpyAsync(h->meta[h->mcur], p, h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyHostToDevice, s));
     p += h->nchunks * sizeof(qs::ChunkMeta);
-    if (hd.arena_bytes) CUDA_TRY(h, cudaMemcpyAsync(h->arena[h->cur], p, hd.arena_bytes, cudaMemcpyHostToDevice, s));
+    if (hd.arena_bytes) CUDA_TRY(h, cudaMemcpyAsync(h->arena[h->cur], p, hd.arena_bytes, cudaMemcpyDefault, s));
     CUDA_TRY(h, cudaStreamSynchronize(s));
     h->arena_used = hd.arena_bytes;
     uint64_t total = 0;

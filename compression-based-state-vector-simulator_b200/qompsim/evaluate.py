@@ -1,6 +1,6 @@
 """Per-configuration evaluation of the compressed pipeline on one GPU.
 
-    python -m qompsim.evaluate [--only ghz20 qft30 brickwork32 hea24 qaoa34] [--quick]
+    python -m qompsim.evaluate [--only ghz20 qft30 brickwork32 hea24 qaoa34 host_store28] [--quick]
 
 For each configuration of the benchmark suite (seeded synthetic circuits) it
 prints one JSON line with the stage list, the compressed size, the apply time
@@ -42,11 +42,12 @@ def _optimized(circuit, block_size):
     return circuit
 
 
-def _compressed_run(circuit, n, B, I, dtype, eps_rel=1e-3, eps_abs=1e-7, reps=2):
+def _compressed_run(circuit, n, B, I, dtype, eps_rel=1e-3, eps_abs=1e-7, reps=2, host_store=False):
     import qulacs
     from qulacs import _native
     cq = qulacs.CompressedQuantumState(n, B, dtype=dtype, eps_rel=eps_rel, eps_abs=eps_abs,
-                                       flags=_native.QS_FLAG_QUIET | _native.QS_FLAG_PROFILE)
+                                       flags=_native.QS_FLAG_QUIET | _native.QS_FLAG_PROFILE,
+                                       host_store=host_store)
     cq.partition_and_register_circuit(circuit, I, 0)
     times = []
     for _ in range(reps):
@@ -250,7 +251,44 @@ def eval_qaoa(quick):
     return out
 
 
-EVALS = {"ghz20": eval_ghz, "qft30": eval_qft, "brickwork32": eval_brickwork, "hea24": eval_hea, "qaoa34": eval_qaoa}
+def eval_host_store(quick):
+    """Spill tier: the QFT with its payload arenas in pinned host memory
+    (each arena bounded to 4 GiB) against the HBM store, same passes."""
+    import os
+    from qompsim import circuits as C
+    n = 26 if quick else 28
+    B, I = 20, 4
+    out = []
+    first = None
+    for host in (False, True):
+        old = os.environ.get("QOMPSIM_ARENA_BYTES")
+        if host:
+            os.environ["QOMPSIM_ARENA_BYTES"] = str(4 << 30)
+        try:
+            c = _optimized(C.qft_basis(n, 0), B)
+            cq, info = _compressed_run(c, n, B, I, "complex128", host_store=host)
+        finally:
+            if host:
+                if old is None:
+                    os.environ.pop("QOMPSIM_ARENA_BYTES", None)
+                else:
+                    os.environ["QOMPSIM_ARENA_BYTES"] = old
+        st = cq.get_stats()
+        moved = st["bytes_read"] + st["bytes_written"]
+        head = cq.get_amplitudes(0, min(SLICE, 1 << n), renormalize=False)
+        if first is None:
+            first = head
+        info.update(host_store=bool(st["host_store"]), payload_and_header_bytes=int(moved),
+                    effective_gb_per_s=moved / (info["apply_ms"] * 1e6),
+                    first_slice_identical=bool(np.array_equal(head, first)))
+        out.append({"config": f"qft{n} spill tier: n={n} B={B} I={I}, payload in "
+                              f"{'pinned host memory' if host else 'HBM'}", **info})
+        del cq
+    return out
+
+
+EVALS = {"ghz20": eval_ghz, "qft30": eval_qft, "brickwork32": eval_brickwork, "hea24": eval_hea, "qaoa34": eval_qaoa,
+         "host_store28": eval_host_store}
 
 
 def main(argv=None):

@@ -357,10 +357,13 @@ class CompressedQuantumState:
     (default 1e-7) at construction, as in the reference.  QOMPSIM_DTYPE picks
     complex128 (default) or complex64.  QOMPSIM_ZERO_TEST=exact selects the
     reference GPU build's exact zero-block test (default: all codes zero);
-    QOMPSIM_REFERENCE_CONTROLS=1 reproduces the reference's control handling."""
+    QOMPSIM_REFERENCE_CONTROLS=1 reproduces the reference's control handling.
+    host_store=True (or QOMPSIM_HOST_STORE=1) keeps the compressed payload in
+    pinned host memory that the device passes stream over the bus: the
+    spill tier for stores larger than HBM."""
 
     def __init__(self, qubit_count: int, block_size: int, dtype=None, eps_rel: Optional[float] = None,
-                 eps_abs: Optional[float] = None, flags: Optional[int] = None):
+                 eps_abs: Optional[float] = None, flags: Optional[int] = None, host_store: bool = False):
         L = _n.lib()
         self._n = int(qubit_count)
         self._B = int(block_size)
@@ -375,6 +378,8 @@ class CompressedQuantumState:
                 flags |= _n.QS_FLAG_REFERENCE_CONTROLS
             if os.environ.get("QOMPSIM_QUIET", "0") == "1":
                 flags |= _n.QS_FLAG_QUIET
+        if host_store:
+            flags |= _n.QS_FLAG_HOST_STORE
         self._flags = int(flags)
         h = _n.ct.c_void_p()
         _n.check(L.qs_create(_n.ct.byref(h), self._n, self._B, self._dtype, self._eps_rel, self._eps_abs,

@@ -35,6 +35,7 @@ QS_FLAG_EXACT_ZERO_TEST = 0x1
 QS_FLAG_REFERENCE_CONTROLS = 0x2
 QS_FLAG_QUIET = 0x4
 QS_FLAG_PROFILE = 0x8
+QS_FLAG_HOST_STORE = 0x10
 
 STATUS_NAMES = {
     0: "QS_OK", 1: "QS_ERR_ARG", 2: "QS_ERR_CUDA", 3: "QS_ERR_CAPACITY",
@@ -74,6 +75,8 @@ class qs_stats(ct.Structure):
         ("perm_passes", ct.c_uint64),
         ("perm_bytes", ct.c_uint64),
         ("perm_ms", ct.c_double),
+        ("arena_capacity", ct.c_uint64),
+        ("host_store", ct.c_uint64),
     ]
 
 

@@ -10,8 +10,9 @@
  *   qs_state  -- the block-wise compressed state (CompressedQuantumState,
  *                src/cppsim/compressed_state.hpp:9).  The compressed store
  *                lives in device memory (HBM) for the whole life of the
- *                handle; the reference kept it in host malloc buffers and
- *                moved every group over PCIe each stage
+ *                handle (its payload in mapped host memory with
+ *                QS_FLAG_HOST_STORE); the reference kept it in host malloc
+ *                buffers and moved every group over PCIe each stage
  *                (src/cppsim/compressed_state_cuda.cu:209-223, 343-370).
  *   qs_dense  -- an uncompressed state vector in device memory (QuantumState,
  *                src/cppsim/state.hpp:445-1045, updated gate by gate through
@@ -36,7 +37,7 @@ typedef enum qs_status {
     QS_OK = 0,
     QS_ERR_ARG = 1,              /* invalid argument (sizes, indices, bounds)          */
     QS_ERR_CUDA = 2,             /* a CUDA runtime call failed                          */
-    QS_ERR_CAPACITY = 3,         /* compressed store does not fit the device memory     */
+    QS_ERR_CAPACITY = 3,         /* compressed store does not fit its arenas            */
     QS_ERR_UNSUPPORTED_GATE = 4, /* gate with >2 qubits, FusedSWAP (needs MPI ranks)    */
     QS_ERR_TIMEOUT = 5,          /* reserved: a bounded device wait gave up             */
     QS_ERR_CORRUPT = 6,          /* imported store failed its length/header checks      */
@@ -64,6 +65,13 @@ typedef enum qs_dtype {
                                         (compressed_state.hpp:998-1008, compressed_state_cuda.cu:632-642) */
 #define QS_FLAG_QUIET 0x4u           /* no progress prints on stdout */
 #define QS_FLAG_PROFILE 0x8u         /* time every fused pass with CUDA events (qs_stats.kernel_ms) */
+#define QS_FLAG_HOST_STORE 0x10u     /* spill tier: the compressed payload arenas live in pinned,
+                                        device-mapped host memory (a quarter of the host's free
+                                        memory each unless QOMPSIM_ARENA_BYTES says otherwise) and
+                                        the passes stream them over the bus; chunk headers, masks
+                                        and counters stay in HBM.  Also set by QOMPSIM_HOST_STORE=1.
+                                        The reference keeps its blocks in host memory
+                                        (compressed_state_cuda.cu:343) */
 
 /* One gate as the reference's partition_and_register_circuit binding hands
  * it to the engine: to_matrix_gate(gate) with the original name kept
@@ -102,6 +110,8 @@ typedef struct qs_stats {
                                     qubits >= chunk_log2, applied without decoding)     */
     uint64_t perm_bytes;         /* chunk-header bytes read + written by those passes   */
     double perm_ms;              /* their device time (QS_FLAG_PROFILE), else 0         */
+    uint64_t arena_capacity;     /* bytes of each of the two payload arenas             */
+    uint64_t host_store;         /* 1 when the arenas are in host memory (QS_FLAG_HOST_STORE) */
 } qs_stats;
 
 /* ---------------------------------------------------------------- errors */

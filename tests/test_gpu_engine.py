@@ -113,11 +113,12 @@ def test_dense_norm_load_and_basis(qulacs_mod):
 
 
 # ------------------------------------------------------------------ compressed
-def _compressed(qulacs, c, B, I, dtype="complex128", eps_rel=1e-3, eps_abs=1e-7, flags=None, basis=None):
+def _compressed(qulacs, c, B, I, dtype="complex128", eps_rel=1e-3, eps_abs=1e-7, flags=None, basis=None,
+                host_store=False):
     from qulacs import _native
     f = _native.QS_FLAG_QUIET if flags is None else flags
     cq = qulacs.CompressedQuantumState(c.get_qubit_count(), B, dtype=dtype, eps_rel=eps_rel, eps_abs=eps_abs,
-                                       flags=f)
+                                       flags=f, host_store=host_store)
     if basis is not None:
         cq.set_computational_basis(basis)
     cq.partition_and_register_circuit(c, I, 0)
@@ -466,3 +467,38 @@ def test_sampling_blockwise_sparse_and_errors(qulacs_mod):
     z.load(np.zeros(1 << 10, dtype=np.complex128))
     with pytest.raises(ValueError):
         z.sampling_blockwise(10, 1)
+
+
+# ------------------------------------------------------------ spill tier
+@pytest.mark.parametrize("dtype,circ", [("complex128", "random"), ("complex64", "random"), ("complex128", "qft")])
+def test_host_store_bit_identical(qulacs_mod, dtype, circ):
+    """Payload arenas in mapped host memory run the same passes: vectors,
+    masks, byte histories and samples equal the HBM store's (the arena
+    layout itself depends on the order in which tiles reserve space);
+    checkpoints (in HBM) restore into the host arenas and exported stores
+    cross between the tiers."""
+    from qompsim import circuits as C
+    n, B = 16, 9
+    c = helpers.random_circuit(n, 120, seed=5) if circ == "random" else C.qft_basis(n, 3)
+    c = helpers.optimized(c, B)
+    ref = _compressed(qulacs_mod, c, B, 3, dtype=dtype)
+    hs = _compressed(qulacs_mod, c, B, 3, dtype=dtype, host_store=True)
+    assert hs.get_stats()["host_store"] == 1 and ref.get_stats()["host_store"] == 0
+    v = ref.get_vector(renormalize=False)
+    assert np.array_equal(v, hs.get_vector(renormalize=False))
+    assert np.array_equal(ref.get_zero_mask(), hs.get_zero_mask())
+    assert ref.get_SV_bytes_history() == hs.get_SV_bytes_history()
+    assert ref.sampling_blockwise(1000, 3) == hs.sampling_blockwise(1000, 3)
+    hs.checkpoint(0)
+    hs.set_zero_state()
+    hs.restore(0)
+    assert np.array_equal(v, hs.get_vector(renormalize=False))
+    hs.free_checkpoint(0)
+    blob = ref.export_store()
+    hs.set_zero_state()
+    hs.import_store(blob)
+    assert np.array_equal(v, hs.get_vector(renormalize=False))
+    blob = hs.export_store()
+    ref.set_zero_state()
+    ref.import_store(blob)
+    assert np.array_equal(v, ref.get_vector(renormalize=False))
