@@ -746,6 +746,7 @@ struct qs_state {
         int8_t outer_q[qs::kMaxOuterSel];
         bool first, final;
         int kind;             // 0: tile pass, 1: chunk-header permutation only
+        bool code_moves;      // tile pass whose ops only move amplitudes (X / SWAP)
         qs::ChunkPerm perm;   // where the pass stores each chunk
     };
     qs::Sweep *sweeps_dev = nullptr;
@@ -1133,6 +1134,12 @@ static qs_status build_device_plan(qs_state *h) {
             for (size_t i = 0; i < outer.size(); ++i) dp.outer_q[i] = (int8_t)outer[i];
             dp.op_off = (uint32_t)op0;
             dp.sweep_off = (uint32_t)sw.size();
+            // a pass of pure register moves carries codes through the tile
+            dp.code_moves = env_int("QOMPSIM_CODE_MOVES", 1) != 0 && ops.size() > op0;
+            for (size_t o = op0; o < ops.size() && dp.code_moves; ++o) {
+                const int c = ops[o].code;
+                dp.code_moves = (c >= qs::OPC_X && c < qs::OPC_X + 8) || (c >= qs::OPC_SWAP && c < qs::OPC_SWAP + 64);
+            }
             if (std::getenv("QOMPSIM_DEBUG_PLAN")) {
                 int kinds[5] = {0, 0, 0, 0, 0}, sel = 0, half = 0, moves = 0;
                 for (size_t o = op0; o < ops.size(); ++o) {
@@ -1422,6 +1429,7 @@ qs_status qs_apply_circuit(qs_state *h) {
             a.first_pass = dp.first;
             a.final_pass = dp.final;
             a.exact_zero = (h->flags & QS_FLAG_EXACT_ZERO_TEST) ? 1 : 0;
+            a.code_moves = dp.code_moves ? 1 : 0;
             a.block_nz = h->block_nz;
             a.block_bytes = h->block_acc;
             a.error = h->error_dev;
@@ -1456,8 +1464,11 @@ qs_status qs_apply_circuit(qs_state *h) {
     uint64_t updates = 0;
     for (size_t st = 0; st < ns; ++st) updates += (uint64_t)h->stages[st].size() * hist[ns + 1 + st] << h->B;
     double pass_ms = 0, perm_ms = 0;
-    uint64_t perm_passes = 0;
-    for (size_t p = 0; p < h->passes.size(); ++p) perm_passes += h->passes[p].kind == 1 ? 1 : 0;
+    uint64_t perm_passes = 0, code_passes = 0;
+    for (size_t p = 0; p < h->passes.size(); ++p) {
+        perm_passes += h->passes[p].kind == 1 ? 1 : 0;
+        code_passes += (h->passes[p].kind == 0 && h->passes[p].code_moves) ? 1 : 0;
+    }
     for (size_t p = 0; p < h->pass_ev.size() / 2; ++p) {
         float t = 0;
         CUDA_TRY(h, cudaEventElapsedTime(&t, h->pass_ev[2 * p], h->pass_ev[2 * p + 1]));
@@ -1477,6 +1488,7 @@ qs_status qs_apply_circuit(qs_state *h) {
     h->st.chunk_log2 = (int32_t)h->C;
     h->st.tile_log2 = h->tile_log2;
     h->st.perm_passes = perm_passes;
+    h->st.code_move_passes = code_passes;
     h->st.perm_bytes = ctr[6];
     h->st.perm_ms = perm_ms;
     if (!h->quiet()) {
@@ -2093,6 +2105,24 @@ qs_status qs_import_store(qs_state *h, const void *buf, uint64_t size) {
     if (size != need) return fail(h, QS_ERR_CORRUPT, "store length does not match its header");
     if (hd.arena_bytes > h->capacity) return fail(h, QS_ERR_CAPACITY, "store larger than the arena");
     const char *p = (const char *)buf + sizeof(hd);
+    // every header of a stored block must describe a payload inside the
+    // arena, 128-byte aligned (the decoders copy payloads with 16-byte
+    // asynchronous copies); headers of unstored blocks are never read and
+    // are zeroed
+    const uint8_t *imask = (const uint8_t *)p;
+    std::vector<qs::ChunkMeta> metas(h->nchunks);
+    std::memcpy(metas.data(), p + nbpad + h->nb * 8, h->nchunks * sizeof(qs::ChunkMeta));
+    const uint32_t cshift = h->B - h->C;
+    for (uint64_t k = 0; k < h->nchunks; ++k) {
+        qs::ChunkMeta &md = metas[k];
+        if (!imask[k >> cshift]) {
+            md = qs::ChunkMeta{0, 0, 0};
+            continue;
+        }
+        const uint64_t pb = md.width <= 32 ? qs::payload_bytes((int)h->C, md.width) : 0;
+        if (md.width > 32 || (md.offset & 127) != 0 || md.offset > hd.arena_bytes || pb > hd.arena_bytes - md.offset)
+            return fail(h, QS_ERR_CORRUPT, "chunk header outside the stored arena");
+    }
     cudaStream_t s = h->stream;
     CUDA_TRY(h, cudaMemcpyAsync(h->mask, p, h->nb, cudaMemcpyHostToDevice, s));
     p += nbpad;
@@ -2100,7 +2130,8 @@ qs_status qs_import_store(qs_state *h, const void *buf, uint64_t size) {
     std::vector<uint64_t> bb(h->nb);
     std::memcpy(bb.data(), p, h->nb * 8);
     p += h->nb * 8;
-    CUDA_TRY(h, cudaMemcpyAsync(h->meta[h->mcur], p, h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(h, cudaMemcpyAsync(h->meta[h->mcur], metas.data(), h->nchunks * sizeof(qs::ChunkMeta),
+                                cudaMemcpyHostToDevice, s));
     p += h->nchunks * sizeof(qs::ChunkMeta);
     if (hd.arena_bytes) CUDA_TRY(h, cudaMemcpyAsync(h->arena[h->cur], p, hd.arena_bytes, cudaMemcpyDefault, s));
     CUDA_TRY(h, cudaStreamSynchronize(s));

@@ -145,6 +145,8 @@ struct PassArgs {
     const uint8_t *group_active;
     const uint8_t *mask;                // zero-block mask at stage start
     int32_t first_pass, final_pass, exact_zero;
+    int32_t code_moves;                 // 1: every op is an X / SWAP register move (no arithmetic),
+                                        // so the tile carries quantised codes, not values
     uint32_t *block_nz;                 // final pass: any non-zero in block
     unsigned long long *block_bytes;    // final pass: stored bytes of block
     int32_t *error;                     // 1 = arena overflow

@@ -333,33 +333,42 @@ struct TileSlot {
     __device__ __forceinline__ int operator()(int c) const { return 2 * swz<R>(elem0 + (c >> 1), swm) + (c & 1); }
 };
 
+// A quantised code held in a tile slot of type R (its bit pattern; only
+// moved, never used in arithmetic), for passes that move amplitudes
+// without changing them.  quantise(dequantise(c)) == c for every code, so
+// moving codes gives the same store as moving values.
+__device__ __forceinline__ float code_as_value(int32_t c, float) { return __int_as_float(c); }
+__device__ __forceinline__ double code_as_value(int32_t c, double) { return __longlong_as_double((long long)c); }
+__device__ __forceinline__ int32_t value_as_code(float v) { return __float_as_int(v); }
+__device__ __forceinline__ int32_t value_as_code(double v) { return (int32_t)__double_as_longlong(v); }
+
 // Words of the per-warp staging area of decode_chunk: one row more than a
 // chunk can use, so that the look-ahead word of the last row stays inside.
 constexpr int kStageWords = (kMaxPerLane + 1) * 32;
 
-template <typename R, typename Slot = LinearSlot>
+template <typename R, typename Slot = LinearSlot, bool kCodes = false>
 __device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena, const ChunkMeta md,
                                              int per_lane, CodecParams p, R *comp, uint32_t *wstage,
                                              int lane, Slot slot = Slot()) {
     const uint32_t w = md.width;
     if (w == 0) {
-        const R v = dequantize_hot(md.base, p, R());
+        const R v = kCodes ? code_as_value(md.base, R()) : dequantize_hot(md.base, p, R());
         for (int i = 0; i < per_lane; ++i) comp[slot(lane + 32 * i)] = v;
         return;
     }
     const int rows = (int)(((uint32_t)per_lane * w + 31) >> 5);
     const uint32_t *src = arena + (md.offset >> 2);
-    // payload rows into the warp's staging, half of them at a time through registers
-    constexpr int H = kMaxPerLane / 2;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        uint32_t tmp[H];
-#pragma unroll
-        for (int r = 0; r < H; ++r)
-            if (h * H + r < rows) tmp[r] = __ldcs(src + (h * H + r) * 32 + lane);
-#pragma unroll
-        for (int r = 0; r < H; ++r)
-            if (h * H + r < rows) wstage[(h * H + r) * 32 + lane] = tmp[r];
+    // the payload (rows x 128 contiguous bytes, 128-byte aligned) into the
+    // warp's staging with asynchronous 16-byte copies: no registers, one
+    // round trip to memory for the whole chunk
+    {
+        const uint32_t sdst = (uint32_t)__cvta_generic_to_shared(wstage);
+        const char *gsrc = reinterpret_cast<const char *>(src);
+        for (int off = lane * 16; off < rows * 128; off += 32 * 16)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sdst + off), "l"(gsrc + off) : "memory");
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncwarp();
     }
     // element i of this lane's stream starts at bit i*w: every element is
     // extracted independently (one funnel shift); a lane reads only its own words
@@ -369,7 +378,8 @@ __device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena,
         if (i < per_lane) {
             const uint32_t bit = (uint32_t)i * w, r = bit >> 5;
             const uint32_t u = __funnelshift_r(wstage[r * 32 + lane], wstage[(r + 1) * 32 + lane], bit & 31) & mask;
-            comp[slot(lane + 32 * i)] = dequantize_hot((int32_t)((uint32_t)md.base + u), p, R());
+            const int32_t code = (int32_t)((uint32_t)md.base + u);
+            comp[slot(lane + 32 * i)] = kCodes ? code_as_value(code, R()) : dequantize_hot(code, p, R());
         }
     }
 }
@@ -377,7 +387,7 @@ __device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena,
 // Per-warp quantisation of one chunk held in comp[]: codes overwrite the
 // chunk's own shared memory as int32.  Returns
 // base/width/non-zero flag (valid in every lane).
-template <typename R, typename Slot = LinearSlot>
+template <typename R, typename Slot = LinearSlot, bool kCodes = false>
 __device__ __forceinline__ void quantize_chunk(R *comp, int per_lane, CodecParams p, bool exact_zero,
                                                int lane, int32_t *base_out, uint32_t *width_out,
                                                bool *nz_out, Slot slot = Slot(), int32_t *codes = nullptr) {
@@ -398,11 +408,12 @@ __device__ __forceinline__ void quantize_chunk(R *comp, int per_lane, CodecParam
 #pragma unroll
         for (int i = 0; i < H; ++i) {
             if (h * H + i < per_lane) {
-                const int32_t q = quantize_hot(v[i], p);
+                const int32_t q = kCodes ? value_as_code(v[i]) : quantize_hot(v[i], p);
                 codes[lane + 32 * (h * H + i)] = q;
                 lo = min(lo, q);
                 hi = max(hi, q);
-                nz |= exact_zero ? (v[i] != R(0)) : (q != 0);
+                // code 0 is exactly the value 0
+                nz |= (exact_zero && !kCodes) ? (v[i] != R(0)) : (q != 0);
             }
         }
         __syncwarp();
@@ -486,7 +497,10 @@ static_assert((kSweepThreads / 32) * kStageWords * 4 >= 2 * kMaxDiagTerms * size
               "the pass kernel's decode staging holds the diagonal-sum coefficients");
 
 // ------------------------------------------------------------ pass kernel
-template <typename R, int RB>
+// kCodes: every op of the pass only moves amplitudes (X / SWAP register
+// moves, chunk permutations), so the tile holds the quantised codes
+// themselves and the pass skips dequantisation and quantisation.
+template <typename R, int RB, bool kCodes>
 __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -557,8 +571,8 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
                     for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = R(0);
                     continue;
                 }
-                decode_chunk<R>(a.arena_in, md[b], per_lane, a.codec, reinterpret_cast<R *>(tile), wstage, lane,
-                                TileSlot<R>{c << C, swm});
+                decode_chunk<R, TileSlot<R>, kCodes>(a.arena_in, md[b], per_lane, a.codec,
+                                                     reinterpret_cast<R *>(tile), wstage, lane, TileSlot<R>{c << C, swm});
                 if (lane == 0) rd += payload_bytes(C, md[b].width) + sizeof(ChunkMeta);
             }
         }
@@ -568,8 +582,10 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
         tile_sweeps<R, RB>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool),
                            outer_word(chunk_base << C, s_oq, a.nouter));
         // the decode staging area is free here: it holds the tile's term coefficients
-        if (a.diag.nterms)
-            tile_diag_sum<R>(tile, nb, swm, a.diag, chunk_base << C, reinterpret_cast<double *>(stage_all));
+        if constexpr (!kCodes) {
+            if (a.diag.nterms)
+                tile_diag_sum<R>(tile, nb, swm, a.diag, chunk_base << C, reinterpret_cast<double *>(stage_all));
+        }
 
         // ---- quantise (codes replace values in shared memory)
         for (int c = warp; c < nchunks; c += nwarps) {
@@ -577,8 +593,9 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
             int32_t base;
             uint32_t width;
             bool nz;
-            quantize_chunk<R>(reinterpret_cast<R *>(tile), per_lane, a.codec, a.exact_zero != 0, lane, &base,
-                              &width, &nz, TileSlot<R>{c << C, swm}, reinterpret_cast<int32_t *>(comp));
+            quantize_chunk<R, TileSlot<R>, kCodes>(reinterpret_cast<R *>(tile), per_lane, a.codec, a.exact_zero != 0,
+                                                   lane, &base, &width, &nz, TileSlot<R>{c << C, swm},
+                                                   reinterpret_cast<int32_t *>(comp));
             if (lane == 0) {
                 s_base[c] = base;
                 s_width[c] = width;
@@ -835,7 +852,7 @@ __global__ void sum_mask_bytes_kernel(const uint8_t *mask, const unsigned long l
 template <typename R>
 __global__ void readout_kernel(const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B, int C,
                                CodecParams p, uint64_t chunk0, uint64_t nchunks, double *out, double scale) {
-    __shared__ uint32_t stage[kPassThreads / 32][kStageWords];
+    __shared__ __align__(16) uint32_t stage[kPassThreads / 32][kStageWords];
     __shared__ R vals[kPassThreads / 32][2 << kMaxChunkLog2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ncomp = 2 << C, per_lane = ncomp >> 5;
@@ -873,7 +890,7 @@ __device__ __forceinline__ double amp_norm(const R *vals, int a) {
 template <typename R>
 __global__ void block_mass_kernel(const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B, int C,
                                   CodecParams p, uint32_t nblocks, double *prefix, double *block_mass) {
-    __shared__ uint32_t stage[kPassThreads / 32][kStageWords];
+    __shared__ __align__(16) uint32_t stage[kPassThreads / 32][kStageWords];
     __shared__ R vals[kPassThreads / 32][2 << kMaxChunkLog2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int namps = 1 << C, per_lane = (2 << C) >> 5;
@@ -913,7 +930,7 @@ __global__ void sample_in_block_kernel(const ChunkMeta *meta, const uint32_t *ar
                                        int C, CodecParams p, const double *prefix, const double *block_mass,
                                        const uint32_t *shot_block, const double *rin, uint64_t nshots,
                                        uint64_t *out) {
-    __shared__ uint32_t stage[kPassThreads / 32][kStageWords];
+    __shared__ __align__(16) uint32_t stage[kPassThreads / 32][kStageWords];
     __shared__ R vals[kPassThreads / 32][2 << kMaxChunkLog2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int namps = 1 << C, per_lane = (2 << C) >> 5;
@@ -958,7 +975,7 @@ __global__ void sample_in_block_kernel(const ChunkMeta *meta, const uint32_t *ar
 template <typename R>
 __global__ void norm_kernel(const ChunkMeta *meta, const uint32_t *arena, const uint8_t *mask, int B, int C,
                             CodecParams p, uint64_t nchunks, double *out) {
-    __shared__ uint32_t stage[kPassThreads / 32][kStageWords];
+    __shared__ __align__(16) uint32_t stage[kPassThreads / 32][kStageWords];
     __shared__ R vals[kPassThreads / 32][2 << kMaxChunkLog2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ncomp = 2 << C, per_lane = ncomp >> 5;
@@ -1024,7 +1041,7 @@ __global__ void encode_kernel(const double *vals, int B, int C, CodecParams p, u
 template <typename R>
 __global__ void codec_test_kernel(const R *vals, int C, CodecParams p, uint64_t nchunks, uint32_t *words,
                                   int32_t *bases, uint32_t *widths, R *decoded) {
-    __shared__ uint32_t stage[kPassThreads / 32][kStageWords];
+    __shared__ __align__(16) uint32_t stage[kPassThreads / 32][kStageWords];
     __shared__ R buf[kPassThreads / 32][2 << kMaxChunkLog2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ncomp = 2 << C, per_lane = ncomp >> 5;
@@ -1360,26 +1377,30 @@ int sm_count() {
     return g_sm_count;
 }
 
-template <typename R, int RB>
+template <typename R, int RB, bool kCodes>
 static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
     const int nb = a.C + a.j;
     const size_t smem = pass_smem_bytes(sizeof(R) == 8, nb, a.j);
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, RB, kCodes>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<R, RB>, kSweepThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<R, RB, kCodes>, kSweepThreads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t grid = (uint64_t)per_sm * sm_count();
     if (grid > a.n_tiles) grid = a.n_tiles;
     if (grid == 0) grid = 1;
-    pass_kernel<R, RB><<<(unsigned)grid, kSweepThreads, smem, s>>>(a);
+    pass_kernel<R, RB, kCodes><<<(unsigned)grid, kSweepThreads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pass(bool f64, const PassArgs &a, int, cudaStream_t s) {
     if (a.rb != kRegBits || a.C + a.j < kRegBits || a.diag.nterms > kMaxDiagTerms) return cudaErrorInvalidValue;
-    return f64 ? launch_pass_t<double, kRegBits>(a, s) : launch_pass_t<float, kRegBits>(a, s);
+    if (a.code_moves && a.diag.nterms) return cudaErrorInvalidValue;
+    if (a.code_moves)
+        return f64 ? launch_pass_t<double, kRegBits, true>(a, s) : launch_pass_t<float, kRegBits, true>(a, s);
+    return f64 ? launch_pass_t<double, kRegBits, false>(a, s) : launch_pass_t<float, kRegBits, false>(a, s);
 }
 
 cudaError_t launch_perm_pass(const PermPassArgs &a, cudaStream_t s) {

@@ -75,6 +75,7 @@ class qs_stats(ct.Structure):
         ("perm_passes", ct.c_uint64),
         ("perm_bytes", ct.c_uint64),
         ("perm_ms", ct.c_double),
+        ("code_move_passes", ct.c_uint64),
         ("arena_capacity", ct.c_uint64),
         ("host_store", ct.c_uint64),
     ]

@@ -110,6 +110,8 @@ typedef struct qs_stats {
                                     qubits >= chunk_log2, applied without decoding)     */
     uint64_t perm_bytes;         /* chunk-header bytes read + written by those passes   */
     double perm_ms;              /* their device time (QS_FLAG_PROFILE), else 0         */
+    uint64_t code_move_passes;   /* tile passes made only of X / SWAP moves, which carry the
+                                    quantised codes through the tile without dequantising */
     uint64_t arena_capacity;     /* bytes of each of the two payload arenas             */
     uint64_t host_store;         /* 1 when the arenas are in host memory (QS_FLAG_HOST_STORE) */
 } qs_stats;

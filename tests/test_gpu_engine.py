@@ -326,6 +326,25 @@ def test_compressed_export_import_roundtrip(qulacs_mod):
     with pytest.raises(_native.QompsimError) as e:
         other.import_store(blob[:-16])
     assert e.value.status == _native.QS_ERR_CORRUPT
+    # chunk headers of stored blocks: misaligned offset, offset past the
+    # arena, width above 32 -- each rejected before anything is launched
+    nb, nchunks = 1 << (14 - 8), 1 << (14 - 8)
+    meta0 = 56 + (nb + 7) // 8 * 8 + nb * 8
+    mask = np.frombuffer(blob, dtype=np.uint8, count=nb, offset=56)
+    k = int(np.flatnonzero(mask)[0]) * (nchunks // nb)
+    arena_bytes = int(np.frombuffer(blob, dtype=np.uint64, count=1, offset=48)[0])
+    for field, value in [("offset", 8), ("offset", arena_bytes + 128), ("width", 40)]:
+        bad = bytearray(blob)
+        pos = meta0 + 16 * k + (0 if field == "offset" else 12)
+        if field == "offset":
+            bad[pos:pos + 8] = int(value).to_bytes(8, "little")
+        else:
+            bad[pos:pos + 4] = int(value).to_bytes(4, "little")
+        with pytest.raises(_native.QompsimError) as e:
+            other.import_store(bytes(bad))
+        assert e.value.status == _native.QS_ERR_CORRUPT, field
+    other.import_store(blob)
+    assert np.array_equal(other.get_vector(renormalize=False), v)
 
 
 def test_compressed_error_paths(qulacs_mod, monkeypatch):
@@ -502,3 +521,45 @@ def test_host_store_bit_identical(qulacs_mod, dtype, circ):
     ref.set_zero_state()
     ref.import_store(blob)
     assert np.array_equal(v, ref.get_vector(renormalize=False))
+
+
+# ------------------------------------------------------------ code-domain moves
+def _moves_circuit(n, seed):
+    """Random gates, then blocks of SWAP / X gates alone (bit reversal, which
+    pairs chunk bits with high qubits, and X layers), then random gates."""
+    import qulacs
+    rng = np.random.default_rng(seed)
+    c = qulacs.QuantumCircuit(n)
+    for g in helpers.random_circuit(n, 40, seed)._gates:
+        c.add_gate(g)
+    for _ in range(2):
+        for q in range(n // 2):
+            c.add_SWAP_gate(q, n - 1 - q)
+        for q in rng.choice(n, size=3, replace=False):
+            c.add_X_gate(int(q))
+    for g in helpers.random_circuit(n, 20, seed + 1)._gates:
+        c.add_gate(g)
+    return c
+
+
+@pytest.mark.parametrize("dtype", ["complex128", "complex64"])
+@pytest.mark.parametrize("circ,exact", [("qft", False), ("moves", False), ("moves", True)])
+def test_code_move_passes_bit_identical(qulacs_mod, monkeypatch, dtype, circ, exact):
+    """Passes made only of X / SWAP moves carry quantised codes through the
+    tile; since quantise(dequantise(c)) == c the store decodes to exactly the
+    values of the value-domain pass, with the same masks and byte totals."""
+    from qulacs import _native
+    from qompsim import circuits as C
+    n, B = 16, 9
+    c = helpers.optimized(C.qft_basis(n, 5), B) if circ == "qft" else _moves_circuit(n, 7)
+    flags = _native.QS_FLAG_QUIET | (_native.QS_FLAG_EXACT_ZERO_TEST if exact else 0)
+    out = []
+    for on in ("1", "0"):
+        monkeypatch.setenv("QOMPSIM_CODE_MOVES", on)
+        cq = _compressed(qulacs_mod, c, B, 3, dtype=dtype, flags=flags)
+        out.append((cq.get_vector(renormalize=False), cq.get_zero_mask(), cq.get_SV_bytes_history(),
+                    cq.get_stats()["code_move_passes"]))
+    assert out[0][3] > 0 and out[1][3] == 0
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
