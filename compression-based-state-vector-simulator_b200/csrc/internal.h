@@ -11,6 +11,9 @@ namespace qs {
 
 // Largest chunk: 2^8 amplitudes = 512 real components = 16 per lane.
 constexpr int kMaxChunkLog2 = 8;
+// Arena space a pass-kernel CTA takes at once (when the arena holds at least
+// eight per CTA), sub-allocated to its tiles without the shared counter.
+constexpr uint64_t kArenaSlabBytes = 256 << 10;
 constexpr int kMinChunkLog2 = 4;
 constexpr int kMaxPerLane = (2 << kMaxChunkLog2) / 32;
 // Largest tile: 2^14 amplitudes; at most kMaxTileQubits qubits above the chunk.
@@ -141,6 +144,7 @@ struct PassArgs {
     uint32_t *arena_out;
     unsigned long long *bump;           // bytes used in arena_out
     uint64_t capacity;                  // bytes of arena_out
+    uint64_t slab;                      // > 0: CTAs take arena space in slabs of this many bytes
     const uint32_t *block_to_group;     // stage's map
     const uint8_t *group_active;
     const uint8_t *mask;                // zero-block mask at stage start

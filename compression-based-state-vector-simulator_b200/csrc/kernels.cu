@@ -16,6 +16,7 @@
 // and writes the packed chunks back with coalesced stores.
 #include <cstdio>
 #include <climits>
+#include <cstdlib>
 #include <mutex>
 
 #include "codec.cuh"
@@ -504,12 +505,16 @@ template <typename R, int RB, bool kCodes>
 __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ unsigned long long s_tile_off;
+    __shared__ unsigned long long s_tile_off, s_next, s_slab_end;
     __shared__ int s_flag;
     __shared__ int32_t s_tq[kMaxTileQubits];
     __shared__ int8_t s_oq[kMaxOuterSel];
     if (threadIdx.x < kMaxTileQubits) s_tq[threadIdx.x] = a.tq[threadIdx.x];
     if (threadIdx.x < kMaxOuterSel) s_oq[threadIdx.x] = a.outer_q[threadIdx.x];
+    if (threadIdx.x == 0) {
+        s_next = 0;
+        s_slab_end = 0;
+    }
     __syncthreads();
 
     const int C = a.C, j = a.j, nb = C + j;
@@ -624,14 +629,23 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
             }
             const unsigned long long total = __shfl_sync(0xffffffffu, incl, 31);
             if (lane == 0) {
-                const unsigned long long off = atomicAdd(a.bump, total);
-                if (off + total > a.capacity) {
-                    atomicExch(a.error, 1);
-                    s_flag = 1;
-                } else {
-                    s_flag = 0;
+                // the tile goes at the CTA's next free byte of its current
+                // slab; one that does not fit takes a new slab of a.slab
+                // bytes (or exactly its own size) from the arena, so most
+                // tiles reserve without touching the shared counter
+                unsigned long long off = s_next;
+                s_flag = 0;
+                if (a.slab == 0 || off + total > s_slab_end) {
+                    const unsigned long long want = total > a.slab ? total : a.slab;
+                    off = atomicAdd(a.bump, want);
+                    if (off + want > a.capacity) {
+                        atomicExch(a.error, 1);
+                        s_flag = 1;
+                    }
+                    s_slab_end = off + want;
                 }
                 s_tile_off = off;
+                s_next = off + total;
                 wr += total + (unsigned long long)nchunks * sizeof(ChunkMeta);
             }
         }
@@ -1391,7 +1405,12 @@ static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
     uint64_t grid = (uint64_t)per_sm * sm_count();
     if (grid > a.n_tiles) grid = a.n_tiles;
     if (grid == 0) grid = 1;
-    pass_kernel<R, RB, kCodes><<<(unsigned)grid, kSweepThreads, smem, s>>>(a);
+    // arena slabs per CTA when the arena can spare 8 of them per CTA
+    PassArgs b = a;
+    const char *env = std::getenv("QOMPSIM_SLAB_BYTES");
+    const uint64_t slab = env ? (uint64_t)std::strtoull(env, nullptr, 10) : (uint64_t)kArenaSlabBytes;
+    b.slab = (slab && a.capacity / grid >= 8 * slab) ? (slab + 127) / 128 * 128 : 0;
+    pass_kernel<R, RB, kCodes><<<(unsigned)grid, kSweepThreads, smem, s>>>(b);
     return cudaGetLastError();
 }
 

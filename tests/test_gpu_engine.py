@@ -563,3 +563,23 @@ def test_code_move_passes_bit_identical(qulacs_mod, monkeypatch, dtype, circ, ex
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
     assert out[0][2] == out[1][2]
+
+
+@pytest.mark.parametrize("dtype", ["complex128", "complex64"])
+def test_arena_slabs_same_store(qulacs_mod, monkeypatch, dtype):
+    """CTAs that sub-allocate arena slabs (forced small here) produce the same
+    decoded state, masks and byte totals as exact per-tile reservations; the
+    store round-trips through export / import with the slabs' slack."""
+    n, B = 16, 9
+    c = helpers.optimized(helpers.random_circuit(n, 150, seed=12), B)
+    out = []
+    for slab in ("1024", "0"):
+        monkeypatch.setenv("QOMPSIM_SLAB_BYTES", slab)
+        cq = _compressed(qulacs_mod, c, B, 3, dtype=dtype)
+        out.append((cq.get_vector(renormalize=False), cq.get_zero_mask(), cq.get_SV_bytes_history(), cq))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
+    blob = out[0][3].export_store()
+    out[1][3].import_store(blob)
+    assert np.array_equal(out[1][3].get_vector(renormalize=False), out[0][0])
