@@ -1078,7 +1078,9 @@ static void make_block_groups(qs_state *h) {
 static qs_status build_device_plan(qs_state *h) {
     const int C = (int)h->C;
     const int jmax = std::min(h->tile_log2 - C, qs::kMaxTileQubits);
-    const int jmin = std::min(jmax, std::max(3, qs::kRegBits - C));
+    // tiles are padded to the largest size: fewer tiles, each with its fixed
+    // costs (headers, reservation, barriers) spread over more chunks
+    const int jmin = std::min(jmax, std::max(env_int("QOMPSIM_TILE_MIN_QUBITS", jmax), qs::kRegBits - C));
     std::vector<qs::KGate> kg;
     std::vector<qs::Sweep> sw;
     std::vector<qs::ROp> ops;

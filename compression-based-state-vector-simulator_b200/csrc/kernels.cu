@@ -347,32 +347,36 @@ __device__ __forceinline__ int32_t value_as_code(double v) { return (int32_t)__d
 // chunk can use, so that the look-ahead word of the last row stays inside.
 constexpr int kStageWords = (kMaxPerLane + 1) * 32;
 
+// Start the asynchronous copy of a chunk's payload (rows x 128 contiguous
+// bytes, 128-byte aligned) into a warp's staging buffer: 16-byte cp.async
+// copies, no registers, one commit group per call (empty for width 0).
+__device__ __forceinline__ void issue_payload(const uint32_t *__restrict__ arena, const ChunkMeta md, int per_lane,
+                                              uint32_t *dst, int lane) {
+    const int rows = (int)(((uint32_t)per_lane * md.width + 31) >> 5);
+    const uint32_t sdst = (uint32_t)__cvta_generic_to_shared(dst);
+    const char *gsrc = reinterpret_cast<const char *>(arena + (md.offset >> 2));
+    for (int off = lane * 16; off < rows * 128; off += 32 * 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sdst + off), "l"(gsrc + off) : "memory");
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Unpack a chunk whose payload is in the warp's staging buffer (the copy
+// complete and visible to the warp): every element is extracted on its own
+// (one funnel shift); a lane reads only its own words.
 template <typename R, typename Slot = LinearSlot, bool kCodes = false>
-__device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena, const ChunkMeta md,
-                                             int per_lane, CodecParams p, R *comp, uint32_t *wstage,
-                                             int lane, Slot slot = Slot()) {
+__device__ __forceinline__ void unpack_chunk(const ChunkMeta md, int per_lane, CodecParams p, R *comp,
+                                             const uint32_t *wstage, int lane, Slot slot = Slot()) {
     const uint32_t w = md.width;
     if (w == 0) {
         const R v = kCodes ? code_as_value(md.base, R()) : dequantize_hot(md.base, p, R());
         for (int i = 0; i < per_lane; ++i) comp[slot(lane + 32 * i)] = v;
         return;
     }
-    const int rows = (int)(((uint32_t)per_lane * w + 31) >> 5);
-    const uint32_t *src = arena + (md.offset >> 2);
-    // the payload (rows x 128 contiguous bytes, 128-byte aligned) into the
-    // warp's staging with asynchronous 16-byte copies: no registers, one
-    // round trip to memory for the whole chunk
-    {
-        const uint32_t sdst = (uint32_t)__cvta_generic_to_shared(wstage);
-        const char *gsrc = reinterpret_cast<const char *>(src);
-        for (int off = lane * 16; off < rows * 128; off += 32 * 16)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sdst + off), "l"(gsrc + off) : "memory");
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        __syncwarp();
-    }
-    // element i of this lane's stream starts at bit i*w: every element is
-    // extracted independently (one funnel shift); a lane reads only its own words
     const uint32_t mask = (w >= 32) ? 0xffffffffu : ((1u << w) - 1u);
 #pragma unroll
     for (int i = 0; i < kMaxPerLane; ++i) {
@@ -383,6 +387,20 @@ __device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena,
             comp[slot(lane + 32 * i)] = kCodes ? code_as_value(code, R()) : dequantize_hot(code, p, R());
         }
     }
+}
+
+// Per-warp decode of one chunk: copy its payload into the warp's staging
+// area (one round trip to memory), then unpack it.
+template <typename R, typename Slot = LinearSlot, bool kCodes = false>
+__device__ __forceinline__ void decode_chunk(const uint32_t *__restrict__ arena, const ChunkMeta md,
+                                             int per_lane, CodecParams p, R *comp, uint32_t *wstage,
+                                             int lane, Slot slot = Slot()) {
+    if (md.width != 0) {
+        issue_payload(arena, md, per_lane, wstage, lane);
+        cp_async_wait<0>();
+        __syncwarp();
+    }
+    unpack_chunk<R, Slot, kCodes>(md, per_lane, p, comp, wstage, lane, slot);
 }
 
 // Per-warp quantisation of one chunk held in comp[]: codes overwrite the
@@ -462,7 +480,8 @@ size_t pass_smem_bytes(bool f64, int nb, int j) {
     const size_t stage = (size_t)(kSweepThreads / 32) * kStageWords * 4;
     const size_t tables = ((size_t)3 * 4 << j) + 8;
     const size_t offs = (size_t)8 << j;
-    return tile + stage + ((tables + 7) / 8) * 8 + offs;
+    const size_t headers = sizeof(ChunkMeta) << j;
+    return tile + stage + ((tables + 7) / 8) * 8 + offs + headers;
 }
 
 // ------------------------------------------------------------ diagonal Pauli sum
@@ -496,6 +515,14 @@ __device__ void tile_diag_sum(typename Cplx<R>::T *tile, int nb, int swm, const 
 
 static_assert((kSweepThreads / 32) * kStageWords * 4 >= 2 * kMaxDiagTerms * sizeof(double),
               "the pass kernel's decode staging holds the diagonal-sum coefficients");
+
+// ------------------------------------------------------------ pass kernel
+// Whether a warp loads all its chunk headers at once and copies its next
+// chunk's payload while it unpacks the current one (complex128, measured
+// faster there), or loads headers four at a time and copies each payload
+// just before unpacking it (complex64, measured faster there).
+template <typename R>
+constexpr bool kPrefetchDecode = sizeof(R) == 8;
 
 // ------------------------------------------------------------ pass kernel
 // kCodes: every op of the pass only moves amplitudes (X / SWAP register
@@ -533,6 +560,7 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
     uint32_t *s_nz = s_width + nchunks;
     unsigned long long *s_off = reinterpret_cast<unsigned long long *>(
         reinterpret_cast<unsigned char *>(s_base) + ((((size_t)3 * 4 << j) + 8 + 7) / 8) * 8);
+    ChunkMeta *s_md = reinterpret_cast<ChunkMeta *>(s_off + nchunks);
 
     unsigned long long rd = 0, wr = 0, ntiles = 0;
 
@@ -545,40 +573,81 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
         if (s_flag) break;
         ++ntiles;
 
-        // ---- decode: the headers of HB of the warp's chunks are loaded
-        // together, then the chunks are unpacked one by one (complex64 takes
-        // four at a time; complex128 one, its register budget being tighter)
-        constexpr int HB = sizeof(R) == 4 ? 4 : 1;
-        for (int c0 = warp; c0 < nchunks; c0 += HB * nwarps) {
-            ChunkMeta md[HB];
-            bool zero[HB];
+        if constexpr (!kPrefetchDecode<R>) {
+            // ---- decode: the headers of four of the warp's chunks are
+            // loaded together, then the chunks are unpacked one by one
+            constexpr int HB = 4;
+            for (int c0 = warp; c0 < nchunks; c0 += HB * nwarps) {
+                ChunkMeta md[HB];
+                bool zero[HB];
 #pragma unroll
-            for (int b = 0; b < HB; ++b) {
-                const int c = c0 + b * nwarps;
-                md[b].offset = 0;
-                md[b].base = 0;
-                md[b].width = 0;
-                zero[b] = true;
-                if (c < nchunks) {
-                    const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
-                    if (!a.first_pass || a.mask[chunk >> blk_shift]) {
-                        md[b] = a.meta_in[chunk];
-                        zero[b] = false;
+                for (int b = 0; b < HB; ++b) {
+                    const int c = c0 + b * nwarps;
+                    md[b] = ChunkMeta{0, 0, 0};
+                    zero[b] = true;
+                    if (c < nchunks) {
+                        const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
+                        if (!a.first_pass || a.mask[chunk >> blk_shift]) {
+                            md[b] = a.meta_in[chunk];
+                            zero[b] = false;
+                        }
                     }
                 }
-            }
 #pragma unroll
-            for (int b = 0; b < HB; ++b) {
-                const int c = c0 + b * nwarps;
-                if (c >= nchunks) break;
-                R *comp = reinterpret_cast<R *>(tile) + (size_t)c * ncomp;
-                if (zero[b]) {
-                    for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = R(0);
-                    continue;
+                for (int b = 0; b < HB; ++b) {
+                    const int c = c0 + b * nwarps;
+                    if (c >= nchunks) break;
+                    R *comp = reinterpret_cast<R *>(tile) + (size_t)c * ncomp;
+                    if (zero[b]) {
+                        for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = R(0);
+                        continue;
+                    }
+                    decode_chunk<R, TileSlot<R>, kCodes>(a.arena_in, md[b], per_lane, a.codec,
+                                                         reinterpret_cast<R *>(tile), wstage, lane,
+                                                         TileSlot<R>{c << C, swm});
+                    if (lane == 0) rd += payload_bytes(C, md[b].width) + sizeof(ChunkMeta);
                 }
-                decode_chunk<R, TileSlot<R>, kCodes>(a.arena_in, md[b], per_lane, a.codec,
-                                                     reinterpret_cast<R *>(tile), wstage, lane, TileSlot<R>{c << C, swm});
-                if (lane == 0) rd += payload_bytes(C, md[b].width) + sizeof(ChunkMeta);
+            }
+        } else {
+            // ---- decode.  A warp's lanes load the headers of all of the
+            // warp's chunks at once (a chunk of a zero block reads as width 0,
+            // base 0: zeros).  The warp then walks its chunks and copies the
+            // next chunk's payload with cp.async while it unpacks the current
+            // one; the two payload buffers are the warp's staging area and
+            // the tile region of the warp's last chunk, which nothing uses
+            // until that chunk is unpacked.
+            for (int c = warp + lane * nwarps; c < nchunks; c += 32 * nwarps) {
+                ChunkMeta md{0, 0, 0};
+                const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
+                if (!a.first_pass || a.mask[chunk >> blk_shift]) {
+                    md = a.meta_in[chunk];
+                    rd += payload_bytes(C, md.width) + sizeof(ChunkMeta);
+                }
+                s_md[c] = md;
+            }
+            __syncwarp();
+            const int m = warp < nchunks ? (nchunks - warp + nwarps - 1) / nwarps : 0;
+            if (m > 0) {
+                uint32_t *bufR = reinterpret_cast<uint32_t *>(reinterpret_cast<R *>(tile) +
+                                                              (size_t)(warp + (m - 1) * nwarps) * ncomp);
+                issue_payload(a.arena_in, s_md[warp], per_lane, wstage, lane);
+                for (int i = 0; i < m; ++i) {
+                    const int c = warp + i * nwarps;
+                    uint32_t *cur = (i < m - 1 && (i & 1)) ? bufR : wstage;
+                    uint32_t *nxt = (i + 1 < m - 1 && ((i + 1) & 1)) ? bufR : wstage;
+                    const bool pre = i + 1 < m && nxt != cur;
+                    if (pre) {
+                        issue_payload(a.arena_in, s_md[c + nwarps], per_lane, nxt, lane);
+                        cp_async_wait<1>();
+                    } else {
+                        cp_async_wait<0>();
+                    }
+                    __syncwarp();
+                    unpack_chunk<R, TileSlot<R>, kCodes>(s_md[c], per_lane, a.codec, reinterpret_cast<R *>(tile), cur,
+                                                         lane, TileSlot<R>{c << C, swm});
+                    __syncwarp();
+                    if (i + 1 < m && !pre) issue_payload(a.arena_in, s_md[c + nwarps], per_lane, nxt, lane);
+                }
             }
         }
         __syncthreads();
@@ -674,7 +743,7 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
         }
         __syncthreads();
     }
-    if (lane == 0 && rd) atomicAdd(&a.stats[0], rd);
+    if (rd) atomicAdd(&a.stats[0], rd);
     if (threadIdx.x == 0) {
         if (wr) atomicAdd(&a.stats[1], wr);
         if (ntiles) atomicAdd(&a.stats[2], ntiles);
