@@ -1432,6 +1432,9 @@ qs_status qs_apply_circuit(qs_state *h) {
             a.final_pass = dp.final;
             a.exact_zero = (h->flags & QS_FLAG_EXACT_ZERO_TEST) ? 1 : 0;
             a.code_moves = dp.code_moves ? 1 : 0;
+            // complex64: passes of several sweeps measured faster with eight
+            // headers per batch, single-sweep (codec-bound) passes with four
+            a.header_batch = (!h->f64 && dp.nsweeps >= 2) ? 8 : 4;
             a.block_nz = h->block_nz;
             a.block_bytes = h->block_acc;
             a.error = h->error_dev;
@@ -1471,11 +1474,18 @@ qs_status qs_apply_circuit(qs_state *h) {
         perm_passes += h->passes[p].kind == 1 ? 1 : 0;
         code_passes += (h->passes[p].kind == 0 && h->passes[p].code_moves) ? 1 : 0;
     }
+    const bool print_passes = std::getenv("QOMPSIM_DEBUG_PASS_MS") != nullptr;
     for (size_t p = 0; p < h->pass_ev.size() / 2; ++p) {
         float t = 0;
         CUDA_TRY(h, cudaEventElapsedTime(&t, h->pass_ev[2 * p], h->pass_ev[2 * p + 1]));
         (h->passes[p].kind == 1 ? perm_ms : pass_ms) += t;
+        if (print_passes) {
+            const auto &dp = h->passes[p];
+            printf("pass %zu stage %u kind %d j %d gates %u sweeps %u codes %d ms %.3f\n", p, dp.stage, dp.kind, dp.j,
+                   dp.ngates, dp.nsweeps, dp.code_moves ? 1 : 0, t);
+        }
     }
+    if (print_passes) fflush(stdout);
     h->times[1] += ms / 1000.0;
     h->st.stages = h->stages.size();
     h->st.passes = h->passes.size();
@@ -1945,6 +1955,7 @@ qs_status qs_apply_diagonal_pauli_sum(qs_state *out, const qs_state *in, const u
         return fail(out, QS_ERR_CUDA, std::string("diagonal Pauli sum: ") + cudaGetErrorString(e));
     }
     qs::PassArgs a{};
+    a.header_batch = 4;
     a.n = (int)out->n;
     a.B = (int)out->B;
     a.C = C;

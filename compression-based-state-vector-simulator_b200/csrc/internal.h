@@ -151,6 +151,7 @@ struct PassArgs {
     int32_t first_pass, final_pass, exact_zero;
     int32_t code_moves;                 // 1: every op is an X / SWAP register move (no arithmetic),
                                         // so the tile carries quantised codes, not values
+    int32_t header_batch;               // complex64: chunk headers a warp loads at once (4 or 8)
     uint32_t *block_nz;                 // final pass: any non-zero in block
     unsigned long long *block_bytes;    // final pass: stored bytes of block
     int32_t *error;                     // 1 = arena overflow

@@ -528,7 +528,8 @@ constexpr bool kPrefetchDecode = sizeof(R) == 8;
 // kCodes: every op of the pass only moves amplitudes (X / SWAP register
 // moves, chunk permutations), so the tile holds the quantised codes
 // themselves and the pass skips dequantisation and quantisation.
-template <typename R, int RB, bool kCodes>
+// kHB: complex64 chunk headers loaded per warp batch (4 or 8).
+template <typename R, int RB, bool kCodes, int kHB>
 __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -574,9 +575,9 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
         ++ntiles;
 
         if constexpr (!kPrefetchDecode<R>) {
-            // ---- decode: the headers of four of the warp's chunks are
+            // ---- decode: the headers of kHB of the warp's chunks are
             // loaded together, then the chunks are unpacked one by one
-            constexpr int HB = 4;
+            constexpr int HB = kHB;
             for (int c0 = warp; c0 < nchunks; c0 += HB * nwarps) {
                 ChunkMeta md[HB];
                 bool zero[HB];
@@ -1460,15 +1461,15 @@ int sm_count() {
     return g_sm_count;
 }
 
-template <typename R, int RB, bool kCodes>
+template <typename R, int RB, bool kCodes, int kHB>
 static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
     const int nb = a.C + a.j;
     const size_t smem = pass_smem_bytes(sizeof(R) == 8, nb, a.j);
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, RB, kCodes>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, RB, kCodes, kHB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<R, RB, kCodes>, kSweepThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<R, RB, kCodes, kHB>, kSweepThreads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t grid = (uint64_t)per_sm * sm_count();
@@ -1479,16 +1480,21 @@ static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
     const char *env = std::getenv("QOMPSIM_SLAB_BYTES");
     const uint64_t slab = env ? (uint64_t)std::strtoull(env, nullptr, 10) : (uint64_t)kArenaSlabBytes;
     b.slab = (slab && a.capacity / grid >= 8 * slab) ? (slab + 127) / 128 * 128 : 0;
-    pass_kernel<R, RB, kCodes><<<(unsigned)grid, kSweepThreads, smem, s>>>(b);
+    pass_kernel<R, RB, kCodes, kHB><<<(unsigned)grid, kSweepThreads, smem, s>>>(b);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pass(bool f64, const PassArgs &a, int, cudaStream_t s) {
     if (a.rb != kRegBits || a.C + a.j < kRegBits || a.diag.nterms > kMaxDiagTerms) return cudaErrorInvalidValue;
     if (a.code_moves && a.diag.nterms) return cudaErrorInvalidValue;
+    if (a.header_batch != 4 && a.header_batch != 8) return cudaErrorInvalidValue;
+    if (f64)
+        return a.code_moves ? launch_pass_t<double, kRegBits, true, 4>(a, s) : launch_pass_t<double, kRegBits, false, 4>(a, s);
     if (a.code_moves)
-        return f64 ? launch_pass_t<double, kRegBits, true>(a, s) : launch_pass_t<float, kRegBits, true>(a, s);
-    return f64 ? launch_pass_t<double, kRegBits, false>(a, s) : launch_pass_t<float, kRegBits, false>(a, s);
+        return a.header_batch == 8 ? launch_pass_t<float, kRegBits, true, 8>(a, s)
+                                   : launch_pass_t<float, kRegBits, true, 4>(a, s);
+    return a.header_batch == 8 ? launch_pass_t<float, kRegBits, false, 8>(a, s)
+                               : launch_pass_t<float, kRegBits, false, 4>(a, s);
 }
 
 cudaError_t launch_perm_pass(const PermPassArgs &a, cudaStream_t s) {
