@@ -2627,25 +2627,35 @@ qs_status qs_dense_adjoint(qs_dense *psi, qs_dense *lam, const qs_gate *gates, c
     std::vector<uint32_t> ids(count);
     for (size_t i = 0; i < count; ++i) ids[i] = (uint32_t)i;
     auto pl = plan_passes(ids, cg, C, jmax, std::min(jmax, 3), C, n);
-    std::vector<double> acc(2 * (size_t)nslots, 0.0);
-    double *dout = nullptr;
-    qs::AdjGate *dg = nullptr;
-    cudaError_t e = cudaSuccess;
+    // every launch's gate records (at most 128 parametric gates each) are
+    // built first and uploaded at once; the launches then run back to back
+    // and their slot sums are read back with one copy at the end
+    struct Launch {
+        int j;
+        int32_t tq[qs::kMaxTileQubits];
+        size_t gate_off, ngates, out_off;
+        std::vector<int32_t> local_to_global;
+    };
+    std::vector<qs::AdjGate> ag;
+    std::vector<Launch> launches;
+    size_t nout = 0;
     for (auto &p : pl) {
-        // local slots of this pass (at most 128)
-        for (size_t g0 = 0; g0 < p.gates.size() && e == cudaSuccess;) {
-            std::vector<qs::AdjGate> ag;
-            std::vector<int32_t> local_to_global;
+        for (size_t g0 = 0; g0 < p.gates.size();) {
+            Launch L{};
+            L.j = (int)p.tile.size();
+            for (int k = 0; k < L.j; ++k) L.tq[k] = p.tile[k] - C;
+            L.gate_off = ag.size();
+            L.out_off = nout;
             size_t g1 = g0;
             for (; g1 < p.gates.size(); ++g1) {
                 const uint32_t gi = p.gates[g1];
-                if (slots[gi] >= 0 && local_to_global.size() >= 128) break;
+                if (slots[gi] >= 0 && L.local_to_global.size() >= 128) break;
                 qs::AdjGate a{};
                 a.g = to_kgate(cg[gi], p.tile, C);
                 a.slot = -1;
                 if (slots[gi] >= 0) {
-                    a.slot = (int32_t)local_to_global.size();
-                    local_to_global.push_back(slots[gi]);
+                    a.slot = (int32_t)L.local_to_global.size();
+                    L.local_to_global.push_back(slots[gi]);
                     uint32_t xt = 0, zt = 0;
                     uint64_t zo = 0;
                     for (int q = 0; q < n; ++q) {
@@ -2666,43 +2676,46 @@ qs_status qs_dense_adjoint(qs_dense *psi, qs_dense *lam, const qs_gate *gates, c
                 }
                 ag.push_back(a);
             }
-            const size_t ns = local_to_global.size();
-            if (dg) cudaFree(dg);
-            if (dout) cudaFree(dout);
-            dg = nullptr;
-            dout = nullptr;
-            e = cudaMalloc(&dg, std::max<size_t>(1, ag.size()) * sizeof(qs::AdjGate));
-            if (e == cudaSuccess) e = cudaMalloc(&dout, std::max<size_t>(1, 2 * ns) * sizeof(double));
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(dg, ag.data(), ag.size() * sizeof(qs::AdjGate), cudaMemcpyHostToDevice, psi->stream);
-            if (e == cudaSuccess) e = cudaMemsetAsync(dout, 0, std::max<size_t>(1, 2 * ns) * sizeof(double), psi->stream);
-            if (e == cudaSuccess) {
-                qs::AdjPassArgs a{};
-                a.n = n;
-                a.C = C;
-                a.j = (int)p.tile.size();
-                for (int k = 0; k < a.j; ++k) a.tq[k] = p.tile[k] - C;
-                a.n_tiles = uint64_t(1) << (n - C - a.j);
-                a.gates = dg;
-                a.ngates = (int)ag.size();
-                a.psi = psi->state;
-                a.lam = lam->state;
-                a.out = dout;
-                a.nslots = (int)ns;
-                e = qs::launch_adjoint_pass(psi->f64, a, psi->stream);
-            }
-            std::vector<double> h(2 * ns);
-            if (e == cudaSuccess && ns)
-                e = cudaMemcpyAsync(h.data(), dout, 2 * ns * sizeof(double), cudaMemcpyDeviceToHost, psi->stream);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(psi->stream);
-            if (e == cudaSuccess)
-                for (size_t k = 0; k < ns; ++k) {
-                    acc[2 * local_to_global[k]] += h[2 * k];
-                    acc[2 * local_to_global[k] + 1] += h[2 * k + 1];
-                }
+            L.ngates = ag.size() - L.gate_off;
+            nout += L.local_to_global.size();
+            launches.push_back(std::move(L));
             g0 = g1;
         }
     }
+    std::vector<double> acc(2 * (size_t)nslots, 0.0);
+    double *dout = nullptr;
+    qs::AdjGate *dg = nullptr;
+    cudaError_t e = cudaMalloc(&dg, std::max<size_t>(1, ag.size()) * sizeof(qs::AdjGate));
+    if (e == cudaSuccess) e = cudaMalloc(&dout, std::max<size_t>(1, 2 * nout) * sizeof(double));
+    if (e == cudaSuccess && !ag.empty())
+        e = cudaMemcpyAsync(dg, ag.data(), ag.size() * sizeof(qs::AdjGate), cudaMemcpyHostToDevice, psi->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dout, 0, std::max<size_t>(1, 2 * nout) * sizeof(double), psi->stream);
+    for (const Launch &L : launches) {
+        if (e != cudaSuccess) break;
+        qs::AdjPassArgs a{};
+        a.n = n;
+        a.C = C;
+        a.j = L.j;
+        for (int k = 0; k < L.j; ++k) a.tq[k] = L.tq[k];
+        a.n_tiles = uint64_t(1) << (n - C - L.j);
+        a.gates = dg + L.gate_off;
+        a.ngates = (int)L.ngates;
+        a.psi = psi->state;
+        a.lam = lam->state;
+        a.out = dout + 2 * L.out_off;
+        a.nslots = (int)L.local_to_global.size();
+        e = qs::launch_adjoint_pass(psi->f64, a, psi->stream);
+    }
+    std::vector<double> h(2 * nout);
+    if (e == cudaSuccess && nout)
+        e = cudaMemcpyAsync(h.data(), dout, 2 * nout * sizeof(double), cudaMemcpyDeviceToHost, psi->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(psi->stream);
+    if (e == cudaSuccess)
+        for (const Launch &L : launches)
+            for (size_t k = 0; k < L.local_to_global.size(); ++k) {
+                acc[2 * L.local_to_global[k]] += h[2 * (L.out_off + k)];
+                acc[2 * L.local_to_global[k] + 1] += h[2 * (L.out_off + k) + 1];
+            }
     if (dg) cudaFree(dg);
     if (dout) cudaFree(dout);
     if (e != cudaSuccess) return dfail(psi, QS_ERR_CUDA, std::string("adjoint: ") + cudaGetErrorString(e));
