@@ -1,0 +1,83 @@
+"""Host logic of the engine on the CPU (tests/engine_host_check.cpp, built
+with engine.cpp by the host compiler; no GPU):
+
+* imported stores: chunk headers of stored blocks are checked before any
+  upload (misaligned offsets, widths above 32 and payloads past the arena are
+  rejected; headers of unstored blocks are never read and are ignored);
+* the planner: the QFT's bit-reversal SWAPs between chunk bits and outer
+  qubits become code-domain passes while the QFT's own passes carry values,
+  and every tile is padded to the largest tile of its precision when the
+  block has the qubits for it.
+"""
+import os
+import shutil
+import struct
+import subprocess
+
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(ROOT, "compression-based-state-vector-simulator_b200", "csrc")
+CUDA = "/usr/local/cuda"
+
+
+@pytest.fixture(scope="module")
+def checker(tmp_path_factory):
+    gxx = shutil.which("g++")
+    if gxx is None or not os.path.isdir(os.path.join(CUDA, "include")):
+        pytest.skip("no host C++ compiler or CUDA headers")
+    exe = tmp_path_factory.mktemp("engine") / "engine_host_check"
+    cmd = [gxx, "-O1", "-std=c++17", "-w", "-pthread", "-I", CSRC, "-I", os.path.join(CUDA, "include"),
+           "-o", str(exe), os.path.join(HERE, "engine_host_check.cpp"), "-L", os.path.join(CUDA, "lib64"),
+           "-lcudart", "-Wl,--unresolved-symbols=ignore-all", "-Wl,-rpath," + os.path.join(CUDA, "lib64")]
+    env = dict(os.environ)
+    env.pop("CXX", None)
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    assert r.returncode == 0, r.stderr[-3000:]
+    return str(exe)
+
+
+def test_store_header_check(checker):
+    r = subprocess.run([checker, "headers"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "0 failures" in r.stdout, r.stdout + r.stderr
+
+
+def _plan(checker, tmp_path, circuit, n, B, I, f64):
+    import ctypes as ct
+    from qulacs import _native
+    from qulacs.circuit import QuantumCircuitOptimizer
+    QuantumCircuitOptimizer(sv_block_size=B).optimize(circuit, block_size=2)
+    arr = _native.make_gate_array(circuit._gates)
+    path = tmp_path / "gates.bin"
+    with open(path, "wb") as f:
+        f.write(struct.pack("<Q", len(circuit._gates)))
+        f.write(ct.string_at(ct.addressof(arr), ct.sizeof(_native.qs_gate) * len(circuit._gates)))
+    r = subprocess.run([checker, "plan", str(path), str(n), str(B), str(I), "1" if f64 else "0"],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    passes = []
+    for line in r.stdout.splitlines():
+        if line.startswith("pass kind"):
+            t = line.split()
+            passes.append(dict(kind=int(t[2]), j=int(t[4]), codes=int(t[6]), jmax=int(t[8])))
+    return passes
+
+
+@pytest.mark.parametrize("f64", [True, False])
+def test_plan_code_domain_and_header_passes(checker, tmp_path, f64):
+    from qompsim import circuits as C
+    passes = _plan(checker, tmp_path, C.qft_basis(16, 5), 16, 9, 3, f64)
+    assert passes
+    assert any(p["kind"] == 0 and p["codes"] for p in passes)      # chunk bit <-> outer qubit SWAPs
+    assert not all(p["codes"] for p in passes if p["kind"] == 0)   # the QFT's own passes carry values
+
+
+@pytest.mark.parametrize("f64", [True, False])
+def test_plan_tiles_padded_to_largest(checker, tmp_path, f64):
+    import helpers
+    passes = _plan(checker, tmp_path, helpers.random_circuit(16, 80, seed=3), 16, 14, 3, f64)
+    tiles = [p for p in passes if p["kind"] == 0]
+    assert tiles
+    assert all(p["j"] == p["jmax"] for p in tiles), tiles
+    assert tiles[0]["jmax"] == (4 if f64 else 5)
