@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -58,6 +59,13 @@ def build_circuit(spec):
 def describe(spec) -> str:
     return (f"{spec['name']}: n={spec['n']} {spec['dtype']} compressed, block_size={spec['block_size']}, "
             f"inner_size={spec['inner_size']}, eps_rel={spec['eps_rel']}, eps_abs={spec['eps_abs']}")
+
+
+def config_of(spec, updates: int) -> dict:
+    """The workload fields both arms print (identical on the two lines)."""
+    return {"workload": describe(spec), "n": spec["n"], "block_size": spec["block_size"],
+            "inner_size": spec["inner_size"], "eps_rel": spec["eps_rel"], "eps_abs": spec["eps_abs"],
+            "amp_gate_updates_per_step": int(updates)}
 
 
 def measured_peaks():
@@ -167,41 +175,137 @@ def aggregate(pg, torch, local_ms: float, updates_per_step: int, steps: int, wor
     return ms, world * updates_per_step * steps / (ms * 1e-3)
 
 
-# ----------------------------------------------------------------- CPU baseline
-def cpu_sample(spec, budget_s: float = 12.0):
-    """The reference's csim FP64 kernels (oracle/_ref) applying the fused
-    gate list uncompressed on the host cores, on a bounded sample: the first
-    gates of the same QFT construction on a smaller register (2^ncpu
-    amplitudes), timed until ~budget_s.  Returns (updates/s, cores, sample)."""
+# ----------------------------------------------------------------- CPU baseline / reference arm
+def workload_updates(gates, n, B, I):
+    """Amplitude-gate updates of one apply of `gates`, counted as the
+    compressed engine counts them: sum over stages of (gates in the stage) x
+    (amplitudes of the stage's active groups), with the reference's stage plan
+    (partition_circuit / make_block_groups, compressed_state.hpp:509-671) and
+    its active-group and stored-block rules (:791-837, Q1: a stored block
+    stays stored).  Which blocks hold amplitude is propagated block by block
+    through each gate (a block reaches another through any non-zero matrix
+    entry between their global-qubit patterns).  The count is exact when a
+    gate's effect on a block's support does not depend on which local
+    amplitudes the block holds -- the QFT workloads (checked against the
+    engine's device count) -- and can over-count otherwise (a GHZ fan-out,
+    whose CNOTs move only the amplitudes with control 1).  Host-only (oracle
+    planner)."""
     import numpy as np
-    from oracle import csim_ref
-    from qompsim import circuits as C
-    from qulacs.circuit import QuantumCircuitOptimizer
+    from oracle import pipeline, planner
+    desc = planner.describe(gates)
+    stages = planner.partition_circuit(desc, B, I)
+    maps, counts = planner.make_block_groups(desc, stages, n, B)
+    nb = 1 << (n - B)
+    idx = np.arange(nb, dtype=np.int64)
+    support = np.zeros(nb, dtype=bool)
+    support[0] = True
+    stored = support.copy()
+    total = 0
+    for si, stage in enumerate(stages):
+        gmap = np.asarray(maps[si], dtype=np.int64)
+        active_groups = np.zeros(counts[si], dtype=bool)
+        active_groups[gmap[stored]] = True
+        in_active = active_groups[gmap]
+        total += len(stage) * int(in_active.sum()) << B
+        for gi in stage:
+            m, qs = pipeline._full_matrix(gates[gi])
+            gpos = [i for i, q in enumerate(qs) if q >= B]
+            if not gpos:
+                continue
+            gbits = [qs[i] - B for i in gpos]
+            gmask = sum(1 << b for b in gbits)
+            k = len(qs)
+            ng = 1 << len(gpos)
 
+            def gpat(x):  # pattern of matrix index x on the gate's global qubits
+                return sum(((x >> p) & 1) << j for j, p in enumerate(gpos))
+            reach = np.zeros((ng, ng), dtype=bool)
+            nzr, nzc = np.nonzero(np.abs(m) > 0)
+            for r, c in zip(nzr, nzc):
+                reach[gpat(int(r)), gpat(int(c))] = True
+            pat = np.zeros(nb, dtype=np.int64)
+            for j, b in enumerate(gbits):
+                pat |= ((idx >> b) & 1) << j
+            base = idx & ~gmask
+            new = np.zeros(nb, dtype=bool)
+            for gf in range(ng):
+                dep = sum(((gf >> j) & 1) << b for j, b in enumerate(gbits))
+                new |= reach[pat, gf] & support[base | dep]
+            support = new
+        stored |= support & in_active
+    return total
+
+
+def _host_memory_bytes() -> int:
     try:
-        mem = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
+        return os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
     except (ValueError, OSError):
-        mem = 0
-    ncpu = 28 if mem >= (64 << 30) else 24
-    c = C.qft_basis(ncpu, seed=0)
-    QuantumCircuitOptimizer(sv_block_size=spec["block_size"]).optimize(c, block_size=2)
-    state = csim_ref.zero_state(ncpu)
-    t0 = time.perf_counter()
-    done = 0
-    for g in c._gates:
-        csim_ref.apply_gate(state, g)
-        done += 1
-        if time.perf_counter() - t0 > budget_s:
-            break
-    dt = time.perf_counter() - t0
-    rate = done * float(1 << ncpu) / dt
+        return 0
+
+
+def reference_setup(spec):
+    """The workload's fused gate list and its update count (the numerator
+    both arms divide by their time)."""
+    gates = list(build_circuit(spec)._gates)
+    return gates, workload_updates(gates, spec["n"], spec["block_size"], spec["inner_size"])
+
+
+def csim_slices(state, gates, parts):
+    """Apply each contiguous run of gate indices in `parts` to `state` with
+    the reference's csim kernels; returns the seconds of each run."""
+    from oracle import csim_ref
+    times = []
+    for run in parts:
+        t0 = time.perf_counter()
+        for i in run:
+            csim_ref.apply_gate(state, gates[int(i)])
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def sample_runs(ngates: int, nslices: int, frac: float):
+    """A stratified sample of the gate list: the list cut into `nslices`
+    contiguous slices, and of each slice its first ceil(frac * len) gates."""
+    import numpy as np
+    parts = np.array_split(np.arange(ngates), max(1, nslices))
+    return [p[:max(1, math.ceil(frac * len(p)))] for p in parts if len(p)]
+
+
+def cpu_slice(spec, gates, updates):
+    """CPU baseline inside our arm: the reference's csim FP64 kernels
+    (oracle/_ref) apply a contiguous run of the workload's fused gate list
+    -- the first half of its middle twentieth -- to a 2^n state,
+    uncompressed, on all host cores (10-30 s of CPU work).  csim's time per
+    gate does not depend on the amplitudes, so the value is the run's share
+    of the workload's updates over its time.  Returns (updates/s, cores,
+    sample), or None without host memory for the state."""
+    from oracle import csim_ref
+    n = spec["n"]
+    if _host_memory_bytes() < (16 << n) + (4 << 30):
+        return None
+    state = csim_ref.zero_state(n)
+    run = sample_runs(len(gates), 20, 0.5)[10]
+    dt = csim_slices(state, gates, [run])[0]
     cores = csim_ref.max_threads()
-    sample = (f"csim FP64 uncompressed (reference kernels, OpenMP {cores} threads): first {done} of "
-              f"{len(c._gates)} fused gates of QFT n={ncpu} on 2^{ncpu} amplitudes, {dt:.1f} s")
+    rate = updates * (len(run) / len(gates)) / dt
+    sample = (f"csim FP64 uncompressed (reference kernels, OpenMP {cores} threads): gates {int(run[0])}..{int(run[-1])} "
+              f"of the {len(gates)} fused gates of this workload on its 2^{n}-amplitude state, {dt:.1f} s; "
+              f"value = their share of the workload's updates per second")
+    del state
     return rate, cores, sample
 
 
 def run_reference(args, spec):
+    """The reference's CPU path on this workload: its csim FP64 kernels
+    (src/csim, compiled by oracle/Makefile) apply the same fused gate list to
+    one 2^n complex128 state on all host cores.  The gate list is cut into
+    `steps` contiguous slices and step k applies the first quarter of slice k
+    (a stratified sample of the whole circuit that keeps the run within a few
+    minutes: the full n=30 circuit takes csim several minutes); value = the
+    sampled gates' share of the workload's updates (the same numerator as our
+    arm) over their time.  csim's time per gate does not depend on the
+    amplitudes.  The reference's own compressed CPU path (SZ3) cannot be
+    built here; csim uncompressed stands in for it."""
     # under torchrun only rank 0 runs the CPU baseline; the others exit at once
     if int(os.environ.get("RANK", "0")) != 0:
         return
@@ -209,29 +313,67 @@ def run_reference(args, spec):
     if not csim_ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcsim_ref.so not built"}))
         return
-    for _ in range(args.warmup):
-        cpu_sample(spec, budget_s=1.0)
-    rates = []
-    t0 = time.perf_counter()
-    sample = ""
-    cores = 1
-    for _ in range(args.steps):
-        r, cores, sample = cpu_sample(spec, budget_s=max(2.0, 60.0 / max(1, args.steps)))
-        rates.append(r)
-    wall = time.perf_counter() - t0
-    value = statistics.median(rates)
+    n = spec["n"]
+    if _host_memory_bytes() < (16 << n) + (4 << 30):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": f"host memory below the 2^{n} complex128 state of this workload"}))
+        return
+    from qulacs import gate as G
+    gates, updates = reference_setup(spec)
+    state = csim_ref.zero_state(n)
+    h = G.H(0)
+    for _ in range(args.warmup):        # H H = I: warm-up leaves the state unchanged
+        csim_ref.apply_gate(state, h)
+        csim_ref.apply_gate(state, h)
+    runs = sample_runs(len(gates), args.steps, 0.25)
+    times = csim_slices(state, gates, runs)
+    total = sum(times)
+    sampled = sum(len(r) for r in runs)
+    value = updates * (sampled / len(gates)) / total
+    cores = csim_ref.max_threads()
+    sample = (f"csim FP64 uncompressed (reference kernels, OpenMP {cores} threads) on one 2^{n}-amplitude state: "
+              f"{sampled} of the workload's {len(gates)} fused gates, the first quarter of each of {len(runs)} "
+              f"contiguous slices (one per step), {total:.1f} s; value = their share of the workload's updates "
+              f"per second")
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * wall / max(1, args.steps),
+        "steps": len(runs), "warmup": args.warmup, "ms_per_step": 1000 * total / max(1, len(runs)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": describe(spec)},
+        "data": "synthetic", "config": config_of(spec, updates),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "circuit_s_estimate": total * len(gates) / sampled,
     }
     print(json.dumps(out))
 
 
 # ----------------------------------------------------------------- our arm
+SLICE_LOG2 = 24
+
+
+def qft_fidelity(torch, cq, n, x):
+    """|<QFT x|psi>| (the reference's fidelity, script/run_sim.py:201-206) of
+    a compressed QFT|x> result, renormalised as get_vector does, and the
+    largest amplitude error, against the analytic FP64 state
+    2^{-n/2} e^{2 pi i x k / 2^n}; computed on the GPU in slices of 2^24
+    amplitudes."""
+    scale = 1.0 / math.sqrt(cq.get_squared_norm())
+    amp = 1.0 / math.sqrt(float(1 << n))
+    cnt = min(1 << SLICE_LOG2, 1 << n)
+    buf = torch.empty(2 * cnt, dtype=torch.float64, device="cuda")
+    acc = torch.zeros((), dtype=torch.complex128, device="cuda")
+    err = torch.zeros((), dtype=torch.float64, device="cuda")
+    for first in range(0, 1 << n, cnt):
+        cq.get_amplitudes_to(buf.data_ptr(), first, cnt, renormalize=False)
+        psi = torch.view_as_complex(buf.view(-1, 2)) * scale
+        k = torch.arange(first, first + cnt, dtype=torch.int64, device="cuda")
+        ph = ((k * x) & ((1 << n) - 1)).to(torch.float64) * (2.0 * math.pi / float(1 << n))
+        ref = torch.polar(torch.full_like(ph, amp), ph)
+        acc += torch.vdot(ref, psi)
+        err = torch.maximum(err, (ref - psi).abs().max())
+    return float(acc.abs().item()), float(err.item())
+
+
 def complex64_leg(spec, circuit, updates_per_step, torch, steps: int = 3):
     """The same fused gate list through the complex64 compressed pipeline
     (FP32 gate arithmetic and stored amplitudes, FP64 reductions)."""
@@ -254,8 +396,73 @@ def complex64_leg(spec, circuit, updates_per_step, torch, steps: int = 3):
     ms = e0.elapsed_time(e1) / steps
     out = {"ms_per_step": ms, "value": updates_per_step / (ms * 1e-3), "unit": UNIT, "steps": steps,
            "max_sv_bytes": cq.get_max_SV_bytes()}
+    if spec.get("qft_input") is not None:
+        f, e = qft_fidelity(torch, cq, spec["n"], spec["qft_input"])
+        out["fidelity"] = {"vs": "analytic QFT state (FP64)", "fidelity": f, "max_abs_err": e}
     del cq
     return out
+
+
+def brickwork_leg(torch, n: int = 32, layers: int = 20, B: int = 22, I: int = 4):
+    """Brickwork n=32, 20 layers (Haar SU(2) on every qubit, CZ on alternating
+    pairs; dense state, no zero blocks): the compressed pipeline in complex64
+    and complex128 against the plain per-gate complex128 path and this
+    package's fused uncompressed complex128 passes on the same fused gates;
+    the fused uncompressed state (64 GiB) is the FP64 oracle of the fidelity.
+    One timed apply each (the kernels are warm from the QFT legs)."""
+    import qulacs
+    from qulacs import _native
+    from qompsim import circuits as C
+    c = C.brickwork(n, layers, seed=0)
+    from qulacs.circuit import QuantumCircuitOptimizer
+    QuantumCircuitOptimizer(sv_block_size=B).optimize(c, block_size=2)
+    gates = list(c._gates)
+    res = {"workload": f"brickwork: n={n} {layers} layers, block_size={B}, inner_size={I}, eps_rel=1e-3, "
+                       f"eps_abs=1e-7", "gates": len(gates)}
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    ds = qulacs.QuantumState(n, dtype="complex128")
+    ds.set_computational_basis(0)
+    res["pergate_c128_ms"] = timed(lambda: ds._apply_gates(gates, pergate=True))
+    ds.set_computational_basis(0)
+    res["fused_dense_c128_ms"] = timed(lambda: ds._apply_gates(gates, pergate=False))
+    for dtype in ("complex64", "complex128"):
+        cq = qulacs.CompressedQuantumState(n, B, dtype=dtype, eps_rel=1e-3, eps_abs=1e-7,
+                                           flags=_native.QS_FLAG_QUIET)
+        cq.partition_and_register_circuit(c, I, 0)
+        ms = timed(cq.apply_circuit)
+        st = cq.get_stats()
+        scale = 1.0 / math.sqrt(cq.get_squared_norm())
+        cnt = 1 << SLICE_LOG2
+        rbuf = torch.empty(2 * cnt, dtype=torch.float64, device="cuda")
+
+        acc = torch.zeros((), dtype=torch.complex128, device="cuda")
+        err = torch.zeros((), dtype=torch.float64, device="cuda")
+        pbuf = torch.empty(2 * cnt, dtype=torch.float64, device="cuda")
+        for first in range(0, 1 << n, cnt):
+            cq.get_amplitudes_to(pbuf.data_ptr(), first, cnt, renormalize=False)
+            psi = torch.view_as_complex(pbuf.view(-1, 2)) * scale
+            ds.get_amplitudes_to(rbuf.data_ptr(), first, cnt)
+            ref = torch.view_as_complex(rbuf.view(-1, 2))
+            acc += torch.vdot(ref, psi)
+            err = torch.maximum(err, (ref - psi).abs().max())
+        res[dtype] = {"ms": ms, "passes": int(st["passes"]), "stages": int(st["stages"]),
+                      "amp_gate_updates": int(st["amp_gate_updates"]),
+                      "updates_per_s": st["amp_gate_updates"] / (ms * 1e-3),
+                      "max_sv_bytes": cq.get_max_SV_bytes(),
+                      "fidelity": float(acc.abs().item()), "max_abs_err": float(err.item()),
+                      "speedup_vs_pergate_c128": res["pergate_c128_ms"] / ms}
+        del cq
+    del ds
+    return res
 
 
 def adjoint_leg(torch, n: int = 24, depth: int = 8, reps: int = 5):
@@ -333,6 +540,12 @@ def run_ours(args, spec):
     barrier(pg, torch)
     clocks = clk.summary()
 
+    # ---- parity of the timed result: fidelity against the analytic state (outside the timed region)
+    fidelity = None
+    if spec.get("qft_input") is not None:
+        f, e = qft_fidelity(torch, cq, spec["n"], spec["qft_input"])
+        fidelity = {"vs": "analytic QFT state (FP64)", "fidelity": f, "max_abs_err": e}
+
     # ---- end to end through the C ABI with host buffers
     cq.set_computational_basis(0)
     blob_in = cq.export_store()
@@ -385,8 +598,8 @@ def run_ours(args, spec):
         dense = legs
         dense["compressed_speedup_vs_pergate_c128"] = legs["pergate_c128"]["ms_per_step"] / (ms / args.steps)
 
-    # ---- the same circuit in the complex64 pipeline, and the adjoint gradient of the
-    # hardware-efficient ansatz against its forward pass (rank 0, N=1 only)
+    # ---- the same circuit in the complex64 pipeline, the adjoint gradient of the
+    # hardware-efficient ansatz against its forward pass, brickwork n=32 (rank 0, N=1 only)
     extra = {}
     max_sv = cq.get_max_SV_bytes()
     if rank == 0 and world == 1 and not args.no_legs:
@@ -396,14 +609,19 @@ def run_ours(args, spec):
             extra["complex64"]["speedup_vs_pergate_c128"] = (dense["pergate_c128"]["ms_per_step"]
                                                              / extra["complex64"]["ms_per_step"])
         extra["adjoint"] = adjoint_leg(torch)
+        if not args.no_brickwork:
+            extra["brickwork32"] = brickwork_leg(torch)
 
-    # ---- CPU baseline (rank 0, N=1 only)
+    # ---- CPU baseline (rank 0, N=1 only): a bounded slice of the same workload
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import csim_ref
         if csim_ref.available():
-            rate, cores, sample = cpu_sample(spec)
-            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample}
+            gates_ref, updates_ref = reference_setup(spec)
+            got = cpu_slice(spec, gates_ref, updates_ref)
+            if got is not None:
+                rate, cores, sample = got
+                cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample}
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -411,24 +629,24 @@ def run_ours(args, spec):
         ratio = ncu_traffic_ratio()
         traffic = ratio * pass_bytes / max(1, passes) if ratio is not None else None
         launches_per_step = int(st["passes"]) + 4 * int(st["stages"]) + 1
+        config = config_of(spec, updates_per_step)
+        config.update({"stages": int(st["stages"]), "passes": int(st["passes"]),
+                       "header_only_passes": int(st["perm_passes"]), "gates": circuit.get_gate_count(),
+                       "parallelism": f"replicas x{world}",
+                       "l2": "compressed store larger than L2 (126 MB); no flush between steps",
+                       "max_sv_bytes": max_sv})
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if spec["dtype"] == "complex128" else "f32",
             "data": "synthetic",
-            "config": {"workload": describe(spec), "n": spec["n"], "block_size": spec["block_size"],
-                       "inner_size": spec["inner_size"], "stages": int(st["stages"]), "passes": int(st["passes"]),
-                       "header_only_passes": int(st["perm_passes"]),
-                       "gates": circuit.get_gate_count(), "amp_gate_updates_per_step": updates_per_step,
-                       "parallelism": f"replicas x{world}",
-                       "l2": "compressed store larger than L2 (126 MB); no flush between steps",
-                       "max_sv_bytes": max_sv},
+            "config": config,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
                          "traffic_source": "ncu DRAM/algorithmic ratio of QFT n=26 (profiles/) x bytes per launch",
-                         "kernel": f"pass_kernel<{'double' if spec['dtype'] == 'complex128' else 'float'}, 4, *> "
+                         "kernel": f"pass_kernel<{'double' if spec['dtype'] == 'complex128' else 'float'}, *> "
                                    "(value and code-domain tile passes)",
                          "pass_ms_per_step": pass_ms / args.steps,
                          "bytes_per_launch": pass_bytes / max(1, passes)},
@@ -437,6 +655,7 @@ def run_ours(args, spec):
                     "ms_per_step": e2e_ms / args.steps},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clocks,
+            "fidelity": fidelity,
             "cpu_baseline": cpu,
             "uncompressed": dense,
         }
@@ -455,7 +674,8 @@ def main():
     ap.add_argument("--workload", default="qft30")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-dense", action="store_true", help="skip the uncompressed per-gate comparison leg")
-    ap.add_argument("--no-legs", action="store_true", help="skip the complex64 and adjoint-gradient legs")
+    ap.add_argument("--no-legs", action="store_true", help="skip the complex64, adjoint-gradient and brickwork legs")
+    ap.add_argument("--no-brickwork", action="store_true", help="skip the brickwork n=32 leg")
     args = ap.parse_args()
     spec = workload_spec(args.workload)
     if args.impl == "reference":

@@ -1075,17 +1075,29 @@ static void make_block_groups(qs_state *h) {
     }
 }
 
-// Device-side plan: passes of every stage, gates with tile positions, maps.
-static qs_status build_device_plan(qs_state *h) {
+// The device passes of every stage as host data: h->passes plus the op
+// records, sweeps and matrix pool they index.  Host code only.
+struct HostPlan {
+    std::vector<qs::KGate> kg;
+    std::vector<qs::Sweep> sw;
+    std::vector<qs::ROp> ops;
+    std::vector<cplx> pool;
+};
+
+static qs_status plan_device_passes(qs_state *h, HostPlan *plan) {
     const int C = (int)h->C;
     const int jmax = std::min(h->tile_log2 - C, qs::kMaxTileQubits);
     // tiles are padded to the largest size: fewer tiles, each with its fixed
     // costs (headers, reservation, barriers) spread over more chunks
     const int jmin = std::min(jmax, std::max(env_int("QOMPSIM_TILE_MIN_QUBITS", jmax), qs::kRegBits - C));
-    std::vector<qs::KGate> kg;
-    std::vector<qs::Sweep> sw;
-    std::vector<qs::ROp> ops;
-    std::vector<cplx> pool;
+    std::vector<qs::KGate> &kg = plan->kg;
+    std::vector<qs::Sweep> &sw = plan->sw;
+    std::vector<qs::ROp> &ops = plan->ops;
+    std::vector<cplx> &pool = plan->pool;
+    kg.clear();
+    sw.clear();
+    ops.clear();
+    pool.clear();
     h->passes.clear();
     const bool permute = env_int("QOMPSIM_PERMUTE_CHUNKS", 1) != 0;
     for (uint32_t s = 0; s < h->stages.size(); ++s) {
@@ -1166,6 +1178,14 @@ static qs_status build_device_plan(qs_state *h) {
             h->passes.push_back(dp);
         }
     }
+    return QS_OK;
+}
+
+// Upload a host plan: op records, matrix pool, sweeps, block-to-group maps.
+static qs_status upload_device_plan(qs_state *h, const HostPlan &plan) {
+    const std::vector<qs::Sweep> &sw = plan.sw;
+    const std::vector<qs::ROp> &ops = plan.ops;
+    const std::vector<cplx> &pool = plan.pool;
     if (h->kgates) { cudaFree(h->kgates); h->kgates = nullptr; }
     if (h->sweeps_dev) { cudaFree(h->sweeps_dev); h->sweeps_dev = nullptr; }
     if (h->ops_dev) { cudaFree(h->ops_dev); h->ops_dev = nullptr; }
@@ -1212,6 +1232,14 @@ static qs_status build_device_plan(qs_state *h) {
     }
     h->planned = true;
     return QS_OK;
+}
+
+// Device-side plan: passes of every stage, gates with tile positions, maps.
+static qs_status build_device_plan(qs_state *h) {
+    HostPlan plan;
+    qs_status st = plan_device_passes(h, &plan);
+    if (st != QS_OK) return st;
+    return upload_device_plan(h, plan);
 }
 
 qs_status qs_partition(qs_state *h, uint32_t inner_size, int verbose) {
@@ -1555,7 +1583,7 @@ qs_status qs_get_amplitudes(qs_state *h, uint64_t first, uint64_t count, double 
                                            h->codec, cfirst + c0, cnt, dbuf, scale, h->stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(out + c0 * chunk_amps * 2, dbuf, cnt * chunk_amps * 2 * sizeof(double),
-                                cudaMemcpyDeviceToHost, h->stream);
+                                cudaMemcpyDefault, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) {
             (void)cudaGetLastError();
@@ -2171,6 +2199,8 @@ qs_status qs_import_store(qs_state *h, const void *buf, uint64_t size) {
     CUDA_TRY(h, cudaMemcpyAsync(h->meta[h->mcur], p, h->nchunks * sizeof(qs::ChunkMeta), cudaMemcpyHostToDevice, s));
     p += h->nchunks * sizeof(qs::ChunkMeta);
     if (hd.arena_bytes) CUDA_TRY(h, cudaMemcpyAsync(h->arena[h->cur], p, hd.arena_bytes, cudaMemcpyDefault, s));
+    // headers of unstored blocks were not validated: zero them on the device
+    CUDA_TRY(h, qs::launch_zero_unstored_headers(h->meta[h->mcur], h->mask, h->nchunks, (int)(h->B - h->C), s));
     CUDA_TRY(h, cudaStreamSynchronize(s));
     h->arena_used = hd.arena_bytes;
     uint64_t total = 0;
@@ -2426,13 +2456,13 @@ qs_status qs_dense_get_amplitudes(qs_dense *h, uint64_t first, uint64_t count, d
     if (!count) return QS_OK;
     if (h->f64) {
         CUDA_TRY(h, cudaMemcpyAsync(out, static_cast<const double *>(h->state) + 2 * first, count * 16,
-                                    cudaMemcpyDeviceToHost, h->stream));
+                                    cudaMemcpyDefault, h->stream));
     } else {
         double *tmp = nullptr;
         CUDA_TRY(h, cudaMalloc(&tmp, count * 16));
         cudaError_t e = qs::launch_dense_to_c128(false, static_cast<const float *>(h->state) + 2 * first, count, tmp,
                                                  h->stream);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, count * 16, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, count * 16, cudaMemcpyDefault, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         cudaFree(tmp);
         if (e != cudaSuccess) {

@@ -25,6 +25,10 @@ constexpr int kPassThreads = 128;
 
 // Header of one encoded chunk (16 bytes).  offset is a byte offset into the
 // payload arena; the payload is 128 * rows bytes (see codec.cuh).
+// Invariant every device reader relies on: the header of a chunk is read only
+// when its block is stored (zero mask set) or the pass is not the first of
+// its stage (every block of an active group has been written by then); the
+// headers of unstored blocks are zero (offset 0, width 0) after an import.
 struct ChunkMeta {
     uint64_t offset;
     int32_t base;
@@ -310,6 +314,10 @@ cudaError_t launch_codec_test(bool f64, const void *vals, int C, CodecParams cod
 cudaError_t launch_codec_roundtrip_noalloc(bool f64, const void *vals, int C, CodecParams codec, uint64_t nchunks,
                                            int32_t *bases, uint32_t *widths, void *decoded, cudaStream_t stream);
 uint64_t noalloc_scratch_words();
+
+// Imported stores: headers of the chunks of unstored blocks set to zero.
+cudaError_t launch_zero_unstored_headers(ChunkMeta *meta, const uint8_t *mask, uint64_t nchunks, int cshift,
+                                         cudaStream_t stream);
 
 int sm_count();
 

@@ -1433,6 +1433,15 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_pass_kernel(const AdjPass
         if (s_acc[i] != 0.0) atomicAdd(&a.out[i], s_acc[i]);
 }
 
+// Imported stores: the header of every chunk of an unstored block is set to
+// zero (offset 0, width 0), so that a reader that skipped the zero-mask gate
+// would still read inside the arena.
+__global__ void zero_unstored_headers_kernel(ChunkMeta *meta, const uint8_t *mask, uint64_t nchunks, int cshift) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nchunks;
+         k += (uint64_t)gridDim.x * blockDim.x)
+        if (!mask[k >> cshift]) meta[k] = ChunkMeta{0, 0, 0};
+}
+
 int g_sm_count = 0;
 
 // Scratch of the allocation-free codec round trip (qs_codec_roundtrip_noalloc):
@@ -1629,6 +1638,13 @@ cudaError_t launch_codec_test(bool f64, const void *vals, int C, CodecParams p, 
 
 uint64_t noalloc_scratch_words() { return kNoAllocScratchWords; }
 
+cudaError_t launch_zero_unstored_headers(ChunkMeta *meta, const uint8_t *mask, uint64_t nchunks, int cshift,
+                                         cudaStream_t s) {
+    const unsigned grid = grid_for(nchunks, 256, 8);
+    zero_unstored_headers_kernel<<<grid, 256, 0, s>>>(meta, mask, nchunks, cshift);
+    return cudaGetLastError();
+}
+
 template <typename R>
 static cudaError_t launch_adjoint_pass_t(const AdjPassArgs &a, cudaStream_t s) {
     if (a.nslots > kMaxAdjSlots) return cudaErrorInvalidValue;
@@ -1653,7 +1669,11 @@ cudaError_t launch_adjoint_pass(bool f64, const AdjPassArgs &a, cudaStream_t s) 
 
 // Host code may not use g_noalloc_words directly: in host code the name is a
 // host-side stand-in, not a device address.  The device address is looked up
-// once per device, with that device current, and cached.
+// with the device current on every call made outside a stream capture (a
+// host-side table lookup once the module is loaded), so a device reset or a
+// different context on the same device is picked up; a call inside a
+// capture uses the address that the last call outside one found on that
+// device (the first call on a device must come before any capture).
 cudaError_t launch_codec_roundtrip_noalloc(bool f64, const void *vals, int C, CodecParams p, uint64_t nchunks,
                                            int32_t *bases, uint32_t *widths, void *decoded, cudaStream_t s) {
     static std::mutex mu;
@@ -1662,10 +1682,13 @@ cudaError_t launch_codec_roundtrip_noalloc(bool f64, const void *vals, int C, Co
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) return e;
     uint32_t *words = nullptr;
     {
         std::lock_guard<std::mutex> lock(mu);
-        if (addr[dev] == nullptr) {
+        if (cap == cudaStreamCaptureStatusNone || addr[dev] == nullptr) {
             void *ptr = nullptr;
             e = cudaGetSymbolAddress(&ptr, g_noalloc_words);
             if (e != cudaSuccess) return e;

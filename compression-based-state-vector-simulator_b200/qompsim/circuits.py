@@ -153,12 +153,12 @@ def qaoa_maxcut(n: int, p: int = 4, seed: int = 0) -> qulacs.QuantumCircuit:
 WORKLOADS = {
     "ghz20": dict(builder=lambda: ghz_fanout(20), n=20, block_size=12, inner_size=4, dtype="complex128",
                   eps_rel=1e-3, eps_abs=1e-7),
-    "qft30": dict(builder=lambda: qft_basis(30, seed=0), n=30, block_size=20, inner_size=4, dtype="complex128",
+    "qft30": dict(builder=lambda: qft_basis(30, seed=0), qft_input=qft_input(30, 0), n=30, block_size=20, inner_size=4, dtype="complex128",
                   eps_rel=1e-3, eps_abs=1e-7),
-    "qft26": dict(builder=lambda: qft_basis(26, seed=0), n=26, block_size=20, inner_size=4, dtype="complex128",
+    "qft26": dict(builder=lambda: qft_basis(26, seed=0), qft_input=qft_input(26, 0), n=26, block_size=20, inner_size=4, dtype="complex128",
                   eps_rel=1e-3, eps_abs=1e-7),
     # the QFT workload in the complex64 pipeline (FP32 gate arithmetic, FP64 reductions)
-    "qft30c64": dict(builder=lambda: qft_basis(30, seed=0), n=30, block_size=20, inner_size=4, dtype="complex64",
+    "qft30c64": dict(builder=lambda: qft_basis(30, seed=0), qft_input=qft_input(30, 0), n=30, block_size=20, inner_size=4, dtype="complex64",
                      eps_rel=1e-3, eps_abs=1e-7),
     "brickwork32": dict(builder=lambda: brickwork(32, 20, seed=0), n=32, block_size=22, inner_size=4,
                         dtype="complex64", eps_rel=1e-3, eps_abs=1e-7),

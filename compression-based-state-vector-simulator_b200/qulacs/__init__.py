@@ -314,6 +314,13 @@ class QuantumState:
                                                      out.view(np.float64).ctypes.data_as(_n.ct.POINTER(_n.ct.c_double))))
         return out
 
+    def get_amplitudes_to(self, address: int, first: int, count: int) -> None:
+        """get_amplitudes written as 2*count interleaved doubles at `address`
+        (host memory or device memory of the state's GPU)."""
+        self._check(_n.lib().qs_dense_get_amplitudes(self._h, int(first), int(count),
+                                                     _n.ct.cast(_n.ct.c_void_p(int(address)),
+                                                                _n.ct.POINTER(_n.ct.c_double))))
+
     def get_squared_norm(self) -> float:
         v = _n.ct.c_double()
         self._check(_n.lib().qs_dense_norm_squared(self._h, _n.ct.byref(v)))
@@ -487,6 +494,14 @@ class CompressedQuantumState:
                                                out.view(np.float64).ctypes.data_as(_n.ct.POINTER(_n.ct.c_double)),
                                                1 if renormalize else 0))
         return out
+
+    def get_amplitudes_to(self, address: int, first: int, count: int, renormalize: bool = True) -> None:
+        """The amplitudes of get_amplitudes written as 2*count interleaved
+        doubles at `address`: host memory or device memory of the state's
+        GPU (e.g. a torch CUDA tensor's data_ptr())."""
+        self._check(_n.lib().qs_get_amplitudes(self._h, int(first), int(count),
+                                               _n.ct.cast(_n.ct.c_void_p(int(address)), _n.ct.POINTER(_n.ct.c_double)),
+                                               1 if renormalize else 0))
 
     def get_squared_norm(self) -> float:
         v = _n.ct.c_double()

@@ -204,7 +204,9 @@ qs_status qs_get_vector(qs_state *h, double *out, int renormalize);
 /* Amplitudes [first, first + count) of the same dense vector (2*count
  * doubles); first and count are multiples of the chunk size 2^chunk_log2.
  * Lets a caller stream a state larger than host memory allows at once
- * (fidelity in slices); the reference reads only whole vectors. */
+ * (fidelity in slices); the reference reads only whole vectors.  out may be
+ * host memory or device memory of the state's GPU (the copy direction is
+ * taken from the pointer), so a slice can be compared on the device. */
 qs_status qs_get_amplitudes(qs_state *h, uint64_t first, uint64_t count, double *out, int renormalize);
 
 /* sampling_blockwise(sampling_count, random_seed) -- compressed_state.hpp:
@@ -319,7 +321,8 @@ qs_status qs_dense_apply_gates_pergate(qs_dense *h, const qs_gate *gates, size_t
 
 /* QuantumState::get_vector / load (state.hpp:445-1045); 2*2^n doubles. */
 qs_status qs_dense_get_vector(qs_dense *h, double *out);
-/* Amplitudes [first, first + count) as complex128 (2*count doubles). */
+/* Amplitudes [first, first + count) as complex128 (2*count doubles); out
+ * may be host memory or device memory of the state's GPU. */
 qs_status qs_dense_get_amplitudes(qs_dense *h, uint64_t first, uint64_t count, double *out);
 qs_status qs_dense_set_vector(qs_dense *h, const double *in);
 qs_status qs_dense_set_basis_state(qs_dense *h, uint64_t basis);
@@ -392,8 +395,11 @@ qs_status qs_codec_test(qs_dtype dtype, double eps_rel, double eps_abs, uint32_t
  * return QS_ERR_ARG, nothing is launched).  The call allocates nothing,
  * enqueues one kernel on `stream` (a cudaStream_t, NULL = default stream)
  * and does not synchronise.  Its first call on a device looks up the
- * array's device address (once per device, with that device current), so
- * make that first call before any stream capture.  Every call shares the
+ * array's device address with that device current, so make that first call
+ * before any stream capture.  Every later call made outside a capture looks
+ * the address up again (after cudaDeviceReset, or under another context on
+ * the same device, the array has a new address); a call inside a capture
+ * uses the address that the last call outside one found.  Every call shares the
  * one array: calls that overlap on the GPU (different streams, no ordering
  * between them) race on it.  Nothing in the array needs to start at zero;
  * it keeps the last call's words.  Errors are reported through

@@ -1,7 +1,8 @@
 // CPU check of host logic of the engine that the device tests only reach
 // indirectly.  Compiled together with engine.cpp (included below) by
-// tests/test_engine_host.py; nothing here touches a GPU: the planner builds
-// its passes before any upload, and the store-header check is host code.
+// tests/test_engine_host.py; nothing here touches a GPU: the planner's host
+// step (plan_device_passes) uploads nothing, and the store-header check is
+// host code.
 //
 //   engine_host_check headers
 //       store_headers_valid: valid stores pass; a misaligned offset, a width
@@ -79,7 +80,11 @@ static int check_plan(const char *path, uint32_t n, uint32_t B, uint32_t I, bool
     }
     h.stages = partition_circuit(&h, I);
     make_block_groups(&h);
-    (void)build_device_plan(&h);  // fails at the upload without a GPU; the passes are planned by then
+    HostPlan plan;
+    if (plan_device_passes(&h, &plan) != QS_OK) {
+        printf("plan: %s\n", h.err.c_str());
+        return 2;
+    }
     const int jmax = std::min(h.tile_log2 - (int)h.C, qs::kMaxTileQubits);
     for (const auto &dp : h.passes)
         printf("pass kind %d j %d codes %d jmax %d\n", dp.kind, dp.j, dp.code_moves ? 1 : 0, jmax);

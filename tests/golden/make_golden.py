@@ -2,7 +2,7 @@
 
 Run in a container where the reference is mounted (it does not travel):
 
-    python tests/golden/make_golden.py [/root/reference]
+    python tests/golden/make_golden.py <reference checkout>
 
 What comes from the reference:
 * the circuits: the reference's own generators (benchmark/circuit_factory.py,
@@ -74,4 +74,6 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference checkout (the directory holding src/ and benchmark/)>")
+    main(sys.argv[1])

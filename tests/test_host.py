@@ -225,3 +225,15 @@ def test_stage_chunk_permutation_leaves_low_qubits_alone():
     assert cnt.value == 3
     assert [out[k].targets[0] for k in range(3)] == [0, 1, 5]
     assert list(dst) == [0, 3, 2, 1] and flip.value == 1 << 2
+
+
+def test_bench_workload_update_count_qft30():
+    """The QFT n=30 bench workload's amplitude-gate updates per apply, as
+    bench.py's reference arm computes them on the host, equal the engine's
+    device count for that workload (341525397504, read from its stats on a
+    B200)."""
+    import bench
+    spec = bench.workload_spec("qft30")
+    gates, updates = bench.reference_setup(spec)
+    assert len(gates) == 456
+    assert updates == 341525397504

@@ -81,3 +81,35 @@ def test_noalloc_refuses_more_than_its_scratch():
     st = L.qs_codec_roundtrip_noalloc(0, 1e-3, 1e-7, C, p, too_many, p, p, p, None)
     assert st == _native.QS_ERR_ARG
     assert b"scratch" in L.qs_dense_last_error(None)
+
+
+@pytest.mark.parametrize("C", [8, 4])
+def test_noalloc_at_exact_capacity(C):
+    """A call of exactly as many chunks as the fixed scratch holds
+    (2^20 / 2^(C+1)): the last chunk's slot ends at the array's last word;
+    the result equals the allocating entry point's bit for bit."""
+    import torch
+    from qulacs import _native
+
+    L = _native.load_library()
+    n = 2 << C
+    nch = (1 << 20) // n
+    rng = np.random.default_rng(30 + C)
+    scale = 10.0 ** -rng.uniform(0, 6, size=(nch, 1))
+    vals = (rng.normal(size=(nch, n)) * scale).reshape(-1)
+    # the last chunk as wide as codes get (magnitudes from 1e-300 to 1e300), deep into its slot
+    vals[-n:] = rng.choice([-1.0, 1.0], size=n) * 10.0 ** rng.uniform(-300, 300, size=n)
+    ref_bases, ref_widths, ref_dec = _allocating(L, True, C, vals, nch)
+    d_vals = torch.from_numpy(vals).cuda()
+    d_bases = torch.full((nch,), -1, dtype=torch.int32, device="cuda")
+    d_widths = torch.full((nch,), -1, dtype=torch.int32, device="cuda")
+    d_dec = torch.full_like(d_vals, float("nan"))
+    stream = ct.c_void_p(torch.cuda.current_stream().cuda_stream)
+    st = L.qs_codec_roundtrip_noalloc(0, 1e-3, 1e-7, C, ct.c_void_p(d_vals.data_ptr()), nch,
+                                      ct.c_void_p(d_bases.data_ptr()), ct.c_void_p(d_widths.data_ptr()),
+                                      ct.c_void_p(d_dec.data_ptr()), stream)
+    assert st == 0, L.qs_dense_last_error(None)
+    torch.cuda.synchronize()
+    assert np.array_equal(d_bases.cpu().numpy(), ref_bases)
+    assert np.array_equal(d_widths.cpu().numpy().view(np.uint32), ref_widths)
+    assert np.array_equal(d_dec.cpu().numpy(), ref_dec)
