@@ -466,6 +466,7 @@ def brickwork_leg(torch, n: int = 32, layers: int = 20, B: int = 22, I: int = 4)
 
 
 def adjoint_leg(torch, n: int = 24, depth: int = 8, reps: int = 5):
+    import numpy as np
     """Hardware-efficient ansatz n=24, depth 8 (RY RZ per qubit + CNOT ladder,
     384 parameters), H = sum Z_i Z_i+1 + 0.5 sum X_i: wall time of the energy
     alone and of energy + adjoint gradient through the public API, each call
@@ -495,7 +496,32 @@ def adjoint_leg(torch, n: int = 24, depth: int = 8, reps: int = 5):
         fwd = best(energy)
         grad = best(energy_and_gradient)
         res[dtype] = {"energy_ms": fwd * 1e3, "energy_and_gradient_ms": grad * 1e3, "ratio": grad / fwd}
+    res["compressed"] = compressed_adjoint_leg(torch, circ, obs, n)
     return res
+
+
+def compressed_adjoint_leg(torch, circ, obs, n: int, B: int = 18, I: int = 4, reps: int = 3):
+    import numpy as np
+    """The same ansatz with both states compressed (complex64, FP64
+    reductions, eps_rel 1e-3 / eps_abs 1e-7), device checkpoints after every
+    layer's 48 parameters: device times (CUDA events) of the forward pass with
+    its energy, of lambda = H psi and of the backward sweep, the best of
+    `reps` calls; gradient error against the uncompressed FP64 adjoint."""
+    from qulacs.torch import compressed_adjoint_gradient, energy_and_gradient
+    e_ref, g_ref = energy_and_gradient(circ, obs, "complex128")
+    best = None
+    for _ in range(reps):
+        tm = {}
+        e, g = compressed_adjoint_gradient(circ, obs, B, I, "complex64", checkpoint_every=2 * n, timings=tm)
+        if best is None or sum(tm.values()) < sum(best[0].values()):
+            best = (tm, e, g)
+    tm, e, g = best
+    fwd = tm["forward_ms"]
+    return {"block_size": B, "inner_size": I, "dtype": "complex64", "checkpoint_every": 2 * n,
+            "forward_ms": fwd, "lambda_ms": tm["lambda_ms"], "backward_ms": tm["backward_ms"],
+            "ratio": (fwd + tm["lambda_ms"] + tm["backward_ms"]) / fwd,
+            "energy_err": abs(e - e_ref), "grad_max_abs_err_vs_fp64": float(np.max(np.abs(g - g_ref))),
+            "grad_max_abs": float(np.max(np.abs(g_ref)))}
 
 
 def run_ours(args, spec):
@@ -595,8 +621,31 @@ def run_ours(args, spec):
             legs[name] = {"ms_per_step": dms, "value": updates_per_step / (dms * 1e-3), "unit": UNIT,
                           "launches_per_step": len(gates) if pergate else None}
         del ds
+        # the reference's own plain complex128 GPU path (src/gpusim, built
+        # from source): one reference kernel per gate on its own stream
+        from oracle import gpusim_ref
+        if gpusim_ref.available():
+            gs = gpusim_ref.GpuState(spec["n"])
+            recs = gs.prepare(gates)
+            gs.apply_prepared(recs)     # warm-up
+            gs.sync()
+            gs.set_zero_state()
+            gs.sync()
+            t0 = time.perf_counter()
+            gs.apply_prepared(recs)
+            gs.sync()
+            gms = (time.perf_counter() - t0) * 1e3
+            legs["pergate_reference_gpusim_c128"] = {
+                "ms_per_step": gms, "value": updates_per_step / (gms * 1e-3), "unit": UNIT,
+                "launches_per_step": len(gates),
+                "note": "the reference's src/gpusim kernels built for sm_100a, timed on the host clock around one "
+                        "synchronised apply of the gate list"}
+            del gs
         dense = legs
         dense["compressed_speedup_vs_pergate_c128"] = legs["pergate_c128"]["ms_per_step"] / (ms / args.steps)
+        if "pergate_reference_gpusim_c128" in legs:
+            dense["compressed_speedup_vs_reference_gpusim_c128"] = (
+                legs["pergate_reference_gpusim_c128"]["ms_per_step"] / (ms / args.steps))
 
     # ---- the same circuit in the complex64 pipeline, the adjoint gradient of the
     # hardware-efficient ansatz against its forward pass, brickwork n=32 (rank 0, N=1 only)

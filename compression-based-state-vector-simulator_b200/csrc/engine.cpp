@@ -686,6 +686,117 @@ std::vector<PassPlan> plan_passes(const std::vector<uint32_t> &gate_ids, const s
     return out;
 }
 
+// The same split with commuting gates reordered: two gates that share a
+// qubit commute when neither mixes amplitudes along it (both are then
+// block-diagonal in that qubit and act on disjoint other qubits), so a gate
+// waits only for the earlier gates it does not commute with.  Each pass
+// takes, in index order and repeatedly, every ready gate whose mixing qubits
+// >= C still fit the tile and whose other qubits >= C fit the outer
+// selectors; a gate made ready by one taken in this pass may join it.  A
+// pass's gate list is a valid order of its gates.
+std::vector<PassPlan> plan_passes_dag(const std::vector<uint32_t> &gate_ids, const std::vector<CGate> &cg, int C,
+                                      int jmax, int jmin, int pad_lo, int pad_hi) {
+    const size_t G = gate_ids.size();
+    std::vector<std::vector<uint32_t>> succ(G);
+    std::vector<int> indeg(G, 0);
+    {
+        std::vector<int> last_mix;                 // per qubit: last gate mixing it
+        std::vector<std::vector<uint32_t>> users;  // per qubit: non-mixing gates since then
+        for (size_t i = 0; i < G; ++i) {
+            const CGate &g = cg[gate_ids[i]];
+            std::vector<uint32_t> preds;
+            for (int b = 0; b < g.nq; ++b) {
+                const int q = g.q[b];
+                if ((int)last_mix.size() <= q) {
+                    last_mix.resize(q + 1, -1);
+                    users.resize(q + 1);
+                }
+                if (last_mix[q] >= 0) preds.push_back((uint32_t)last_mix[q]);
+                if (g.mix[b]) {
+                    preds.insert(preds.end(), users[q].begin(), users[q].end());
+                    last_mix[q] = (int)i;
+                    users[q].clear();
+                } else {
+                    users[q].push_back((uint32_t)i);
+                }
+            }
+            std::sort(preds.begin(), preds.end());
+            preds.erase(std::unique(preds.begin(), preds.end()), preds.end());
+            for (uint32_t p : preds) {
+                succ[p].push_back((uint32_t)i);
+                ++indeg[i];
+            }
+        }
+    }
+    std::set<uint32_t> ready;
+    for (size_t i = 0; i < G; ++i)
+        if (indeg[i] == 0) ready.insert((uint32_t)i);
+    auto outside = [](const std::set<int> &a, const std::set<int> &t) {
+        int k = 0;
+        for (int q : a) k += t.count(q) ? 0 : 1;
+        return k;
+    };
+    // Fill one pass starting from gate `seed` (taken first), then every
+    // fitting ready gate in index order; works on copies unless `commit`.
+    // Returns the gates taken.  (Seeding each pass with the ready gate whose
+    // fill takes the most gates measured no better than the lowest one.)
+    auto fill = [&](uint32_t seed, bool commit, std::set<int> *tile_out) -> std::vector<uint32_t> {
+        std::vector<int> deg_copy;
+        std::set<uint32_t> ready_copy;
+        std::vector<int> &deg = commit ? indeg : (deg_copy = indeg);
+        std::set<uint32_t> &rdy = commit ? ready : (ready_copy = ready);
+        std::set<int> cur, sel;
+        std::vector<uint32_t> taken;
+        auto take = [&](uint32_t i) {
+            const CGate &g = cg[gate_ids[i]];
+            for (int b = 0; b < g.nq; ++b) {
+                if (g.q[b] < C) continue;
+                (g.mix[b] ? cur : sel).insert(g.q[b]);
+            }
+            taken.push_back(i);
+            rdy.erase(i);
+            for (uint32_t sx : succ[i])
+                if (--deg[sx] == 0) rdy.insert(sx);
+        };
+        take(seed);
+        bool grew = true;
+        while (grew) {
+            grew = false;
+            for (uint32_t i : rdy) {
+                const CGate &g = cg[gate_ids[i]];
+                std::set<int> need = cur, nsel = sel;
+                for (int b = 0; b < g.nq; ++b) {
+                    if (g.q[b] < C) continue;
+                    (g.mix[b] ? need : nsel).insert(g.q[b]);
+                }
+                if ((int)need.size() > jmax || outside(nsel, need) > qs::kMaxOuterSel) continue;
+                take(i);
+                grew = true;
+                break;  // the ready set changed: rescan from the lowest index
+            }
+        }
+        if (tile_out) *tile_out = cur;
+        return taken;
+    };
+    std::vector<PassPlan> out;
+    size_t placed = 0;
+    while (placed < G) {
+        const uint32_t best = *ready.begin();
+        PassPlan p;
+        std::set<int> cur;
+        for (uint32_t i : fill(best, true, &cur)) p.gates.push_back(gate_ids[i]);
+        placed += p.gates.size();
+        p.tile.assign(cur.begin(), cur.end());
+        out.push_back(p);
+    }
+    for (auto &pp : out) {
+        std::set<int> s2(pp.tile.begin(), pp.tile.end());
+        for (int q = pad_lo; q < pad_hi && (int)s2.size() < jmin; ++q) s2.insert(q);
+        pp.tile.assign(s2.begin(), s2.end());
+    }
+    return out;
+}
+
 std::string format_size(unsigned long long size) {
     char buf[64];
     if (size > (1ULL << 30)) snprintf(buf, sizeof(buf), "%.3f GiB", (double)size / (1ULL << 30));
@@ -754,12 +865,42 @@ struct qs_state {
     qs::ROp *ops_dev = nullptr;
     void *pool_dev = nullptr;
     std::vector<DevPass> passes;
+    // Merged tail: once every block is stored, the remaining stages run as
+    // one gate sequence (plan_tail_passes), planned for the first stage at
+    // which that happened and kept while the circuit stays registered.
+    bool merge_tail = true;
+    int tail_from = -1;
+    std::vector<DevPass> tail_passes;
+    std::vector<int> tail_stage_end;      // per stage from tail_from: the tail pass ending it
+    qs::Sweep *tail_sweeps_dev = nullptr;
+    qs::ROp *tail_ops_dev = nullptr;
+    void *tail_pool_dev = nullptr;
+    unsigned long long *tail_stats = nullptr;  // 3 counters per tail pass
+    size_t tail_stats_cap = 0;
+    std::vector<cudaEvent_t> tail_ev;
+    uint32_t *full_dev = nullptr;         // 1 when every block is stored (mask_full_kernel)
+    uint32_t *full_host = nullptr;        // pinned copy read after the stage
+    int last_tail_from = -1;              // stage the last apply merged from (-1: none)
+    void drop_tail() {
+        if (tail_sweeps_dev) cudaFree(tail_sweeps_dev);
+        if (tail_ops_dev) cudaFree(tail_ops_dev);
+        if (tail_pool_dev) cudaFree(tail_pool_dev);
+        for (auto e : tail_ev) cudaEventDestroy(e);
+        tail_ev.clear();
+        tail_sweeps_dev = nullptr;
+        tail_ops_dev = nullptr;
+        tail_pool_dev = nullptr;
+        tail_passes.clear();
+        tail_stage_end.clear();
+        tail_from = -1;
+    }
     std::vector<uint64_t> stage_amps;   // amplitudes in active groups (for stats), filled on demand
 
     qs::ChunkMeta *meta[2] = {nullptr, nullptr};
     uint32_t *arena[2] = {nullptr, nullptr};
     uint64_t capacity = 0;
     bool host_store = false;   // arenas in pinned, device-mapped host memory (QS_FLAG_HOST_STORE)
+    bool staged = true;        // tile passes prefetch payloads with bulk copies (staged_pass_kernel)
     unsigned long long *counters = nullptr;  // [0..1] bump, [2..4] stats, [5] init scratch, [6] header-pass bytes, [7] diagonal-pass total
     uint8_t *mask = nullptr;
     uint32_t *block_nz = nullptr;
@@ -811,6 +952,10 @@ struct qs_state {
         if (sweeps_dev) cudaFree(sweeps_dev);
         if (ops_dev) cudaFree(ops_dev);
         if (pool_dev) cudaFree(pool_dev);
+        drop_tail();
+        if (tail_stats) cudaFree(tail_stats);
+        if (full_dev) cudaFree(full_dev);
+        if (full_host) cudaFreeHost(full_host);
         if (history_dev) cudaFree(history_dev);
         for (auto e : pass_ev) cudaEventDestroy(e);
         if (error_dev) cudaFree(error_dev);
@@ -912,6 +1057,10 @@ qs_status qs_create(qs_state **out, uint32_t n, uint32_t block_size, qs_dtype dt
     if (env_int("QOMPSIM_HOST_STORE", 0)) flags |= QS_FLAG_HOST_STORE;
     h->flags = flags;
     h->host_store = (flags & QS_FLAG_HOST_STORE) != 0;
+    // the host-store arenas are read chunk by chunk with cp.async (pass_kernel);
+    // QOMPSIM_STAGED_PASS=0 selects that kernel for HBM stores too
+    h->staged = !h->host_store && env_int("QOMPSIM_STAGED_PASS", 1) != 0;
+    h->merge_tail = env_int("QOMPSIM_MERGE_TAIL", 1) != 0;
     h->tile_log2 = env_int("QOMPSIM_TILE_LOG2", h->f64 ? 12 : 13);
     h->tile_log2 = std::max<int>(h->tile_log2, (int)h->C + 2);
     h->tile_log2 = std::min<int>(h->tile_log2, std::min<int>(qs::kMaxTileLog2, (int)h->C + qs::kMaxTileQubits));
@@ -1084,7 +1233,14 @@ struct HostPlan {
     std::vector<cplx> pool;
 };
 
-static qs_status plan_device_passes(qs_state *h, HostPlan *plan) {
+// The device passes of one gate sequence (already relabelled through the
+// chunk permutation P that its last pass applies), appended to *out with
+// their ops, sweeps and matrices in *plan.  A sequence of chunk permutations
+// only becomes one header pass.  *last_gate (when given) receives, per pass,
+// the number k such that gates sg[0..k) have all been applied once the pass
+// is done (passes may take commuting gates out of order).
+static qs_status emit_passes(qs_state *h, uint32_t stage, const std::vector<CGate> &sg, const HostPerm &P,
+                             HostPlan *plan, std::vector<qs_state::DevPass> *out, std::vector<size_t> *last_gate) {
     const int C = (int)h->C;
     const int jmax = std::min(h->tile_log2 - C, qs::kMaxTileQubits);
     // tiles are padded to the largest size: fewer tiles, each with its fixed
@@ -1094,10 +1250,97 @@ static qs_status plan_device_passes(qs_state *h, HostPlan *plan) {
     std::vector<qs::Sweep> &sw = plan->sw;
     std::vector<qs::ROp> &ops = plan->ops;
     std::vector<cplx> &pool = plan->pool;
-    kg.clear();
-    sw.clear();
-    ops.clear();
-    pool.clear();
+    if (sg.empty()) {  // only chunk permutations: one header pass does the sequence
+        qs_state::DevPass dp{};
+        dp.stage = stage;
+        dp.kind = 1;
+        dp.first = dp.final = true;
+        dp.perm = P.device();
+        if (std::getenv("QOMPSIM_DEBUG_PLAN")) printf("stage %u: header permutation only\n", stage);
+        out->push_back(dp);
+        if (last_gate) last_gate->push_back(0);
+        return QS_OK;
+    }
+    std::vector<uint32_t> ids(sg.size());
+    for (size_t i = 0; i < ids.size(); ++i) ids[i] = (uint32_t)i;
+    std::vector<char> placed_mark(sg.size(), 0);
+    auto pl = env_int("QOMPSIM_DAG_PLAN", 1) ? plan_passes_dag(ids, sg, C, jmax, jmin, C, (int)h->B)
+                                             : plan_passes(ids, sg, C, jmax, jmin, C, (int)h->B);
+    for (size_t p = 0; p < pl.size(); ++p) {
+        qs_state::DevPass dp{};
+        dp.stage = stage;
+        dp.j = (int)pl[p].tile.size();
+        if (dp.j > qs::kMaxTileQubits) return fail(h, QS_ERR_ARG, "tile plan exceeds the tile size");
+        for (int k = 0; k < dp.j; ++k) dp.tq[k] = pl[p].tile[k] - C;
+        dp.gate_off = (uint32_t)kg.size();
+        dp.ngates = (uint32_t)pl[p].gates.size();
+        dp.first = p == 0;
+        dp.final = p + 1 == pl.size();
+        dp.kind = 0;
+        dp.perm = dp.final ? P.device() : identity_perm();
+        for (uint32_t gi : pl[p].gates) kg.push_back(to_kgate(sg[gi], pl[p].tile, C));
+        if (last_gate) {
+            // gates of sg applied once this pass is done: every gate below the
+            // lowest index not yet placed (passes may take gates out of order)
+            size_t upto = last_gate->empty() ? 0 : last_gate->back();
+            for (uint32_t gi : pl[p].gates) placed_mark[gi] = 1;
+            while (upto < sg.size() && placed_mark[upto]) ++upto;
+            last_gate->push_back(upto);
+        }
+        const int RB = qs::kRegBits;
+        dp.rb = RB;
+        auto swp = plan_sweeps(kg, dp.gate_off, kg.size(), C + dp.j, RB);
+        const size_t op0 = ops.size();
+        std::vector<RawOp> raw;
+        std::vector<cplx> rpool;
+        build_ops(kg, dp.gate_off, swp, RB, &raw, &rpool);
+        std::vector<qs::Sweep> merged;
+        merge_diagonal_ops(swp, 0, &raw, &rpool, &merged);
+        swp.swap(merged);
+        std::vector<int> outer;
+        if (!finalize_ops(raw, rpool, C + dp.j, &outer, &ops, &pool))
+            return fail(h, QS_ERR_ARG, "a pass needs more outer selector qubits than the planner allows");
+        dp.nouter = (int)outer.size();
+        for (size_t i = 0; i < outer.size(); ++i) dp.outer_q[i] = (int8_t)outer[i];
+        dp.op_off = (uint32_t)op0;
+        dp.sweep_off = (uint32_t)sw.size();
+        // a pass of pure register moves carries codes through the tile
+        dp.code_moves = env_int("QOMPSIM_CODE_MOVES", 1) != 0 && ops.size() > op0;
+        for (size_t o = op0; o < ops.size() && dp.code_moves; ++o) {
+            const int c = ops[o].code;
+            dp.code_moves = (c >= qs::OPC_X && c < qs::OPC_X + 8) || (c >= qs::OPC_SWAP && c < qs::OPC_SWAP + 64);
+        }
+        if (std::getenv("QOMPSIM_DEBUG_PLAN")) {
+            int kinds[5] = {0, 0, 0, 0, 0}, sel = 0, half = 0, moves = 0;
+            for (size_t o = op0; o < ops.size(); ++o) {
+                const int c = ops[o].code;
+                const int kind = c == qs::OPC_SCALAR ? 0 : c < qs::OPC_M2 ? 1 : c < qs::OPC_D4 ? 2
+                               : c < qs::OPC_M4 ? 3 : 4;
+                ++kinds[kind];
+                sel += ops[o].nsel;
+                half += (c >= qs::OPC_D2H && c < qs::OPC_M2) || (c >= qs::OPC_D4H && c < qs::OPC_M4);
+                moves += (c >= qs::OPC_X && c < qs::OPC_D4) || c >= qs::OPC_SWAP;
+            }
+            printf("stage %u pass %zu: j=%d gates=%u sweeps=%zu ops=%zu (scalar %d d2 %d m2 %d d4 %d m4 %d, "
+                   "half-diagonal %d, moves %d, selectors %d, outer %d)%s tile=[", stage, p, dp.j, dp.ngates,
+                   swp.size(), ops.size() - op0, kinds[0], kinds[1], kinds[2], kinds[3], kinds[4], half, moves,
+                   sel, dp.nouter, dp.final && !P.identity() ? " +perm" : "");
+            for (int t : pl[p].tile) printf(" %d", t);
+            printf(" ]\n");
+        }
+        dp.nsweeps = (uint32_t)swp.size();
+        sw.insert(sw.end(), swp.begin(), swp.end());
+        out->push_back(dp);
+    }
+    return QS_OK;
+}
+
+static qs_status plan_device_passes(qs_state *h, HostPlan *plan) {
+    const int C = (int)h->C;
+    plan->kg.clear();
+    plan->sw.clear();
+    plan->ops.clear();
+    plan->pool.clear();
     h->passes.clear();
     const bool permute = env_int("QOMPSIM_PERMUTE_CHUNKS", 1) != 0;
     for (uint32_t s = 0; s < h->stages.size(); ++s) {
@@ -1106,109 +1349,103 @@ static qs_status plan_device_passes(qs_state *h, HostPlan *plan) {
         std::vector<CGate> sg;
         HostPerm P((int)(h->n - h->C));
         stage_relabel(h->cgates, h->stages[s], C, permute, &sg, &P);
-        if (sg.empty()) {  // only chunk permutations: one header pass does the stage
-            qs_state::DevPass dp{};
-            dp.stage = s;
-            dp.kind = 1;
-            dp.first = dp.final = true;
-            dp.perm = P.device();
-            if (std::getenv("QOMPSIM_DEBUG_PLAN")) printf("stage %u: header permutation only\n", s);
-            h->passes.push_back(dp);
-            continue;
-        }
-        std::vector<uint32_t> ids(sg.size());
-        for (size_t i = 0; i < ids.size(); ++i) ids[i] = (uint32_t)i;
-        auto pl = plan_passes(ids, sg, C, jmax, jmin, C, (int)h->B);
-        for (size_t p = 0; p < pl.size(); ++p) {
-            qs_state::DevPass dp{};
-            dp.stage = s;
-            dp.j = (int)pl[p].tile.size();
-            if (dp.j > qs::kMaxTileQubits) return fail(h, QS_ERR_ARG, "tile plan exceeds the tile size");
-            for (int k = 0; k < dp.j; ++k) dp.tq[k] = pl[p].tile[k] - C;
-            dp.gate_off = (uint32_t)kg.size();
-            dp.ngates = (uint32_t)pl[p].gates.size();
-            dp.first = p == 0;
-            dp.final = p + 1 == pl.size();
-            dp.kind = 0;
-            dp.perm = dp.final ? P.device() : identity_perm();
-            for (uint32_t gi : pl[p].gates) kg.push_back(to_kgate(sg[gi], pl[p].tile, C));
-            const int RB = qs::kRegBits;
-            dp.rb = RB;
-            auto swp = plan_sweeps(kg, dp.gate_off, kg.size(), C + dp.j, RB);
-            const size_t op0 = ops.size();
-            std::vector<RawOp> raw;
-            std::vector<cplx> rpool;
-            build_ops(kg, dp.gate_off, swp, RB, &raw, &rpool);
-            std::vector<qs::Sweep> merged;
-            merge_diagonal_ops(swp, 0, &raw, &rpool, &merged);
-            swp.swap(merged);
-            std::vector<int> outer;
-            if (!finalize_ops(raw, rpool, C + dp.j, &outer, &ops, &pool))
-                return fail(h, QS_ERR_ARG, "a pass needs more outer selector qubits than the planner allows");
-            dp.nouter = (int)outer.size();
-            for (size_t i = 0; i < outer.size(); ++i) dp.outer_q[i] = (int8_t)outer[i];
-            dp.op_off = (uint32_t)op0;
-            dp.sweep_off = (uint32_t)sw.size();
-            // a pass of pure register moves carries codes through the tile
-            dp.code_moves = env_int("QOMPSIM_CODE_MOVES", 1) != 0 && ops.size() > op0;
-            for (size_t o = op0; o < ops.size() && dp.code_moves; ++o) {
-                const int c = ops[o].code;
-                dp.code_moves = (c >= qs::OPC_X && c < qs::OPC_X + 8) || (c >= qs::OPC_SWAP && c < qs::OPC_SWAP + 64);
+        qs_status st = emit_passes(h, s, sg, P, plan, &h->passes, nullptr);
+        if (st != QS_OK) return st;
+    }
+    return QS_OK;
+}
+
+// The passes of stages [s0, end) planned as one gate sequence: once every
+// block is stored, no stage boundary changes the zero mask or the active
+// groups (every group is active, a stored block stays stored), so the
+// stages' gates can share passes.  stage_end_pass[s - s0] is the first pass
+// after which every gate of stages s0..s has been applied (-1: only chunk
+// permutations so far).
+static qs_status plan_tail_passes(qs_state *h, uint32_t s0, HostPlan *plan, std::vector<qs_state::DevPass> *passes,
+                                  std::vector<int> *stage_end_pass) {
+    const int C = (int)h->C;
+    plan->kg.clear();
+    plan->sw.clear();
+    plan->ops.clear();
+    plan->pool.clear();
+    passes->clear();
+    stage_end_pass->clear();
+    const bool permute = env_int("QOMPSIM_PERMUTE_CHUNKS", 1) != 0;
+    std::vector<uint32_t> ids;
+    std::vector<size_t> stage_end;  // one past the last id of each stage in `ids`
+    for (uint32_t s = s0; s < h->stages.size(); ++s) {
+        ids.insert(ids.end(), h->stages[s].begin(), h->stages[s].end());
+        stage_end.push_back(ids.size());
+    }
+    // relabel through the permutation accumulated over the whole tail, and
+    // count, per stage end, the relabelled gates before it
+    std::vector<CGate> sg;
+    HostPerm P((int)(h->n - h->C));
+    std::vector<size_t> kept_before(ids.size() + 1, 0);
+    for (size_t i = 0; i < ids.size(); ++i) {
+        std::vector<CGate> one;
+        const std::vector<uint32_t> single(1, ids[i]);
+        stage_relabel(h->cgates, single, C, permute, &one, &P);
+        sg.insert(sg.end(), one.begin(), one.end());
+        kept_before[i + 1] = sg.size();
+    }
+    std::vector<size_t> last_gate;
+    qs_status st = emit_passes(h, s0, sg, P, plan, passes, &last_gate);
+    if (st != QS_OK) return st;
+    for (size_t k = 0; k < stage_end.size(); ++k) {
+        const size_t kept = kept_before[stage_end[k]];  // relabelled gates up to this stage's end
+        int pe = -1;
+        for (size_t p = 0; p < passes->size(); ++p)
+            if ((*passes)[p].kind == 0 && last_gate[p] >= kept) {
+                pe = (int)p;
+                break;
             }
-            if (std::getenv("QOMPSIM_DEBUG_PLAN")) {
-                int kinds[5] = {0, 0, 0, 0, 0}, sel = 0, half = 0, moves = 0;
-                for (size_t o = op0; o < ops.size(); ++o) {
-                    const int c = ops[o].code;
-                    const int kind = c == qs::OPC_SCALAR ? 0 : c < qs::OPC_M2 ? 1 : c < qs::OPC_D4 ? 2
-                                   : c < qs::OPC_M4 ? 3 : 4;
-                    ++kinds[kind];
-                    sel += ops[o].nsel;
-                    half += (c >= qs::OPC_D2H && c < qs::OPC_M2) || (c >= qs::OPC_D4H && c < qs::OPC_M4);
-                    moves += (c >= qs::OPC_X && c < qs::OPC_D4) || c >= qs::OPC_SWAP;
-                }
-                printf("stage %u pass %zu: j=%d gates=%u sweeps=%zu ops=%zu (scalar %d d2 %d m2 %d d4 %d m4 %d, "
-                       "half-diagonal %d, moves %d, selectors %d, outer %d)%s tile=[", s, p, dp.j, dp.ngates,
-                       swp.size(), ops.size() - op0, kinds[0], kinds[1], kinds[2], kinds[3], kinds[4], half, moves,
-                       sel, dp.nouter, dp.final && !P.identity() ? " +perm" : "");
-                for (int t : pl[p].tile) printf(" %d", t);
-                printf(" ]\n");
-            }
-            dp.nsweeps = (uint32_t)swp.size();
-            sw.insert(sw.end(), swp.begin(), swp.end());
-            h->passes.push_back(dp);
-        }
+        if (kept == 0) pe = -1;
+        stage_end_pass->push_back(pe);
     }
     return QS_OK;
 }
 
 // Upload a host plan: op records, matrix pool, sweeps, block-to-group maps.
-static qs_status upload_device_plan(qs_state *h, const HostPlan &plan) {
+// Op records, matrix pool (in the state's precision) and sweeps of a host
+// plan into fresh device buffers (the previous ones freed).
+static qs_status upload_plan_buffers(qs_state *h, const HostPlan &plan, qs::ROp **ops_dev, void **pool_dev,
+                                     qs::Sweep **sweeps_dev) {
     const std::vector<qs::Sweep> &sw = plan.sw;
     const std::vector<qs::ROp> &ops = plan.ops;
     const std::vector<cplx> &pool = plan.pool;
-    if (h->kgates) { cudaFree(h->kgates); h->kgates = nullptr; }
-    if (h->sweeps_dev) { cudaFree(h->sweeps_dev); h->sweeps_dev = nullptr; }
-    if (h->ops_dev) { cudaFree(h->ops_dev); h->ops_dev = nullptr; }
-    if (h->pool_dev) { cudaFree(h->pool_dev); h->pool_dev = nullptr; }
+    if (*sweeps_dev) { cudaFree(*sweeps_dev); *sweeps_dev = nullptr; }
+    if (*ops_dev) { cudaFree(*ops_dev); *ops_dev = nullptr; }
+    if (*pool_dev) { cudaFree(*pool_dev); *pool_dev = nullptr; }
     if (!ops.empty()) {
-        CUDA_TRY(h, cudaMalloc(&h->ops_dev, ops.size() * sizeof(qs::ROp)));
-        CUDA_TRY(h, cudaMemcpy(h->ops_dev, ops.data(), ops.size() * sizeof(qs::ROp), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMalloc(ops_dev, ops.size() * sizeof(qs::ROp)));
+        CUDA_TRY(h, cudaMemcpy(*ops_dev, ops.data(), ops.size() * sizeof(qs::ROp), cudaMemcpyHostToDevice));
     }
     if (!pool.empty()) {
         if (h->f64) {
             auto pv = pool_as<double>(pool);
-            CUDA_TRY(h, cudaMalloc(&h->pool_dev, pv.size() * sizeof(double)));
-            CUDA_TRY(h, cudaMemcpy(h->pool_dev, pv.data(), pv.size() * sizeof(double), cudaMemcpyHostToDevice));
+            CUDA_TRY(h, cudaMalloc(pool_dev, pv.size() * sizeof(double)));
+            CUDA_TRY(h, cudaMemcpy(*pool_dev, pv.data(), pv.size() * sizeof(double), cudaMemcpyHostToDevice));
         } else {
             auto pv = pool_as<float>(pool);
-            CUDA_TRY(h, cudaMalloc(&h->pool_dev, pv.size() * sizeof(float)));
-            CUDA_TRY(h, cudaMemcpy(h->pool_dev, pv.data(), pv.size() * sizeof(float), cudaMemcpyHostToDevice));
+            CUDA_TRY(h, cudaMalloc(pool_dev, pv.size() * sizeof(float)));
+            CUDA_TRY(h, cudaMemcpy(*pool_dev, pv.data(), pv.size() * sizeof(float), cudaMemcpyHostToDevice));
         }
     }
     if (!sw.empty()) {
-        CUDA_TRY(h, cudaMalloc(&h->sweeps_dev, sw.size() * sizeof(qs::Sweep)));
-        CUDA_TRY(h, cudaMemcpy(h->sweeps_dev, sw.data(), sw.size() * sizeof(qs::Sweep), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMalloc(sweeps_dev, sw.size() * sizeof(qs::Sweep)));
+        CUDA_TRY(h, cudaMemcpy(*sweeps_dev, sw.data(), sw.size() * sizeof(qs::Sweep), cudaMemcpyHostToDevice));
     }
+    return QS_OK;
+}
+
+static qs_status upload_device_plan(qs_state *h, const HostPlan &plan) {
+    const std::vector<qs::Sweep> &sw = plan.sw;
+    const std::vector<qs::ROp> &ops = plan.ops;
+    if (h->kgates) { cudaFree(h->kgates); h->kgates = nullptr; }
+    qs_status us = upload_plan_buffers(h, plan, &h->ops_dev, &h->pool_dev, &h->sweeps_dev);
+    if (us != QS_OK) return us;
+    h->drop_tail();
     if (h->b2g_dev) { cudaFree(h->b2g_dev); h->b2g_dev = nullptr; }
     if (h->history_dev) { cudaFree(h->history_dev); h->history_dev = nullptr; }
     const size_t ns = h->stages.size();
@@ -1390,92 +1627,179 @@ qs_status qs_apply_circuit(qs_state *h) {
     if (!h->planned) return fail(h, QS_ERR_STATE, "no registered circuit: call qs_partition or qs_register_stages");
     cudaStream_t s = h->stream;
     const int C = (int)h->C;
+    const size_t ns = h->stages.size();
     if (!h->quiet()) {
         printf("# of PUs per rank: 1\n# of streams per PU: 1\n");
         fflush(stdout);
+    }
+    if (h->merge_tail && !h->full_dev) {
+        CUDA_TRY(h, cudaMalloc(&h->full_dev, sizeof(uint32_t)));
+        CUDA_TRY(h, cudaHostAlloc(&h->full_host, sizeof(uint32_t), cudaHostAllocDefault));
     }
     CUDA_TRY(h, cudaMemsetAsync(h->counters, 0, 8 * sizeof(unsigned long long), s));
     CUDA_TRY(h, cudaMemsetAsync(h->history_dev, 0, h->history_cap * sizeof(unsigned long long), s));
     CUDA_TRY(h, cudaMemsetAsync(h->error_dev, 0, sizeof(int32_t), s));
     CUDA_TRY(h, qs::launch_sum_mask_bytes(h->mask, h->block_bytes, h->nb, h->history_dev, s));
     CUDA_TRY(h, cudaEventRecord(h->ev[0], s));
-    size_t pi = 0;
     bool tile_passes = false;
-    for (uint32_t st = 0; st < h->stages.size(); ++st) {
+    uint64_t executed = 0, executed_perm = 0, executed_codes = 0;
+
+    // one device pass of stage map b2g (tile pass or chunk-header pass)
+    auto launch_one = [&](const qs_state::DevPass &dp, const uint32_t *b2g, const qs::ROp *ops_dev,
+                          const void *pool_dev, const qs::Sweep *sweeps_dev, unsigned long long *stats,
+                          cudaEvent_t e0, cudaEvent_t e1) -> qs_status {
+        ++executed;
+        if (dp.kind == 1) {
+            ++executed_perm;
+            qs::PermPassArgs pa{};
+            pa.B = (int)h->B;
+            pa.C = C;
+            pa.nchunks = h->nchunks;
+            pa.meta_in = h->meta[h->mcur];
+            pa.meta_out = h->meta[h->mcur ^ 1];
+            pa.block_to_group = b2g;
+            pa.group_active = h->group_active;
+            pa.mask = h->mask;
+            pa.first_pass = dp.first;
+            pa.final_pass = dp.final;
+            pa.block_nz = h->block_nz;
+            pa.block_bytes = h->block_acc;
+            pa.stats = h->counters + 6;
+            pa.perm = dp.perm;
+            if (e0) CUDA_TRY(h, cudaEventRecord(e0, s));
+            CUDA_TRY(h, qs::launch_perm_pass(pa, s));
+            if (e1) CUDA_TRY(h, cudaEventRecord(e1, s));
+            h->mcur ^= 1;
+            return QS_OK;
+        }
+        executed_codes += dp.code_moves ? 1 : 0;
+        const int out = h->cur ^ 1;
+        tile_passes = true;
+        CUDA_TRY(h, cudaMemsetAsync(h->counters + out, 0, sizeof(unsigned long long), s));
+        qs::PassArgs a{};
+        a.n = (int)h->n;
+        a.B = (int)h->B;
+        a.C = C;
+        a.j = dp.j;
+        for (int k = 0; k < dp.j; ++k) a.tq[k] = dp.tq[k];
+        a.n_tiles = uint64_t(1) << (h->n - C - dp.j);
+        a.ops = ops_dev + dp.op_off;
+        a.pool = pool_dev;
+        a.sweeps = sweeps_dev + dp.sweep_off;
+        a.nsweeps = (int)dp.nsweeps;
+        a.rb = dp.rb;
+        a.nouter = dp.nouter;
+        for (int k = 0; k < qs::kMaxOuterSel; ++k) a.outer_q[k] = dp.outer_q[k];
+        a.codec = h->codec;
+        a.meta_in = h->meta[h->mcur];
+        a.arena_in = h->arena[h->cur];
+        a.meta_out = h->meta[h->mcur ^ 1];
+        a.arena_out = h->arena[out];
+        a.perm = dp.perm;
+        a.bump = h->counters + out;
+        a.capacity = h->capacity;
+        a.block_to_group = b2g;
+        a.group_active = h->group_active;
+        a.mask = h->mask;
+        a.first_pass = dp.first;
+        a.final_pass = dp.final;
+        a.exact_zero = (h->flags & QS_FLAG_EXACT_ZERO_TEST) ? 1 : 0;
+        a.code_moves = dp.code_moves ? 1 : 0;
+        // complex64: passes of several sweeps measured faster with eight
+        // headers per batch, single-sweep (codec-bound) passes with four
+        a.header_batch = (!h->f64 && dp.nsweeps >= 2) ? 8 : 4;
+        a.block_nz = h->block_nz;
+        a.block_bytes = h->block_acc;
+        a.error = h->error_dev;
+        a.stats = stats;
+        a.staged = h->staged ? 1 : 0;
+        if (e0) CUDA_TRY(h, cudaEventRecord(e0, s));
+        CUDA_TRY(h, qs::launch_pass(h->f64, a, h->tile_log2, s));
+        if (e1) CUDA_TRY(h, cudaEventRecord(e1, s));
+        h->cur = out;
+        h->mcur ^= 1;
+        return QS_OK;
+    };
+
+    // whether every block is stored now (one synchronisation)
+    auto mask_full_now = [&](bool *full) -> qs_status {
+        CUDA_TRY(h, qs::launch_mask_full(h->mask, h->nb, h->full_dev, s));
+        CUDA_TRY(h, cudaMemcpyAsync(h->full_host, h->full_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(h, cudaStreamSynchronize(s));
+        *full = *h->full_host != 0;
+        return QS_OK;
+    };
+
+    int merged_from = -1;
+    size_t pi = 0;
+    for (uint32_t st = 0; st < ns; ++st) {
+        // every block stored: the remaining stages (two or more) share passes
+        if (h->merge_tail && ns - st >= 2) {
+            bool full = false;
+            qs_status q = mask_full_now(&full);
+            if (q != QS_OK) return q;
+            if (full) {
+                merged_from = (int)st;
+                break;
+            }
+        }
         const uint32_t *b2g = h->b2g_dev + (size_t)st * h->nb;
         CUDA_TRY(h, qs::launch_stage_begin(b2g, h->mask, h->nb, h->group_active, h->num_groups[st], h->block_nz,
-                                           h->block_acc, h->history_dev + h->stages.size() + 1 + st, s));
+                                           h->block_acc, h->history_dev + ns + 1 + st, s));
         for (; pi < h->passes.size() && h->passes[pi].stage == st; ++pi) {
-            const auto &dp = h->passes[pi];
-            if (dp.kind == 1) {
-                qs::PermPassArgs pa{};
-                pa.B = (int)h->B;
-                pa.C = C;
-                pa.nchunks = h->nchunks;
-                pa.meta_in = h->meta[h->mcur];
-                pa.meta_out = h->meta[h->mcur ^ 1];
-                pa.block_to_group = b2g;
-                pa.group_active = h->group_active;
-                pa.mask = h->mask;
-                pa.first_pass = dp.first;
-                pa.final_pass = dp.final;
-                pa.block_nz = h->block_nz;
-                pa.block_bytes = h->block_acc;
-                pa.stats = h->counters + 6;
-                pa.perm = dp.perm;
-                if (!h->pass_ev.empty()) CUDA_TRY(h, cudaEventRecord(h->pass_ev[2 * pi], s));
-                CUDA_TRY(h, qs::launch_perm_pass(pa, s));
-                if (!h->pass_ev.empty()) CUDA_TRY(h, cudaEventRecord(h->pass_ev[2 * pi + 1], s));
-                h->mcur ^= 1;
-                continue;
-            }
-            const int out = h->cur ^ 1;
-            tile_passes = true;
-            CUDA_TRY(h, cudaMemsetAsync(h->counters + out, 0, sizeof(unsigned long long), s));
-            qs::PassArgs a{};
-            a.n = (int)h->n;
-            a.B = (int)h->B;
-            a.C = C;
-            a.j = dp.j;
-            for (int k = 0; k < dp.j; ++k) a.tq[k] = dp.tq[k];
-            a.n_tiles = uint64_t(1) << (h->n - C - dp.j);
-            a.ops = h->ops_dev + dp.op_off;
-            a.pool = h->pool_dev;
-            a.sweeps = h->sweeps_dev + dp.sweep_off;
-            a.nsweeps = (int)dp.nsweeps;
-            a.rb = dp.rb;
-            a.nouter = dp.nouter;
-            for (int k = 0; k < qs::kMaxOuterSel; ++k) a.outer_q[k] = dp.outer_q[k];
-            a.codec = h->codec;
-            a.meta_in = h->meta[h->mcur];
-            a.arena_in = h->arena[h->cur];
-            a.meta_out = h->meta[h->mcur ^ 1];
-            a.arena_out = h->arena[out];
-            a.perm = dp.perm;
-            a.bump = h->counters + out;
-            a.capacity = h->capacity;
-            a.block_to_group = b2g;
-            a.group_active = h->group_active;
-            a.mask = h->mask;
-            a.first_pass = dp.first;
-            a.final_pass = dp.final;
-            a.exact_zero = (h->flags & QS_FLAG_EXACT_ZERO_TEST) ? 1 : 0;
-            a.code_moves = dp.code_moves ? 1 : 0;
-            // complex64: passes of several sweeps measured faster with eight
-            // headers per batch, single-sweep (codec-bound) passes with four
-            a.header_batch = (!h->f64 && dp.nsweeps >= 2) ? 8 : 4;
-            a.block_nz = h->block_nz;
-            a.block_bytes = h->block_acc;
-            a.error = h->error_dev;
-            a.stats = h->counters + 2;
-            if (!h->pass_ev.empty()) CUDA_TRY(h, cudaEventRecord(h->pass_ev[2 * pi], s));
-            CUDA_TRY(h, qs::launch_pass(h->f64, a, h->tile_log2, s));
-            if (!h->pass_ev.empty()) CUDA_TRY(h, cudaEventRecord(h->pass_ev[2 * pi + 1], s));
-            h->cur = out;
-            h->mcur ^= 1;
+            const bool prof = !h->pass_ev.empty();
+            qs_status q = launch_one(h->passes[pi], b2g, h->ops_dev, h->pool_dev, h->sweeps_dev, h->counters + 2,
+                                     prof ? h->pass_ev[2 * pi] : nullptr, prof ? h->pass_ev[2 * pi + 1] : nullptr);
+            if (q != QS_OK) return q;
         }
         CUDA_TRY(h, qs::launch_stage_end(b2g, h->group_active, h->nb, h->block_nz, h->block_acc, h->mask,
                                          h->block_bytes, h->history_dev + st + 1, s));
+    }
+    const size_t main_passes = pi;
+    size_t ntail = 0;
+    if (merged_from >= 0) {
+        if (h->tail_from != merged_from) {
+            HostPlan plan;
+            std::vector<qs_state::DevPass> tp;
+            std::vector<int> tend;
+            qs_status q = plan_tail_passes(h, (uint32_t)merged_from, &plan, &tp, &tend);
+            if (q != QS_OK) return q;
+            q = upload_plan_buffers(h, plan, &h->tail_ops_dev, &h->tail_pool_dev, &h->tail_sweeps_dev);
+            if (q != QS_OK) return q;
+            for (auto e : h->tail_ev) cudaEventDestroy(e);
+            h->tail_ev.clear();
+            if (h->flags & QS_FLAG_PROFILE) {
+                h->tail_ev.resize(2 * tp.size());
+                for (auto &e : h->tail_ev) CUDA_TRY(h, cudaEventCreate(&e));
+            }
+            if (h->tail_stats_cap < 3 * tp.size()) {
+                if (h->tail_stats) cudaFree(h->tail_stats);
+                h->tail_stats = nullptr;
+                h->tail_stats_cap = 0;
+                CUDA_TRY(h, cudaMalloc(&h->tail_stats, 3 * tp.size() * sizeof(unsigned long long)));
+                h->tail_stats_cap = 3 * tp.size();
+            }
+            h->tail_passes.swap(tp);
+            h->tail_stage_end.swap(tend);
+            h->tail_from = merged_from;
+        }
+        ntail = h->tail_passes.size();
+        // the last stage's map and group flags serve the whole tail (every
+        // group is active); its begin/end bracket the tail's passes
+        const uint32_t last = (uint32_t)ns - 1;
+        const uint32_t *b2g = h->b2g_dev + (size_t)last * h->nb;
+        CUDA_TRY(h, qs::launch_stage_begin(b2g, h->mask, h->nb, h->group_active, h->num_groups[last], h->block_nz,
+                                           h->block_acc, h->history_dev + ns + 1 + last, s));
+        CUDA_TRY(h, cudaMemsetAsync(h->tail_stats, 0, 3 * ntail * sizeof(unsigned long long), s));
+        for (size_t p = 0; p < ntail; ++p) {
+            const bool prof = !h->tail_ev.empty();
+            qs_status q = launch_one(h->tail_passes[p], b2g, h->tail_ops_dev, h->tail_pool_dev, h->tail_sweeps_dev,
+                                     h->tail_stats + 3 * p, prof ? h->tail_ev[2 * p] : nullptr,
+                                     prof ? h->tail_ev[2 * p + 1] : nullptr);
+            if (q != QS_OK) return q;
+        }
+        CUDA_TRY(h, qs::launch_stage_end(b2g, h->group_active, h->nb, h->block_nz, h->block_acc, h->mask,
+                                         h->block_bytes, h->history_dev + last + 1, s));
     }
     CUDA_TRY(h, cudaEventRecord(h->ev[1], s));
     CUDA_TRY(h, cudaStreamSynchronize(s));
@@ -1486,56 +1810,86 @@ qs_status qs_apply_circuit(qs_state *h) {
     std::vector<unsigned long long> hist(h->history_cap);
     CUDA_TRY(h, cudaMemcpy(hist.data(), h->history_dev, hist.size() * sizeof(unsigned long long),
                            cudaMemcpyDeviceToHost));
+    std::vector<unsigned long long> tstats(3 * ntail);
+    if (ntail)
+        CUDA_TRY(h, cudaMemcpy(tstats.data(), h->tail_stats, tstats.size() * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost));
     float ms = 0;
     CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
+    if (errflag == 2)
+        return fail(h, QS_ERR_TIMEOUT,
+                    "a pass gave up waiting for its staged chunk payloads (bounded wait); the state is invalid");
     if (errflag)
         return fail(h, QS_ERR_CAPACITY,
                     "compressed store overflowed its arena (" + std::to_string(h->capacity) +
                         " bytes); the state is invalid.  Set QOMPSIM_ARENA_BYTES larger.");
     if (tile_passes) h->arena_used = ctr[h->cur];
-    const size_t ns = h->stages.size();
+    // stages inside the merged tail: every block active; the stored total at
+    // a stage's end is the store written by the tail pass that applied the
+    // stage's last gate (every tail pass rewrites the whole store)
+    if (merged_from >= 0) {
+        for (size_t st = (size_t)merged_from; st + 1 < ns; ++st) {
+            hist[ns + 1 + st] = h->nb;
+            const int pe = h->tail_stage_end[st - (size_t)merged_from];
+            hist[st + 1] = pe >= 0 ? tstats[3 * (size_t)pe + 1] : hist[st];
+        }
+    }
     h->history.assign(hist.begin(), hist.begin() + ns + 1);
     uint64_t updates = 0;
     for (size_t st = 0; st < ns; ++st) updates += (uint64_t)h->stages[st].size() * hist[ns + 1 + st] << h->B;
     double pass_ms = 0, perm_ms = 0;
-    uint64_t perm_passes = 0, code_passes = 0;
-    for (size_t p = 0; p < h->passes.size(); ++p) {
-        perm_passes += h->passes[p].kind == 1 ? 1 : 0;
-        code_passes += (h->passes[p].kind == 0 && h->passes[p].code_moves) ? 1 : 0;
-    }
     const bool print_passes = std::getenv("QOMPSIM_DEBUG_PASS_MS") != nullptr;
-    for (size_t p = 0; p < h->pass_ev.size() / 2; ++p) {
+    auto account = [&](const qs_state::DevPass &dp, cudaEvent_t e0, cudaEvent_t e1, const char *tag,
+                       size_t p) -> qs_status {
         float t = 0;
-        CUDA_TRY(h, cudaEventElapsedTime(&t, h->pass_ev[2 * p], h->pass_ev[2 * p + 1]));
-        (h->passes[p].kind == 1 ? perm_ms : pass_ms) += t;
-        if (print_passes) {
-            const auto &dp = h->passes[p];
-            printf("pass %zu stage %u kind %d j %d gates %u sweeps %u codes %d ms %.3f\n", p, dp.stage, dp.kind, dp.j,
-                   dp.ngates, dp.nsweeps, dp.code_moves ? 1 : 0, t);
+        CUDA_TRY(h, cudaEventElapsedTime(&t, e0, e1));
+        (dp.kind == 1 ? perm_ms : pass_ms) += t;
+        if (print_passes)
+            printf("%spass %zu stage %u kind %d j %d gates %u sweeps %u codes %d ms %.3f\n", tag, p, dp.stage, dp.kind,
+                   dp.j, dp.ngates, dp.nsweeps, dp.code_moves ? 1 : 0, t);
+        return QS_OK;
+    };
+    if (!h->pass_ev.empty())
+        for (size_t p = 0; p < main_passes; ++p) {
+            qs_status q = account(h->passes[p], h->pass_ev[2 * p], h->pass_ev[2 * p + 1], "", p);
+            if (q != QS_OK) return q;
         }
-    }
+    if (!h->tail_ev.empty())
+        for (size_t p = 0; p < ntail; ++p) {
+            qs_status q = account(h->tail_passes[p], h->tail_ev[2 * p], h->tail_ev[2 * p + 1], "tail ", p);
+            if (q != QS_OK) return q;
+        }
     if (print_passes) fflush(stdout);
+    unsigned long long rd = ctr[2], wr = ctr[3], tiles = ctr[4];
+    for (size_t p = 0; p < ntail; ++p) {
+        rd += tstats[3 * p];
+        wr += tstats[3 * p + 1];
+        tiles += tstats[3 * p + 2];
+    }
     h->times[1] += ms / 1000.0;
-    h->st.stages = h->stages.size();
-    h->st.passes = h->passes.size();
-    h->st.bytes_read = ctr[2];
-    h->st.bytes_written = ctr[3];
-    h->st.tiles = ctr[4];
+    h->st.stages = ns;
+    h->st.passes = executed;
+    h->st.bytes_read = rd;
+    h->st.bytes_written = wr;
+    h->st.tiles = tiles;
     h->st.amp_gate_updates = updates;
-    h->st.kernel_ms = h->pass_ev.empty() ? ms : pass_ms;
+    h->st.kernel_ms = (h->pass_ev.empty() && h->tail_ev.empty()) ? ms : pass_ms;
     h->st.apply_ms = ms;
     h->st.mantissa_bits = h->codec.m;
     h->st.linear_exp = h->codec.L;
     h->st.chunk_log2 = (int32_t)h->C;
     h->st.tile_log2 = h->tile_log2;
-    h->st.perm_passes = perm_passes;
-    h->st.code_move_passes = code_passes;
+    h->st.perm_passes = executed_perm;
+    h->st.code_move_passes = executed_codes;
     h->st.perm_bytes = ctr[6];
     h->st.perm_ms = perm_ms;
+    h->st.merged_from = merged_from;
+    h->st.tail_passes = ntail;
+    h->last_tail_from = merged_from;
     if (!h->quiet()) {
         printf("Total SV bytes: %s\n", format_size(hist[0]).c_str());
         for (size_t st = 0; st < ns; ++st)
-            printf("[Stage %zu/%zu] Total SV bytes: %s\n", st, h->stages.size() - 1, format_size(hist[st + 1]).c_str());
+            printf("[Stage %zu/%zu] Total SV bytes: %s\n", st, ns - 1, format_size(hist[st + 1]).c_str());
         fflush(stdout);
     }
     return QS_OK;
@@ -2037,6 +2391,280 @@ qs_status qs_apply_diagonal_pauli_sum(qs_state *out, const qs_state *in, const u
     out->mcur ^= 1;
     out->arena_used = ctr[o];
     out->history.assign(1, total);
+    return QS_OK;
+}
+
+// ---- passes over two compressed stores (the compressed adjoint)
+// One launch of dual_pass_kernel over A and B with the tile qubits `tile`;
+// ops and sums already on the device.  Written stores switch to their other
+// arena; afterwards every block of a written store is stored.
+static qs_status dual_launch(qs_state *A, qs_state *B, const std::vector<int> &tile, const qs::DualOp *ops,
+                             int nops, bool write_a, bool b_zero, double *sums, int nslots) {
+    cudaStream_t s = A->stream;
+    const int C = (int)A->C;
+    qs::DualPassArgs d{};
+    d.n = (int)A->n;
+    d.B = (int)A->B;
+    d.C = C;
+    d.j = (int)tile.size();
+    for (int k = 0; k < d.j; ++k) d.tq[k] = tile[k] - C;
+    d.n_tiles = uint64_t(1) << (A->n - C - d.j);
+    d.ops = ops;
+    d.nops = nops;
+    d.codec = A->codec;
+    d.sums = sums;
+    d.nslots = nslots;
+    d.error = A->error_dev;
+    auto store = [&](qs_state *h, bool zero_in, bool write) {
+        qs::DualStore st{};
+        st.meta_in = zero_in ? nullptr : h->meta[h->mcur];
+        st.arena_in = h->arena[h->cur];
+        st.mask_in = h->mask;
+        st.meta_out = write ? h->meta[h->mcur ^ 1] : nullptr;
+        st.arena_out = h->arena[h->cur ^ 1];
+        st.bump = h->counters + (h->cur ^ 1);
+        st.capacity = h->capacity;
+        st.block_bytes = h->block_acc;
+        return st;
+    };
+    d.a = store(A, false, write_a);
+    d.b = store(B, b_zero, true);
+    for (qs_state *h : {A, B}) {
+        if (h == A && !write_a) continue;
+        CUDA_TRY(h, cudaMemsetAsync(h->counters + (h->cur ^ 1), 0, sizeof(unsigned long long), s));
+        CUDA_TRY(h, cudaMemsetAsync(h->block_acc, 0, h->nb * sizeof(unsigned long long), s));
+    }
+    CUDA_TRY(A, qs::launch_dual_pass(A->f64, d, s));
+    for (qs_state *h : {A, B}) {
+        if (h == A && !write_a) continue;
+        h->cur ^= 1;
+        h->mcur ^= 1;
+        CUDA_TRY(h, cudaMemsetAsync(h->mask, 1, h->nb, s));
+        CUDA_TRY(h, cudaMemcpyAsync(h->block_bytes, h->block_acc, h->nb * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToDevice, s));
+    }
+    return QS_OK;
+}
+
+// After a series of dual passes: check the error flag, record the arenas'
+// use and the stores' totals.
+static qs_status dual_finish(qs_state *A, qs_state *B, bool wrote_a) {
+    CUDA_TRY(A, cudaStreamSynchronize(A->stream));
+    int32_t errflag = 0;
+    CUDA_TRY(A, cudaMemcpy(&errflag, A->error_dev, sizeof(errflag), cudaMemcpyDeviceToHost));
+    if (errflag)
+        return fail(A, QS_ERR_CAPACITY, "a compressed store overflowed its arena in a two-store pass; set "
+                                        "QOMPSIM_ARENA_BYTES larger");
+    for (qs_state *h : {A, B}) {
+        if (h == A && !wrote_a) continue;
+        unsigned long long used = 0;
+        CUDA_TRY(h, cudaMemcpy(&used, h->counters + h->cur, sizeof(used), cudaMemcpyDeviceToHost));
+        h->arena_used = used;
+        h->history.assign(1, used + h->nchunks * sizeof(qs::ChunkMeta));
+    }
+    return QS_OK;
+}
+
+// Tile-local masks of a Pauli string for tile qubits `tile` (flip qubits
+// must lie in the tile).
+static qs::PauliTerm tile_term(uint64_t xm, uint64_t zm, const std::vector<int> &tile, int C, int n) {
+    qs::PauliTerm t{};
+    for (int q = 0; q < n; ++q) {
+        int tp = q < C ? q : -1;
+        if (q >= C) {
+            auto it = std::find(tile.begin(), tile.end(), q);
+            if (it != tile.end()) tp = C + (int)(it - tile.begin());
+        }
+        if ((xm >> q) & 1) t.xt |= 1u << tp;
+        if ((zm >> q) & 1) {
+            if (tp >= 0) t.zt |= 1u << tp;
+            else t.zo |= 1ull << q;
+        }
+    }
+    t.xg = xm;
+    t.zg = zm;
+    return t;
+}
+
+static qs_status dual_check(qs_state *A, const qs_state *B) {
+    if (!same_geometry(A, B)) return fail(A, QS_ERR_ARG, "the two states differ in qubits, block, chunk, dtype or codec");
+    if (A->stream != B->stream) return fail(A, QS_ERR_ARG, "the two states must share a stream");
+    if (A->host_store || B->host_store) return fail(A, QS_ERR_ARG, "two-store passes need HBM arenas");
+    if (A->C + std::min<int>(4, (int)A->n - (int)A->C) < qs::kRegBits)
+        return fail(A, QS_ERR_ARG, "state too small for a two-store pass");
+    return QS_OK;
+}
+
+constexpr int kDualTileLog2 = 12;
+
+qs_status qs_apply_pauli_sum(qs_state *out, qs_state *in, const uint64_t *x_masks, const uint64_t *z_masks,
+                             const double *coefs, size_t nterms) {
+    if (!out || !in) return fail(out, QS_ERR_ARG, "NULL handle");
+    if (out == in) return fail(out, QS_ERR_ARG, "out and in must be different states");
+    if (nterms && (!x_masks || !z_masks || !coefs)) return fail(out, QS_ERR_ARG, "NULL argument");
+    qs_status st = dual_check(in, out);
+    if (st != QS_OK) return fail(out, st, in->err);
+    const int C = (int)out->C, n = (int)out->n;
+    const uint64_t full = n >= 64 ? ~0ull : ((1ull << n) - 1);
+    for (size_t t = 0; t < nterms; ++t)
+        if ((x_masks[t] | z_masks[t]) & ~full) return fail(out, QS_ERR_ARG, "Pauli term acts outside the register");
+    const int jmax = std::min(kDualTileLog2 - C, n - C);
+    // terms in order, grouped so that each group's flip qubits >= C fit a tile
+    std::vector<std::vector<size_t>> groups;
+    std::vector<std::set<int>> gq;
+    for (size_t t = 0; t < nterms; ++t) {
+        std::set<int> q;
+        for (int b = C; b < n; ++b)
+            if ((x_masks[t] >> b) & 1) q.insert(b);
+        if ((int)q.size() > jmax) return fail(out, QS_ERR_ARG, "a Pauli term flips more qubits than a tile holds");
+        bool placed = false;
+        for (size_t g = 0; g < groups.size() && !placed; ++g) {
+            std::set<int> u = gq[g];
+            u.insert(q.begin(), q.end());
+            if ((int)u.size() <= jmax) {
+                gq[g] = u;
+                groups[g].push_back(t);
+                placed = true;
+            }
+        }
+        if (!placed) {
+            groups.push_back({t});
+            gq.push_back(q);
+        }
+    }
+    if (groups.empty()) groups.push_back({});
+    std::vector<qs::DualOp> ops;
+    std::vector<std::vector<int>> tiles;
+    std::vector<size_t> op_off;
+    for (size_t g = 0; g < groups.size(); ++g) {
+        std::set<int> tq = g < gq.size() ? gq[g] : std::set<int>();
+        for (int q = C; q < n && (int)tq.size() < jmax; ++q) tq.insert(q);
+        std::vector<int> tile(tq.begin(), tq.end());
+        tiles.push_back(tile);
+        op_off.push_back(ops.size());
+        for (size_t t : groups[g]) {
+            qs::DualOp o{};
+            o.kind = qs::DOP_ACCUM;
+            o.term = tile_term(x_masks[t], z_masks[t], tile, C, n);
+            o.coef[0] = coefs[2 * t];
+            o.coef[1] = coefs[2 * t + 1];
+            ops.push_back(o);
+        }
+    }
+    op_off.push_back(ops.size());
+    qs::DualOp *dops = nullptr;
+    CUDA_TRY(out, cudaMalloc(&dops, std::max<size_t>(1, ops.size()) * sizeof(qs::DualOp)));
+    struct Free { void *p; ~Free() { if (p) cudaFree(p); } } fr{dops};
+    if (!ops.empty())
+        CUDA_TRY(out, cudaMemcpyAsync(dops, ops.data(), ops.size() * sizeof(qs::DualOp), cudaMemcpyHostToDevice,
+                                      out->stream));
+    CUDA_TRY(out, cudaMemsetAsync(in->error_dev, 0, sizeof(int32_t), out->stream));
+    for (size_t g = 0; g < tiles.size(); ++g) {
+        st = dual_launch(in, out, tiles[g], dops + op_off[g], (int)(op_off[g + 1] - op_off[g]), false, g == 0,
+                         nullptr, 0);
+        if (st != QS_OK) return fail(out, st, in->err);
+    }
+    st = dual_finish(in, out, false);
+    if (st != QS_OK) return fail(out, st, in->err);
+    return QS_OK;
+}
+
+qs_status qs_adjoint(qs_state *psi, qs_state *lam, const qs_gate *gates, const int32_t *slots, const uint64_t *gen_x,
+                     const uint64_t *gen_z, size_t count, double *out, uint32_t nslots) {
+    if (!psi || !lam || (count && (!gates || !slots || !gen_x || !gen_z)) || (nslots && !out))
+        return fail(psi, QS_ERR_ARG, "NULL argument");
+    if (psi == lam) return fail(psi, QS_ERR_ARG, "psi and lam must be distinct states");
+    qs_status st = dual_check(psi, lam);
+    if (st != QS_OK) return st;
+    for (size_t i = 0; i < count; ++i)
+        if (slots[i] >= (int32_t)nslots) return fail(psi, QS_ERR_ARG, "slot index out of range");
+    const int C = (int)psi->C, n = (int)psi->n;
+    std::vector<CGate> cg(count);
+    for (size_t i = 0; i < count; ++i) {
+        std::string e;
+        if (!canonicalize(gates[i], false, psi->n, &cg[i], &e))
+            return fail(psi, QS_ERR_UNSUPPORTED_GATE, "gate " + std::to_string(i) + ": " + e);
+    }
+    // generators' flip qubits must lie in the tile too: treat them as mixing
+    for (size_t i = 0; i < count; ++i) {
+        if (slots[i] < 0) continue;
+        uint64_t covered = 0;
+        for (int b = 0; b < cg[i].nq; ++b) {
+            covered |= 1ull << cg[i].q[b];
+            if ((gen_x[i] >> cg[i].q[b]) & 1) cg[i].mix[b] = true;
+        }
+        if (gen_x[i] & ~covered) return fail(psi, QS_ERR_ARG, "a generator flips a qubit its gate does not act on");
+    }
+    const int jmax = std::min(kDualTileLog2 - C, n - C);
+    std::vector<uint32_t> ids(count);
+    for (size_t i = 0; i < count; ++i) ids[i] = (uint32_t)i;
+    auto pl = plan_passes(ids, cg, C, jmax, jmax, C, n);
+    // launches: a pass's gates, split so that each launch has at most
+    // kMaxDualSlots derivative sums
+    struct Launch {
+        std::vector<int> tile;
+        size_t op_off, nops, out_off;
+        std::vector<int32_t> local_to_global;
+    };
+    std::vector<qs::DualOp> ops;
+    std::vector<Launch> launches;
+    size_t nout = 0;
+    for (auto &p : pl) {
+        for (size_t g0 = 0; g0 < p.gates.size();) {
+            Launch L{};
+            L.tile = p.tile;
+            L.op_off = ops.size();
+            L.out_off = nout;
+            size_t g1 = g0;
+            for (; g1 < p.gates.size(); ++g1) {
+                const uint32_t gi = p.gates[g1];
+                if (slots[gi] >= 0) {
+                    if (L.local_to_global.size() >= (size_t)qs::kMaxDualSlots) break;
+                    qs::DualOp o{};
+                    o.kind = qs::DOP_SUM;
+                    o.slot = (int32_t)L.local_to_global.size();
+                    o.term = tile_term(gen_x[gi], gen_z[gi], p.tile, C, n);
+                    ops.push_back(o);
+                    L.local_to_global.push_back(slots[gi]);
+                }
+                qs::DualOp o{};
+                o.kind = qs::DOP_GATE_AB;
+                o.g = to_kgate(cg[gi], p.tile, C);
+                ops.push_back(o);
+            }
+            L.nops = ops.size() - L.op_off;
+            nout += L.local_to_global.size();
+            launches.push_back(std::move(L));
+            g0 = g1;
+        }
+    }
+    qs::DualOp *dops = nullptr;
+    double *dsum = nullptr;
+    CUDA_TRY(psi, cudaMalloc(&dops, std::max<size_t>(1, ops.size()) * sizeof(qs::DualOp)));
+    struct Free { void *p; ~Free() { if (p) cudaFree(p); } } f1{dops};
+    CUDA_TRY(psi, cudaMalloc(&dsum, std::max<size_t>(1, 2 * nout) * sizeof(double)));
+    Free f2{dsum};
+    cudaStream_t s = psi->stream;
+    if (!ops.empty())
+        CUDA_TRY(psi, cudaMemcpyAsync(dops, ops.data(), ops.size() * sizeof(qs::DualOp), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(psi, cudaMemsetAsync(dsum, 0, std::max<size_t>(1, 2 * nout) * sizeof(double), s));
+    CUDA_TRY(psi, cudaMemsetAsync(psi->error_dev, 0, sizeof(int32_t), s));
+    for (const Launch &L : launches) {
+        st = dual_launch(psi, lam, L.tile, dops + L.op_off, (int)L.nops, true, false, dsum + 2 * L.out_off,
+                         (int)L.local_to_global.size());
+        if (st != QS_OK) return st;
+    }
+    std::vector<double> h(2 * nout);
+    if (nout) CUDA_TRY(psi, cudaMemcpyAsync(h.data(), dsum, 2 * nout * sizeof(double), cudaMemcpyDeviceToHost, s));
+    st = dual_finish(psi, lam, true);
+    if (st != QS_OK) return st;
+    std::vector<double> acc(2 * (size_t)nslots, 0.0);
+    for (const Launch &L : launches)
+        for (size_t k = 0; k < L.local_to_global.size(); ++k) {
+            acc[2 * L.local_to_global[k]] += h[2 * (L.out_off + k)];
+            acc[2 * L.local_to_global[k] + 1] += h[2 * (L.out_off + k) + 1];
+        }
+    for (size_t i = 0; i < acc.size(); ++i) out[i] = acc[i];
     return QS_OK;
 }
 

@@ -158,12 +158,14 @@ struct PassArgs {
     int32_t header_batch;               // complex64: chunk headers a warp loads at once (4 or 8)
     uint32_t *block_nz;                 // final pass: any non-zero in block
     unsigned long long *block_bytes;    // final pass: stored bytes of block
-    int32_t *error;                     // 1 = arena overflow
+    int32_t *error;                     // 1 = arena overflow, 2 = a bounded wait for staged payloads gave up
     unsigned long long *stats;          // [0] bytes read [1] bytes written [2] tiles
     ChunkPerm perm;                     // chunk c of the pass is stored as chunk perm(c)
     int32_t nouter;                     // outer selector qubits of the pass
     int8_t outer_q[kMaxOuterSel];       // their global qubit indices (bit nb + i of W)
     DiagSum diag;                       // nterms > 0: multiply by a diagonal Pauli sum after the sweeps
+    int32_t staged;                     // 1: staged_pass_kernel (payloads prefetched with bulk copies),
+                                        // 0: pass_kernel (payloads copied chunk by chunk; the host-store arenas)
 };
 
 // A pass that only permutes chunk headers: meta_out[perm(c)] = meta_in[c]
@@ -249,7 +251,49 @@ struct AdjPassArgs {
     int32_t nslots;
 };
 
+// A pass over two compressed stores A and B of one geometry (the compressed
+// adjoint: A = psi, B = lambda).  Per tile both are decoded, the ops run in
+// order, and the stores are re-encoded into their output arenas.
+enum : int32_t {
+    DOP_GATE_A = 0,     // apply g to A
+    DOP_GATE_B = 1,     // apply g to B
+    DOP_GATE_AB = 2,    // apply g to both
+    DOP_SUM = 3,        // sums[slot] += sum_x conj(B[x ^ xt]) (-1)^{|x & z|} A[x]
+    DOP_ACCUM = 4       // B[x] += coef (-1)^{|y & z|} A[y], y = x ^ xt
+};
+struct DualOp {
+    KGate g;
+    PauliTerm term;     // xt, zt tile-local, zo outer
+    double coef[2];
+    int32_t kind;
+    int32_t slot;
+};
+constexpr int kMaxDualSlots = 128;
+struct DualStore {
+    const ChunkMeta *meta_in;   // NULL: the store starts the pass at zero (B only)
+    const uint32_t *arena_in;
+    const uint8_t *mask_in;     // blocks stored at the start of the pass
+    ChunkMeta *meta_out;        // NULL: not written (A only, when no op changes it)
+    uint32_t *arena_out;
+    unsigned long long *bump;
+    uint64_t capacity;
+    unsigned long long *block_bytes;  // per block: stored bytes written (accumulated)
+};
+struct DualPassArgs {
+    int32_t n, B, C, j;
+    int32_t tq[kMaxTileQubits];
+    uint64_t n_tiles;
+    const DualOp *ops;
+    int32_t nops;
+    CodecParams codec;
+    DualStore a, b;
+    double *sums;               // 2 doubles per slot
+    int32_t nslots;
+    int32_t *error;             // 1 = an output arena overflowed
+};
+
 // ---- launchers (kernels.cu); all asynchronous on `stream` ----
+cudaError_t launch_dual_pass(bool f64, const DualPassArgs &a, cudaStream_t stream);
 cudaError_t launch_adjoint_pass(bool f64, const AdjPassArgs &a, cudaStream_t stream);
 cudaError_t launch_dense_transition(bool f64, const void *bra, const void *ket, int n, const PauliTerm *terms,
                                     int nterms, double *out, cudaStream_t stream);
@@ -260,6 +304,8 @@ cudaError_t launch_expect(bool f64, const ExpectArgs &a, cudaStream_t stream);
 cudaError_t launch_dense_expect(bool f64, const void *state, int n, const PauliTerm *terms, int nterms, double *out,
                                 cudaStream_t stream);
 cudaError_t launch_pass(bool f64, const PassArgs &a, int tile_log2, cudaStream_t stream);
+// Shared memory of one staged_pass_kernel CTA for tiles of 2^(C+j) amplitudes.
+size_t staged_pass_smem_bytes(bool f64, int C, int j, uint32_t nblocks);
 cudaError_t launch_perm_pass(const PermPassArgs &a, cudaStream_t stream);
 cudaError_t launch_dense_pass(bool f64, const DensePassArgs &a, int tile_log2, cudaStream_t stream);
 cudaError_t launch_pergate(bool f64, void *state, int n, const KGate *gate_dev, cudaStream_t stream);
@@ -301,6 +347,8 @@ cudaError_t launch_encode(bool f64, const double *vals, int B, int C, CodecParam
 cudaError_t launch_dense_norm(bool f64, const void *state, uint64_t dim, double *out, cudaStream_t stream);
 cudaError_t launch_dense_to_c128(bool f64, const void *state, uint64_t dim, double *out, cudaStream_t stream);
 cudaError_t launch_c128_to_dense(bool f64, const double *in, uint64_t dim, void *state, cudaStream_t stream);
+// *out = non-zero when every one of the nb blocks is stored, else 0.
+cudaError_t launch_mask_full(const uint8_t *mask, uint32_t nb, uint32_t *out, cudaStream_t stream);
 cudaError_t launch_sum_mask_bytes(const uint8_t *mask, const unsigned long long *block_bytes, uint32_t nb,
                                   unsigned long long *out, cudaStream_t stream);
 

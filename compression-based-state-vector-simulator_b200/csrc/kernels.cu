@@ -371,7 +371,9 @@ __device__ __forceinline__ void cp_async_wait() {
 template <typename R, typename Slot = LinearSlot, bool kCodes = false>
 __device__ __forceinline__ void unpack_chunk(const ChunkMeta md, int per_lane, CodecParams p, R *comp,
                                              const uint32_t *wstage, int lane, Slot slot = Slot()) {
-    const uint32_t w = md.width;
+    // a width above 32 never comes from a pass or a checked import; clamped so
+    // that no header can make the unpack read past its chunk's staged rows
+    const uint32_t w = md.width > 32 ? 32u : md.width;
     if (w == 0) {
         const R v = kCodes ? code_as_value(md.base, R()) : dequantize_hot(md.base, p, R());
         for (int i = 0; i < per_lane; ++i) comp[slot(lane + 32 * i)] = v;
@@ -751,6 +753,377 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
     }
 }
 
+// ------------------------------------------------------------ staged pass kernel
+// The same fused pass as pass_kernel, restructured so that no global-memory
+// latency sits on a tile's critical path:
+//   * persistent CTAs of kStagedThreads threads walk their tiles in order;
+//     while a CTA works on tile t, the compressed payload of its next tile is
+//     already streaming into a shared-memory double buffer with 1-D bulk
+//     asynchronous copies (cp.async.bulk, one per chunk, completion counted
+//     in bytes on an mbarrier), and the chunk headers of the tile after that
+//     with 16-byte cp.async copies;
+//   * which blocks belong to an active group and which were stored at the
+//     start of the stage are read once per CTA into shared-memory bitmasks;
+//   * the error flag is loaded at the start of a tile and tested only at the
+//     tile's output reservation.
+// Decode, sweeps, quantisation, reservation and packing are pass_kernel's.
+// The copies read this GPU's own memory only (no cluster multicast).
+constexpr int kStagedThreads = 256;
+// Blocks whose activity / stored bits are kept in shared memory (two bitmasks
+// of this many bits); passes over more blocks read them from global memory.
+constexpr uint32_t kMaxSmemBlocks = 1u << 16;
+// Iterations of a bounded mbarrier wait (each try_wait itself suspends for a
+// while before it returns false).
+constexpr uint32_t kMbarSpinLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n"
+        " .reg .pred p;\n"
+        " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for the phase of `bar` with the given parity to complete; false when
+// it has not after kMbarSpinLimit tries.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kMbarSpinLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// 1-D bulk copy global -> this CTA's shared memory, completion (in bytes) on
+// `bar`.  Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+// Shared-memory layout of staged_pass_kernel (byte offsets; every region
+// 128-byte aligned).
+struct StagedLayout {
+    size_t tile, buf0, buf1, hdr0, hdr1, poff0, poff1, base, width, nz, off, act, sto, total;
+};
+
+__host__ __device__ inline size_t align128(size_t x) { return (x + 127) / 128 * 128; }
+
+// stage_bytes: one tile's largest payload (every chunk at width 32) plus one
+// 128-byte row read ahead by the last chunk's unpack.
+__host__ __device__ inline size_t staged_stage_bytes(int C, int j) {
+    return ((size_t)1 << j) * payload_bytes(C, 32) + 128;
+}
+
+__host__ __device__ inline StagedLayout staged_layout(bool f64, int C, int j, uint32_t mask_words) {
+    StagedLayout L{};
+    const size_t nch = (size_t)1 << j;
+    size_t o = 0;
+    L.tile = o;  o += align128((f64 ? 16 : 8) << (C + j));
+    const size_t stage = align128(staged_stage_bytes(C, j));
+    L.buf0 = o;  o += stage;
+    L.buf1 = o;  o += stage;
+    L.hdr0 = o;  o += align128(sizeof(ChunkMeta) * nch);
+    L.hdr1 = o;  o += align128(sizeof(ChunkMeta) * nch);
+    L.poff0 = o; o += align128(4 * nch);
+    L.poff1 = o; o += align128(4 * nch);
+    L.base = o;  o += align128(4 * nch);
+    L.width = o; o += align128(4 * nch);
+    L.nz = o;    o += align128(4 * nch);
+    L.off = o;   o += align128(8 * nch);
+    L.act = o;   o += align128(4 * (size_t)mask_words);
+    L.sto = o;   o += align128(4 * (size_t)mask_words);
+    L.total = o;
+    return L;
+}
+
+template <typename R, bool kCodes>
+__global__ void __launch_bounds__(kStagedThreads, 1) staged_pass_kernel(const PassArgs a) {
+    using T = typename Cplx<R>::T;
+    extern __shared__ __align__(128) unsigned char staged_smem[];
+    unsigned char *smem = staged_smem;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ unsigned long long s_tile_off, s_next, s_slab_end;
+    __shared__ int s_flag;
+    __shared__ int32_t s_tq[kMaxTileQubits];
+    __shared__ int8_t s_oq[kMaxOuterSel];
+
+    const int C = a.C, j = a.j, nb = C + j;
+    const int nchunks = 1 << j;
+    const int ncomp = 2 << C;
+    const int per_lane = ncomp >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int blk_shift = a.B - C;
+    const int swm = swizzle_mask<R>(C);
+    const uint32_t nblk = 1u << (a.n - a.B);
+    const bool smask = nblk <= kMaxSmemBlocks;
+    const uint32_t mask_words = smask ? (nblk + 31) / 32 : 0;
+    const StagedLayout Ly = staged_layout(sizeof(R) == 8, C, j, mask_words);
+
+    T *tile = reinterpret_cast<T *>(smem + Ly.tile);
+    // the two slots of each double-buffered region, by pointer arithmetic
+    // (no arrays indexed at run time, which would live in local memory)
+    auto buf = [&](int s) { return reinterpret_cast<uint32_t *>(smem + Ly.buf0 + (size_t)s * (Ly.buf1 - Ly.buf0)); };
+    auto hdr = [&](int s) { return reinterpret_cast<ChunkMeta *>(smem + Ly.hdr0 + (size_t)s * (Ly.hdr1 - Ly.hdr0)); };
+    auto poff = [&](int s) { return reinterpret_cast<uint32_t *>(smem + Ly.poff0 + (size_t)s * (Ly.poff1 - Ly.poff0)); };
+    int32_t *s_base = reinterpret_cast<int32_t *>(smem + Ly.base);
+    uint32_t *s_width = reinterpret_cast<uint32_t *>(smem + Ly.width);
+    uint32_t *s_nz = reinterpret_cast<uint32_t *>(smem + Ly.nz);
+    unsigned long long *s_off = reinterpret_cast<unsigned long long *>(smem + Ly.off);
+    uint32_t *s_act = reinterpret_cast<uint32_t *>(smem + Ly.act);
+    uint32_t *s_sto = reinterpret_cast<uint32_t *>(smem + Ly.sto);
+
+    if (threadIdx.x < kMaxTileQubits) s_tq[threadIdx.x] = a.tq[threadIdx.x];
+    if (threadIdx.x < kMaxOuterSel) s_oq[threadIdx.x] = a.outer_q[threadIdx.x];
+    if (threadIdx.x == 0) {
+        s_next = 0;
+        s_slab_end = 0;
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    // block bitmasks: bit b of s_act = block b's group is active this stage,
+    // of s_sto = block b was stored when the stage began
+    for (uint32_t b0 = (uint32_t)warp * 32; b0 < mask_words * 32; b0 += (uint32_t)nwarps * 32) {
+        const uint32_t b = b0 + lane;
+        const bool act = b < nblk && a.group_active[a.block_to_group[b]] != 0;
+        const bool sto = b < nblk && a.mask[b] != 0;
+        const uint32_t wa = __ballot_sync(0xffffffffu, act), ws = __ballot_sync(0xffffffffu, sto);
+        if (lane == 0) {
+            s_act[b0 >> 5] = wa;
+            s_sto[b0 >> 5] = ws;
+        }
+    }
+    __syncthreads();
+
+    auto block_active = [&](uint64_t blk) -> bool {
+        return smask ? ((s_act[blk >> 5] >> (blk & 31)) & 1u) != 0 : a.group_active[a.block_to_group[blk]] != 0;
+    };
+    auto block_stored = [&](uint64_t blk) -> bool {
+        return smask ? ((s_sto[blk >> 5] >> (blk & 31)) & 1u) != 0 : a.mask[blk] != 0;
+    };
+    // this CTA's first tile at or after t (t in its sequence) whose group is
+    // active; ~0 when none is left (uniform across the CTA)
+    auto next_active = [&](uint64_t t) -> uint64_t {
+        for (; t < a.n_tiles; t += gridDim.x)
+            if (block_active(insert_zero_bits(t, s_tq, j) >> blk_shift)) return t;
+        return ~0ull;
+    };
+    // headers of tile t into hdr(s) (16-byte cp.async copies; a chunk of a
+    // block that is not stored at the start of the stage reads as zeros on
+    // the stage's first pass and its header is not read)
+    auto load_headers = [&](uint64_t t, int s) {
+        const uint64_t cb = insert_zero_bits(t, s_tq, j);
+        for (int c = threadIdx.x; c < nchunks; c += blockDim.x) {
+            const uint64_t chunk = cb | deposit_bits((uint32_t)c, s_tq, j);
+            if (!a.first_pass || block_stored(chunk >> blk_shift)) cp_async16(&hdr(s)[c], &a.meta_in[chunk]);
+            else hdr(s)[c] = ChunkMeta{0, 0, 0};
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    // warp 0: payload copies of the tile whose headers are in hdr(s) into
+    // buf(s); chunk c's payload lands at byte poff(s)[c]
+    auto issue_payload = [&](int s) {
+        uint32_t run = 0;
+        for (int c0 = 0; c0 < nchunks; c0 += 32) {
+            const int c = c0 + lane;
+            const uint32_t w = c < nchunks ? hdr(s)[c].width : 0u;
+            const uint32_t sz = (uint32_t)payload_bytes(C, w > 32 ? 32u : w);
+            uint32_t incl = sz;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t2 = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t2;
+            }
+            if (c < nchunks) poff(s)[c] = run + incl - sz;
+            run += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        // the buffer was last read by generic loads (the decode of two tiles ago)
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        if (lane == 0) mbar_arrive_expect_tx(&s_bar[s], run);
+        __syncwarp();
+        for (int c = lane; c < nchunks; c += 32) {
+            const ChunkMeta md = hdr(s)[c];
+            const uint32_t sz = (uint32_t)payload_bytes(C, md.width > 32 ? 32u : md.width);
+            if (sz) bulk_copy_g2s(reinterpret_cast<unsigned char *>(buf(s)) + poff(s)[c],
+                                  reinterpret_cast<const unsigned char *>(a.arena_in) + md.offset, sz, &s_bar[s]);
+        }
+    };
+
+    unsigned long long rd = 0, wr = 0, ntiles = 0;
+    uint32_t phase = 0u;    // bit s: parity of the next phase of s_bar[s]
+    uint32_t pending = 0u;  // bit s: a payload fill of buf(s) not yet waited for
+
+    uint64_t cur = next_active(blockIdx.x);
+    uint64_t nxt = cur == ~0ull ? ~0ull : next_active(cur + gridDim.x);
+    if (cur != ~0ull) {
+        load_headers(cur, 0);
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        __syncthreads();
+        if (warp == 0) issue_payload(0);
+        pending |= 1u;
+        if (nxt != ~0ull) load_headers(nxt, 1);
+    }
+
+    for (int it = 0; cur != ~0ull; ++it) {
+        const int slot = it & 1;
+        const uint64_t chunk_base = insert_zero_bits(cur, s_tq, j);
+        // error flag of this tile, tested at its reservation
+        int err_seen = 0;
+        if (threadIdx.x == 0) err_seen = *reinterpret_cast<volatile int32_t *>(a.error);
+        // headers of the next tile (issued one tile ago) and this tile's payload
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        const bool mine = mbar_wait_bounded(&s_bar[slot], (phase >> slot) & 1u);
+        const bool ok = __syncthreads_and(mine) != 0;  // uniform: every thread saw the fill complete
+        if (!ok) {
+            if (threadIdx.x == 0) atomicExch(a.error, 2);
+            break;
+        }
+        phase ^= 1u << slot;
+        pending &= ~(1u << slot);
+        ++ntiles;
+        const uint64_t nxt2 = nxt == ~0ull ? ~0ull : next_active(nxt + gridDim.x);
+        if (nxt != ~0ull) {
+            if (warp == 0) issue_payload(slot ^ 1);
+            pending |= 1u << (slot ^ 1);
+        }
+
+        // ---- decode this tile's chunks from buf(slot) into the value tile
+        for (int c = warp; c < nchunks; c += nwarps) {
+            const ChunkMeta md = hdr(slot)[c];
+            unpack_chunk<R, TileSlot<R>, kCodes>(md, per_lane, a.codec, reinterpret_cast<R *>(tile),
+                                                 buf(slot) + (poff(slot)[c] >> 2), lane, TileSlot<R>{c << C, swm});
+            if (lane == 0) {
+                const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
+                if (!a.first_pass || block_stored(chunk >> blk_shift))
+                    rd += payload_bytes(C, md.width) + sizeof(ChunkMeta);
+            }
+        }
+        __syncthreads();
+        // hdr(slot) is free: the headers of the tile after the next one
+        if (nxt2 != ~0ull) load_headers(nxt2, slot);
+
+        // ---- gates
+        tile_sweeps<R, kRegBits>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool),
+                                 outer_word(chunk_base << C, s_oq, a.nouter));
+        if constexpr (!kCodes) {
+            // buf(slot) is free here: it holds the tile's term coefficients
+            if (a.diag.nterms)
+                tile_diag_sum<R>(tile, nb, swm, a.diag, chunk_base << C, reinterpret_cast<double *>(buf(slot)));
+        }
+
+        // ---- quantise (codes replace values in shared memory)
+        for (int c = warp; c < nchunks; c += nwarps) {
+            R *comp = reinterpret_cast<R *>(tile) + (size_t)c * ncomp;
+            int32_t base;
+            uint32_t width;
+            bool nz;
+            quantize_chunk<R, TileSlot<R>, kCodes>(reinterpret_cast<R *>(tile), per_lane, a.codec, a.exact_zero != 0,
+                                                   lane, &base, &width, &nz, TileSlot<R>{c << C, swm},
+                                                   reinterpret_cast<int32_t *>(comp));
+            if (lane == 0) {
+                s_base[c] = base;
+                s_width[c] = width;
+                s_nz[c] = nz ? 1u : 0u;
+            }
+        }
+        __syncthreads();
+
+        // ---- reserve the tile's output bytes (warp 0 scans the chunk sizes)
+        if (warp == 0) {
+            const int per = (nchunks + 31) >> 5;
+            const int c0 = lane * per;
+            unsigned long long mine = 0;
+            for (int c = c0; c < c0 + per && c < nchunks; ++c) mine += payload_bytes(C, s_width[c]);
+            unsigned long long incl = mine;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long t2 = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t2;
+            }
+            unsigned long long run = incl - mine;
+            for (int c = c0; c < c0 + per && c < nchunks; ++c) {
+                s_off[c] = run;
+                run += payload_bytes(C, s_width[c]);
+            }
+            const unsigned long long total = __shfl_sync(0xffffffffu, incl, 31);
+            if (lane == 0) {
+                unsigned long long off = s_next;
+                s_flag = err_seen;
+                if (!err_seen && (a.slab == 0 || off + total > s_slab_end)) {
+                    const unsigned long long want = total > a.slab ? total : a.slab;
+                    off = atomicAdd(a.bump, want);
+                    if (off + want > a.capacity) {
+                        atomicExch(a.error, 1);
+                        s_flag = 1;
+                    }
+                    s_slab_end = off + want;
+                }
+                s_tile_off = off;
+                s_next = off + total;
+                if (!s_flag) wr += total + (unsigned long long)nchunks * sizeof(ChunkMeta);
+            }
+        }
+        __syncthreads();
+        if (s_flag) break;
+
+        // ---- pack and store
+        for (int c = warp; c < nchunks; c += nwarps) {
+            const uint64_t chunk = apply_perm(a.perm, chunk_base | deposit_bits((uint32_t)c, s_tq, j));
+            const int32_t *codes = reinterpret_cast<const int32_t *>(reinterpret_cast<R *>(tile) + (size_t)c * ncomp);
+            const unsigned long long off = s_tile_off + s_off[c];
+            const uint32_t w = s_width[c];
+            pack_chunk(codes, per_lane, s_base[c], w, a.arena_out + (off >> 2), lane);
+            if (lane == 0) {
+                ChunkMeta md;
+                md.offset = off;
+                md.base = s_base[c];
+                md.width = w;
+                a.meta_out[chunk] = md;
+                if (a.final_pass) {
+                    const uint64_t blk = chunk >> blk_shift;
+                    if (s_nz[c]) atomicOr(&a.block_nz[blk], 1u);
+                    atomicAdd(&a.block_bytes[blk], (unsigned long long)(payload_bytes(C, w) + sizeof(ChunkMeta)));
+                }
+            }
+        }
+        cur = nxt;
+        nxt = nxt2;
+    }
+    // a CTA that stopped early still has copies in flight into its shared
+    // memory: wait for them (bounded) before it exits
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    for (int s = 0; s < 2; ++s)
+        if ((pending >> s) & 1u) (void)mbar_wait_bounded(&s_bar[s], (phase >> s) & 1u);
+    __syncthreads();
+    if (rd) atomicAdd(&a.stats[0], rd);
+    if (threadIdx.x == 0) {
+        if (wr) atomicAdd(&a.stats[1], wr);
+        if (ntiles) atomicAdd(&a.stats[2], ntiles);
+    }
+}
+
 // ------------------------------------------------------------ header permutation pass
 __global__ void perm_pass_kernel(const PermPassArgs a) {
     const int blk_shift = a.B - a.C;
@@ -922,6 +1295,13 @@ __global__ void stage_end_kernel(const uint32_t *block_to_group, const uint8_t *
     }
     for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
     if ((threadIdx.x & 31) == 0 && bytes) atomicAdd(history_slot, bytes);
+}
+
+// *out stays non-zero only when every block of the mask is stored (the
+// caller sets it non-zero first).
+__global__ void mask_full_kernel(const uint8_t *mask, uint32_t nb, uint32_t *out) {
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
+        if (!mask[b]) *out = 0u;
 }
 
 __global__ void sum_mask_bytes_kernel(const uint8_t *mask, const unsigned long long *bb, uint32_t nb,
@@ -1433,6 +1813,172 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_pass_kernel(const AdjPass
         if (s_acc[i] != 0.0) atomicAdd(&a.out[i], s_acc[i]);
 }
 
+// ------------------------------------------------------------ dual-store pass
+// One pass over two compressed stores A and B (DualPassArgs): both tiles are
+// decoded into shared memory (linear layout), the op list runs in order
+// (gates with smem_apply_gate, transition sums, Pauli-term accumulation into
+// B), and each written store is re-encoded into its output arena with one
+// reservation per tile.  Blocks not stored at the start of the pass read as
+// zeros; every chunk of a written store is written.
+constexpr int kDualThreads = 256;
+
+template <typename R>
+__device__ void dual_decode_tile(const DualStore &st, int C, int j, int blk_shift, uint64_t chunk_base,
+                                 const int32_t *s_tq, CodecParams p, R *tile, uint32_t *wstage, int warp, int nwarps,
+                                 int lane) {
+    const int nchunks = 1 << j, ncomp = 2 << C, per_lane = ncomp >> 5;
+    for (int c = warp; c < nchunks; c += nwarps) {
+        R *comp = tile + (size_t)c * ncomp;
+        const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
+        if (st.meta_in == nullptr || !st.mask_in[chunk >> blk_shift]) {
+            for (int i = 0; i < per_lane; ++i) comp[lane + 32 * i] = R(0);
+            continue;
+        }
+        decode_chunk<R>(st.arena_in, st.meta_in[chunk], per_lane, p, comp, wstage, lane);
+        __syncwarp();
+    }
+}
+
+// Quantise, reserve and pack one store's tile (codes overwrite the values).
+template <typename R>
+__device__ bool dual_encode_tile(const DualStore &st, int C, int j, int blk_shift, uint64_t chunk_base,
+                                 const int32_t *s_tq, CodecParams p, R *tile, int32_t *s_base, uint32_t *s_width,
+                                 unsigned long long *s_off, unsigned long long *s_tile_off, int *s_flag,
+                                 int32_t *error, int warp, int nwarps, int lane) {
+    const int nchunks = 1 << j, ncomp = 2 << C, per_lane = ncomp >> 5;
+    for (int c = warp; c < nchunks; c += nwarps) {
+        R *comp = tile + (size_t)c * ncomp;
+        int32_t base;
+        uint32_t width;
+        bool nz;
+        quantize_chunk<R>(comp, per_lane, p, false, lane, &base, &width, &nz);
+        if (lane == 0) {
+            s_base[c] = base;
+            s_width[c] = width;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long run = 0;
+        for (int c = 0; c < nchunks; ++c) {
+            s_off[c] = run;
+            run += payload_bytes(C, s_width[c]);
+        }
+        const unsigned long long off = atomicAdd(st.bump, run);
+        *s_flag = 0;
+        if (off + run > st.capacity) {
+            atomicExch(error, 1);
+            *s_flag = 1;
+        }
+        *s_tile_off = off;
+    }
+    __syncthreads();
+    if (*s_flag) return false;
+    for (int c = warp; c < nchunks; c += nwarps) {
+        const uint64_t chunk = chunk_base | deposit_bits((uint32_t)c, s_tq, j);
+        const int32_t *codes = reinterpret_cast<const int32_t *>(tile + (size_t)c * ncomp);
+        const unsigned long long off = *s_tile_off + s_off[c];
+        const uint32_t w = s_width[c];
+        pack_chunk(codes, per_lane, s_base[c], w, st.arena_out + (off >> 2), lane);
+        if (lane == 0) {
+            ChunkMeta md;
+            md.offset = off;
+            md.base = s_base[c];
+            md.width = w;
+            st.meta_out[chunk] = md;
+            atomicAdd(&st.block_bytes[chunk >> blk_shift],
+                      (unsigned long long)(payload_bytes(C, w) + sizeof(ChunkMeta)));
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kDualThreads) dual_pass_kernel(const DualPassArgs a) {
+    using T = typename Cplx<R>::T;
+    extern __shared__ __align__(16) unsigned char dual_smem[];
+    __shared__ double s_acc[2 * kMaxDualSlots];
+    __shared__ int32_t s_tq[kMaxTileQubits];
+    __shared__ unsigned long long s_tile_off;
+    __shared__ int s_flag;
+    const int C = a.C, j = a.j, nb = C + j, size = 1 << nb;
+    const int nchunks = 1 << j;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int blk_shift = a.B - C;
+    T *tA = reinterpret_cast<T *>(dual_smem);
+    T *tB = tA + size;
+    uint32_t *wstage = reinterpret_cast<uint32_t *>(tB + size) + warp * kStageWords;
+    int32_t *s_base = reinterpret_cast<int32_t *>(reinterpret_cast<uint32_t *>(tB + size) + nwarps * kStageWords);
+    uint32_t *s_width = reinterpret_cast<uint32_t *>(s_base + nchunks);
+    unsigned long long *s_off = reinterpret_cast<unsigned long long *>(s_base + 2 * nchunks);  // 8-byte aligned
+    for (int i = threadIdx.x; i < 2 * a.nslots; i += blockDim.x) s_acc[i] = 0.0;
+    if (threadIdx.x < kMaxTileQubits) s_tq[threadIdx.x] = a.tq[threadIdx.x];
+    __syncthreads();
+    for (uint64_t tile_id = blockIdx.x; tile_id < a.n_tiles; tile_id += gridDim.x) {
+        const uint64_t chunk_base = insert_zero_bits(tile_id, s_tq, j);
+        const uint64_t base_amp = chunk_base << C;
+        dual_decode_tile<R>(a.a, C, j, blk_shift, chunk_base, s_tq, a.codec, reinterpret_cast<R *>(tA), wstage,
+                            warp, nwarps, lane);
+        dual_decode_tile<R>(a.b, C, j, blk_shift, chunk_base, s_tq, a.codec, reinterpret_cast<R *>(tB), wstage,
+                            warp, nwarps, lane);
+        __syncthreads();
+        for (int k = 0; k < a.nops; ++k) {
+            const DualOp &op = a.ops[k];
+            if (op.kind == DOP_SUM) {
+                const int outer = __popcll(base_amp & op.term.zo) & 1;
+                double re = 0.0, im = 0.0;
+                for (int x = threadIdx.x; x < size; x += blockDim.x) {
+                    const T ax = tA[x];
+                    const T by = tB[x ^ (int)op.term.xt];
+                    double pr = (double)by.x * (double)ax.x + (double)by.y * (double)ax.y;
+                    double pi = (double)by.x * (double)ax.y - (double)by.y * (double)ax.x;
+                    if ((__popc((uint32_t)x & op.term.zt) + outer) & 1) { pr = -pr; pi = -pi; }
+                    re += pr;
+                    im += pi;
+                }
+                re = block_warp_sum(re);
+                im = block_warp_sum(im);
+                if (lane == 0) {
+                    atomicAdd(&s_acc[2 * op.slot], re);
+                    atomicAdd(&s_acc[2 * op.slot + 1], im);
+                }
+            } else if (op.kind == DOP_ACCUM) {
+                const int outer = __popcll(base_amp & op.term.zo) & 1;
+                const double cr = op.coef[0], ci = op.coef[1];
+                for (int x = threadIdx.x; x < size; x += blockDim.x) {
+                    const int y = x ^ (int)op.term.xt;
+                    const T v = tA[y];
+                    const double sg = ((__popc((uint32_t)y & op.term.zt) + outer) & 1) ? -1.0 : 1.0;
+                    T &o = tB[x];
+                    o.x = (R)((double)o.x + sg * (cr * (double)v.x - ci * (double)v.y));
+                    o.y = (R)((double)o.y + sg * (cr * (double)v.y + ci * (double)v.x));
+                }
+            } else {
+                if (op.kind != DOP_GATE_B) smem_apply_gate<R>(tA, nb, op.g, base_amp);
+                if (op.kind != DOP_GATE_A) smem_apply_gate<R>(tB, nb, op.g, base_amp);
+            }
+            __syncthreads();
+        }
+        if (a.a.meta_out &&
+            !dual_encode_tile<R>(a.a, C, j, blk_shift, chunk_base, s_tq, a.codec, reinterpret_cast<R *>(tA), s_base,
+                                 s_width, s_off, &s_tile_off, &s_flag, a.error, warp, nwarps, lane))
+            break;
+        if (!dual_encode_tile<R>(a.b, C, j, blk_shift, chunk_base, s_tq, a.codec, reinterpret_cast<R *>(tB), s_base,
+                                 s_width, s_off, &s_tile_off, &s_flag, a.error, warp, nwarps, lane))
+            break;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * a.nslots; i += blockDim.x)
+        if (s_acc[i] != 0.0) atomicAdd(&a.sums[i], s_acc[i]);
+}
+
+size_t dual_pass_smem_bytes(bool f64, int C, int j) {
+    const size_t nch = (size_t)1 << j;
+    // two value tiles, the warps' staging areas, then base, width and offset per chunk
+    return ((size_t)2 * (f64 ? 16 : 8) << (C + j)) + (size_t)(kDualThreads / 32) * kStageWords * 4 + 16 * nch;
+}
+
 // Imported stores: the header of every chunk of an unstored block is set to
 // zero (offset 0, width 0), so that a reader that skipped the zero-mask gate
 // would still read inside the arena.
@@ -1493,10 +2039,41 @@ static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <typename R, bool kCodes>
+static cudaError_t launch_staged_t(const PassArgs &a, cudaStream_t s) {
+    const uint32_t nblk = 1u << (a.n - a.B);
+    const uint32_t mask_words = nblk <= kMaxSmemBlocks ? (nblk + 31) / 32 : 0;
+    const size_t smem = staged_layout(sizeof(R) == 8, a.C, a.j, mask_words).total;
+    cudaError_t e = cudaFuncSetAttribute(staged_pass_kernel<R, kCodes>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, staged_pass_kernel<R, kCodes>, kStagedThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    uint64_t grid = (uint64_t)per_sm * sm_count();
+    if (grid > a.n_tiles) grid = a.n_tiles;
+    if (grid == 0) grid = 1;
+    PassArgs b = a;
+    const char *env = std::getenv("QOMPSIM_SLAB_BYTES");
+    const uint64_t slab = env ? (uint64_t)std::strtoull(env, nullptr, 10) : (uint64_t)kArenaSlabBytes;
+    b.slab = (slab && a.capacity / grid >= 8 * slab) ? (slab + 127) / 128 * 128 : 0;
+    staged_pass_kernel<R, kCodes><<<(unsigned)grid, kStagedThreads, smem, s>>>(b);
+    return cudaGetLastError();
+}
+
+size_t staged_pass_smem_bytes(bool f64, int C, int j, uint32_t nblocks) {
+    return staged_layout(f64, C, j, nblocks <= kMaxSmemBlocks ? (nblocks + 31) / 32 : 0).total;
+}
+
 cudaError_t launch_pass(bool f64, const PassArgs &a, int, cudaStream_t s) {
     if (a.rb != kRegBits || a.C + a.j < kRegBits || a.diag.nterms > kMaxDiagTerms) return cudaErrorInvalidValue;
     if (a.code_moves && a.diag.nterms) return cudaErrorInvalidValue;
     if (a.header_batch != 4 && a.header_batch != 8) return cudaErrorInvalidValue;
+    if (a.staged) {
+        if (f64) return a.code_moves ? launch_staged_t<double, true>(a, s) : launch_staged_t<double, false>(a, s);
+        return a.code_moves ? launch_staged_t<float, true>(a, s) : launch_staged_t<float, false>(a, s);
+    }
     if (f64)
         return a.code_moves ? launch_pass_t<double, kRegBits, true, 4>(a, s) : launch_pass_t<double, kRegBits, false, 4>(a, s);
     if (a.code_moves)
@@ -1557,6 +2134,13 @@ cudaError_t launch_stage_end(const uint32_t *b2g, const uint8_t *group_active, u
                              unsigned long long *history_slot, cudaStream_t s) {
     stage_end_kernel<<<(nb + 255) / 256, 256, 0, s>>>(b2g, group_active, nb, block_nz, acc, mask, block_bytes,
                                                       history_slot);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mask_full(const uint8_t *mask, uint32_t nb, uint32_t *out, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(out, 0xff, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    mask_full_kernel<<<grid_for(nb, 256, 4), 256, 0, s>>>(mask, nb, out);
     return cudaGetLastError();
 }
 
@@ -1637,6 +2221,27 @@ cudaError_t launch_codec_test(bool f64, const void *vals, int C, CodecParams p, 
 }
 
 uint64_t noalloc_scratch_words() { return kNoAllocScratchWords; }
+
+template <typename R>
+static cudaError_t launch_dual_t(const DualPassArgs &a, cudaStream_t s) {
+    if (a.nslots > kMaxDualSlots) return cudaErrorInvalidValue;
+    const size_t smem = dual_pass_smem_bytes(sizeof(R) == 8, a.C, a.j);
+    cudaError_t e = cudaFuncSetAttribute(dual_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dual_pass_kernel<R>, kDualThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    uint64_t grid = (uint64_t)per_sm * sm_count();
+    if (grid > a.n_tiles) grid = a.n_tiles;
+    if (grid == 0) grid = 1;
+    dual_pass_kernel<R><<<(unsigned)grid, kDualThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dual_pass(bool f64, const DualPassArgs &a, cudaStream_t s) {
+    return f64 ? launch_dual_t<double>(a, s) : launch_dual_t<float>(a, s);
+}
 
 cudaError_t launch_zero_unstored_headers(ChunkMeta *meta, const uint8_t *mask, uint64_t nchunks, int cshift,
                                          cudaStream_t s) {

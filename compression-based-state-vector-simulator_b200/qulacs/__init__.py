@@ -577,6 +577,18 @@ class CompressedQuantumState:
                                                          ca.view(np.float64).ctypes.data_as(_n.ct.POINTER(_n.ct.c_double)),
                                                          len(za)))
 
+    def load_pauli_sum(self, source: "CompressedQuantumState", xs, zs, coefs) -> None:
+        """self := (sum_t coefs[t] X^{xs[t]} Z^{zs[t]}) source for general
+        Pauli strings, with any i^{ny} of Y factors folded into coefs
+        (qs_apply_pauli_sum): the adjoint's lambda = H psi."""
+        xa = np.ascontiguousarray(np.asarray(xs, dtype=np.uint64))
+        za = np.ascontiguousarray(np.asarray(zs, dtype=np.uint64))
+        ca = np.ascontiguousarray(np.asarray(coefs, dtype=np.complex128))
+        self._check(_n.lib().qs_apply_pauli_sum(self._h, source._h, xa.ctypes.data_as(_n.ct.POINTER(_n.ct.c_uint64)),
+                                                za.ctypes.data_as(_n.ct.POINTER(_n.ct.c_uint64)),
+                                                ca.view(np.float64).ctypes.data_as(_n.ct.POINTER(_n.ct.c_double)),
+                                                len(xa)))
+
     def checkpoint(self, slot: int = 0) -> None:
         """Copy the compressed store into device checkpoint `slot`."""
         self._check(_n.lib().qs_checkpoint(self._h, int(slot)))

@@ -78,6 +78,8 @@ class qs_stats(ct.Structure):
         ("code_move_passes", ct.c_uint64),
         ("arena_capacity", ct.c_uint64),
         ("host_store", ct.c_uint64),
+        ("merged_from", ct.c_int64),
+        ("tail_passes", ct.c_uint64),
     ]
 
 
@@ -113,6 +115,9 @@ SIGNATURES = [
     ("qs_expectation_pauli", ct.c_int, [_P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
     ("qs_transition_pauli", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
     ("qs_apply_diagonal_pauli_sum", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_D), ct.c_size_t]),
+    ("qs_apply_pauli_sum", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_U64), ct.POINTER(_D), ct.c_size_t]),
+    ("qs_adjoint", ct.c_int, [_P, _P, _P, ct.POINTER(_I32), ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t,
+                              ct.POINTER(_D), _U32]),
     ("qs_dense_expectation_pauli", ct.c_int, [_P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
     ("qs_dense_copy", ct.c_int, [_P, _P]),
     ("qs_dense_apply_pauli_sum", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_U64), ct.POINTER(_D), ct.c_size_t]),

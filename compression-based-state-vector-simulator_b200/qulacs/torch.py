@@ -227,6 +227,140 @@ def compressed_energy_and_gradient(circuit, observable: Observable, block_size: 
     return energy_value, grads
 
 
+def _backward_lists(gates, start, end, slot_of):
+    """Inverse gates of gates[start:end] in reverse order, with the slot and
+    generator masks of each parametric one (slot -1 for the others)."""
+    back, slots, gx, gz, gny = [], [], [], [], []
+    for k in reversed(range(start, end)):
+        g = gates[k]
+        back.append(g.get_inverse())
+        if k in slot_of:
+            xm, zm, ny = g.generator_masks()
+            slots.append(slot_of[k])
+            gx.append(xm)
+            gz.append(zm)
+            gny.append(ny)
+        else:
+            slots.append(-1)
+            gx.append(0)
+            gz.append(0)
+            gny.append(0)
+    return back, slots, gx, gz, gny
+
+
+def compressed_adjoint_gradient(circuit, observable: Observable, block_size: int, inner_size: int = 4,
+                                dtype="complex128", eps_rel: float = 1e-3, eps_abs: float = 1e-7,
+                                checkpoint_every: Optional[int] = None, flags: Optional[int] = None,
+                                timings: Optional[dict] = None):
+    """(E, dE/dtheta) of any parametric circuit and observable (X, Y, Z
+    strings) with both states compressed.
+
+    Forward: psi = U|0> on a CompressedQuantumState (the registered circuit's
+    stages and passes), with a device checkpoint of the compressed store after
+    every `checkpoint_every` parametric gates when given.  E = <psi|H|psi> /
+    <psi|psi> (FP64 reductions); lambda = H psi (qs_apply_pauli_sum).
+    Backward, segment by segment from the end: psi is restored from the
+    checkpoint at the segment's end (so its compression error does not build
+    up over the whole circuit: between checkpoints it is recomputed backwards
+    by the inverse gates), then one fused sweep over both compressed stores
+    (qs_adjoint) applies the segment's inverse gates to psi and lambda and, at
+    each parametric gate k, accumulates <lambda_k|P_k|psi_k>:
+    dE/dtheta_k = -Im(i^{ny} <lambda_k|P_k|psi_k>) / <psi|psi>.  This is the
+    reference's backprop (src/vqcsim/parametric_circuit.cpp:180-306) on
+    compressed states.
+
+    timings, when given, receives device milliseconds (CUDA events on the
+    states' stream) of: forward (apply + energy), lambda, backward."""
+    import qulacs
+    from . import CompressedQuantumState
+    n = circuit.get_qubit_count()
+    xs, zs, nys, coefs = observable.term_masks()
+    gates = list(circuit._gates)
+    param_pos = list(getattr(circuit, "_param_pos", []))
+    slot_of = {pos: i for i, pos in enumerate(param_pos)}
+    if flags is None:
+        flags = _n.QS_FLAG_QUIET
+    # segment ends: after every `checkpoint_every` parametric gates
+    bounds = []
+    if checkpoint_every:
+        for k, pos in enumerate(param_pos):
+            if (k + 1) % checkpoint_every == 0 and pos + 1 < len(gates):
+                bounds.append(pos + 1)
+    bounds = sorted(set(bounds))
+
+    ev = None
+    try:
+        import torch as _t
+        if _t.cuda.is_available():
+            ev = [_t.cuda.Event(enable_timing=True) for _ in range(4)]
+    except ImportError:
+        pass
+
+    def rec(i):
+        if ev is not None:
+            ev[i].record()
+
+    def run(st, gate_list):
+        if not gate_list:
+            return
+        c = qulacs.QuantumCircuit(n)
+        c._gates = list(gate_list)
+        st.partition_and_register_circuit(c, inner_size, 0)
+        st.apply_circuit()
+
+    psi = CompressedQuantumState(n, block_size, dtype=dtype, eps_rel=eps_rel, eps_abs=eps_abs, flags=flags)
+    rec(0)
+    pos = 0
+    for k, e in enumerate(bounds):
+        run(psi, gates[pos:e])
+        psi.checkpoint(k)
+        pos = e
+    run(psi, gates[pos:])
+    sums = psi._pauli_sums(list(xs) + [0], list(zs) + [0])
+    norm2 = sums[-1].real
+    energy_value = float(np.real(sum(c * (1j ** ny) * v for c, ny, v in zip(coefs, nys, sums[:-1])) / norm2))
+    rec(1)
+    lam = CompressedQuantumState(n, block_size, dtype=dtype, eps_rel=eps_rel, eps_abs=eps_abs, flags=flags)
+    lam.load_pauli_sum(psi, xs, zs, [c * (1j ** ny) for c, ny in zip(coefs, nys)])
+    rec(2)
+    nslots = len(param_pos)
+    acc = np.zeros(2 * max(1, nslots), dtype=np.float64)
+    ny_of_slot = np.zeros(max(1, nslots), dtype=np.int64)
+    ends = [len(gates)] + list(reversed(bounds))
+    starts = list(reversed(bounds)) + [0]
+    L = _n.lib()
+    for k, (start, end) in enumerate(zip(starts, ends)):
+        if k > 0:
+            psi.restore(len(bounds) - k)   # the forward state at this segment's end
+        back, slots, gx, gz, gny = _backward_lists(gates, start, end, slot_of)
+        if not back:
+            continue
+        for s_, ny in zip(slots, gny):
+            if s_ >= 0:
+                ny_of_slot[s_] = ny
+        arr = _n.make_gate_array(back)
+        sl = np.ascontiguousarray(np.asarray(slots, dtype=np.int32))
+        xa, za = _masks_arrays(gx, gz)
+        out = np.zeros(2 * max(1, nslots), dtype=np.float64)
+        psi._check(L.qs_adjoint(psi._h, lam._h, arr, sl.ctypes.data_as(ct.POINTER(ct.c_int32)),
+                                xa.ctypes.data_as(ct.POINTER(ct.c_uint64)),
+                                za.ctypes.data_as(ct.POINTER(ct.c_uint64)), len(back),
+                                out.ctypes.data_as(ct.POINTER(ct.c_double)), nslots))
+        acc += out
+    rec(3)
+    for k in range(len(bounds)):
+        psi.free_checkpoint(k)
+    sums_g = acc[0:2 * nslots:2] + 1j * acc[1:2 * nslots:2]
+    grads = -np.imag((1j ** ny_of_slot[:nslots]) * sums_g) / norm2
+    if timings is not None and ev is not None:
+        import torch as _t
+        _t.cuda.synchronize()
+        timings["forward_ms"] = ev[0].elapsed_time(ev[1])
+        timings["lambda_ms"] = ev[1].elapsed_time(ev[2])
+        timings["backward_ms"] = ev[2].elapsed_time(ev[3])
+    return energy_value, grads
+
+
 def energy(circuit, observable: Observable, dtype="complex128") -> float:
     psi = QuantumState(circuit.get_qubit_count(), dtype=dtype)
     circuit.update_quantum_state(psi)

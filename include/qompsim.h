@@ -39,7 +39,7 @@ typedef enum qs_status {
     QS_ERR_CUDA = 2,             /* a CUDA runtime call failed                          */
     QS_ERR_CAPACITY = 3,         /* compressed store does not fit its arenas            */
     QS_ERR_UNSUPPORTED_GATE = 4, /* gate with >2 qubits, FusedSWAP (needs MPI ranks)    */
-    QS_ERR_TIMEOUT = 5,          /* reserved: a bounded device wait gave up             */
+    QS_ERR_TIMEOUT = 5,          /* a bounded device wait gave up                       */
     QS_ERR_CORRUPT = 6,          /* imported store failed its length/header checks      */
     QS_ERR_STATE = 7,            /* call out of order (e.g. apply before registration)  */
     QS_ERR_NOMEM = 8,            /* host allocation failed                              */
@@ -114,6 +114,10 @@ typedef struct qs_stats {
                                     quantised codes through the tile without dequantising */
     uint64_t arena_capacity;     /* bytes of each of the two payload arenas             */
     uint64_t host_store;         /* 1 when the arenas are in host memory (QS_FLAG_HOST_STORE) */
+    int64_t merged_from;         /* first stage of the merged tail of the last apply, -1 when none:
+                                    once every block is stored, the remaining stages' gates share
+                                    passes (no stage boundary can change the mask any more) */
+    uint64_t tail_passes;        /* device passes of that merged tail                   */
 } qs_stats;
 
 /* ---------------------------------------------------------------- errors */
@@ -255,6 +259,32 @@ qs_status qs_transition_pauli(const qs_state *bra, qs_state *ket, const uint64_t
  * states, for the adjoint sweep's lambda = H psi. */
 qs_status qs_apply_diagonal_pauli_sum(qs_state *out, const qs_state *in, const uint64_t *z_masks,
                                       const double *coefs, size_t nterms);
+
+/* out := (sum_t c_t P_t) in for general Pauli strings P_t = i^{ny} X^{x_t}
+ * Z^{z_t} (coefs complex interleaved with i^{ny} folded in, so that
+ * (P_t in)[x] = (-1)^{popcount(y & z_t)} in[y], y = x ^ x_t): passes that
+ * decode in's store and accumulate the terms into out's (terms grouped so
+ * that each group's flip qubits fit one tile).  Observable::apply_to_state
+ * (src/cppsim/observable.cpp) on compressed states: the adjoint sweep's
+ * lambda = H psi for observables with X / Y terms.  in and out are distinct
+ * states of the same geometry in HBM; afterwards every block of out is
+ * stored. */
+qs_status qs_apply_pauli_sum(qs_state *out, qs_state *in, const uint64_t *x_masks, const uint64_t *z_masks,
+                             const double *coefs, size_t nterms);
+
+/* Backward sweep of the adjoint gradient over two compressed states, the
+ * compressed counterpart of qs_dense_adjoint: gates (already inverted, in
+ * the order to apply) act on both psi and lam; before a gate with slots[i]
+ * >= 0, out[2 slots[i]], out[2 slots[i] + 1] += sum_x conj(lam[x ^ gen_x])
+ * (-1)^{popcount(x & gen_z)} psi[x].  The reference's
+ * ParametricQuantumCircuit::backprop_inner_product
+ * (src/vqcsim/parametric_circuit.cpp:180-266) on the uncompressed state is
+ * what it computes; the reference has no gradient on its compressed state.
+ * Each fused pass decodes tiles of both stores, applies its gates and sums,
+ * and re-encodes both.  psi and lam are distinct states of one geometry in
+ * HBM on one stream; out (2 * nslots doubles) is overwritten. */
+qs_status qs_adjoint(qs_state *psi, qs_state *lam, const qs_gate *gates, const int32_t *slots, const uint64_t *gen_x,
+                     const uint64_t *gen_z, size_t count, double *out, uint32_t nslots);
 
 /* Zero-block mask: out[b] = 1 when block b is stored (the reference's
  * block_pointers[b] != nullptr, compressed_state.hpp:18-19, 319-325). */

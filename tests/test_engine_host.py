@@ -81,3 +81,41 @@ def test_plan_tiles_padded_to_largest(checker, tmp_path, f64):
     assert tiles
     assert all(p["j"] == p["jmax"] for p in tiles), tiles
     assert tiles[0]["jmax"] == (4 if f64 else 5)
+
+
+def _tail(checker, tmp_path, circuit, n, B, I, f64):
+    import ctypes as ct
+    from qulacs import _native
+    from qulacs.circuit import QuantumCircuitOptimizer
+    QuantumCircuitOptimizer(sv_block_size=B).optimize(circuit, block_size=2)
+    arr = _native.make_gate_array(circuit._gates)
+    path = tmp_path / "gates.bin"
+    with open(path, "wb") as f:
+        f.write(struct.pack("<Q", len(circuit._gates)))
+        f.write(ct.string_at(ct.addressof(arr), ct.sizeof(_native.qs_gate) * len(circuit._gates)))
+    r = subprocess.run([checker, "tail", str(path), str(n), str(B), str(I), "1" if f64 else "0"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = []
+    for line in r.stdout.splitlines():
+        t = line.split()
+        if t and t[0] == "tail":
+            out.append(dict(s0=int(t[1]), per_stage=int(t[3]), merged=int(t[5]), ends=[int(x) for x in t[7:]]))
+    return out
+
+
+@pytest.mark.parametrize("f64", [True, False])
+def test_merged_tail_plan(checker, tmp_path, f64):
+    """Brickwork n=20 (a dense state after its first stages): planned as one
+    gate sequence with commuting gates reordered, the stages from any start
+    need fewer passes than stage by stage (a third fewer from stage 2 on);
+    every stage ends in a tail pass, in order, the last stage in the last
+    pass."""
+    from qompsim import circuits as C
+    tails = _tail(checker, tmp_path, C.brickwork(20, 20, seed=0), 20, 12, 4, f64)
+    assert tails
+    for t in tails:
+        assert 1 <= t["merged"] <= t["per_stage"]
+        assert all(b >= a for a, b in zip(t["ends"], t["ends"][1:]))
+        assert t["ends"][-1] == t["merged"] - 1
+    assert tails[2]["merged"] * 3 < tails[2]["per_stage"] * 2

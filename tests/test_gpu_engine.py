@@ -228,6 +228,8 @@ def test_compressed_random_circuits_vs_csim(qulacs_mod, n, seed):
 
 def _permute_chunks_run(qulacs, c, B, I, on, monkeypatch, **kw):
     monkeypatch.setenv("QOMPSIM_PERMUTE_CHUNKS", "1" if on else "0")
+    # per-stage plans: a merged tail would plan the two variants' passes differently
+    monkeypatch.setenv("QOMPSIM_MERGE_TAIL", "0")
     cq = _compressed(qulacs, c, B, I, **kw)
     return cq, cq.get_vector(renormalize=False), cq.get_zero_mask(), cq.get_SV_bytes_history(), cq.get_stats()
 
@@ -554,6 +556,8 @@ def test_code_move_passes_bit_identical(qulacs_mod, monkeypatch, dtype, circ, ex
     c = helpers.optimized(C.qft_basis(n, 5), B) if circ == "qft" else _moves_circuit(n, 7)
     flags = _native.QS_FLAG_QUIET | (_native.QS_FLAG_EXACT_ZERO_TEST if exact else 0)
     out = []
+    # per-stage plans: in a merged tail the SWAP stages share passes with other gates
+    monkeypatch.setenv("QOMPSIM_MERGE_TAIL", "0")
     for on in ("1", "0"):
         monkeypatch.setenv("QOMPSIM_CODE_MOVES", on)
         cq = _compressed(qulacs_mod, c, B, 3, dtype=dtype, flags=flags)
@@ -583,3 +587,82 @@ def test_arena_slabs_same_store(qulacs_mod, monkeypatch, dtype):
     blob = out[0][3].export_store()
     out[1][3].import_store(blob)
     assert np.array_equal(out[1][3].get_vector(renormalize=False), out[0][0])
+
+
+# ------------------------------------------------------------ merged tail
+def _dense_then_random(n, seed):
+    """H on every qubit (every block stored after the first stages), then a
+    random circuit over every gate form, with SWAP / X gates on high qubits."""
+    import qulacs
+    c = qulacs.QuantumCircuit(n)
+    for q in range(n):
+        c.add_H_gate(q)
+    for g in helpers.perm_heavy_circuit(n, 8, 50, seed)._gates:
+        c.add_gate(g)
+    return c
+
+
+@pytest.mark.parametrize("dtype", ["complex128", "complex64"])
+@pytest.mark.parametrize("n,B,I", [(16, 9, 3), (15, 8, 2)])
+def test_merged_tail_matches_per_stage(qulacs_mod, monkeypatch, dtype, n, B, I):
+    """Once every block is stored the remaining stages share passes: the
+    merged run has the per-stage run's masks, stage list, update count and
+    history length, fewer passes, and the same state within the codec's
+    error (tight bounds; the two plans quantise at different points), and
+    matches csim."""
+    c = helpers.optimized(_dense_then_random(n, 31), B)
+    ref = csim_ref.run_circuit(n, c._gates)
+    kw = dict(dtype=dtype, eps_rel=2.0 ** -22 if dtype == "complex128" else 2.0 ** -20, eps_abs=1e-13)
+    runs = []
+    for merge in ("1", "0"):
+        monkeypatch.setenv("QOMPSIM_MERGE_TAIL", merge)
+        cq = _compressed(qulacs_mod, c, B, I, **kw)
+        runs.append((cq, cq.get_vector(renormalize=False), cq.get_stats()))
+    (m, vm, sm), (u, vu, su) = runs
+    assert sm["merged_from"] >= 1 and su["merged_from"] == -1
+    assert sm["tail_passes"] > 0 and sm["passes"] < su["passes"]
+    assert sm["amp_gate_updates"] == su["amp_gate_updates"]
+    assert m.get_stage_list() == u.get_stage_list()
+    assert np.array_equal(m.get_zero_mask(), u.get_zero_mask()) and m.get_zero_mask().all()
+    assert len(m.get_SV_bytes_history()) == len(u.get_SV_bytes_history())
+    tol = 1e-5 if dtype == "complex128" else 5e-5
+    assert np.abs(vm - vu).max() < tol
+    assert np.abs(vm - ref).max() < tol
+    # a second apply from the same start reuses the tail plan and repeats the result
+    m.set_zero_state()
+    m.apply_circuit()
+    assert np.array_equal(m.get_vector(renormalize=False), vm)
+
+
+# ------------------------------------------------------------ reference gpusim cross-check
+@pytest.mark.parametrize("key", ["qft_8", "hea_9", "ghz_10", "qaoa_9", "grover_11"])
+def test_reference_gpusim_matches_golden_and_our_dense_paths(qulacs_mod, key):
+    """The reference's own plain complex128 GPU kernels (src/gpusim, built
+    from source) reproduce the golden csim states, and this package's
+    per-gate and fused uncompressed paths match them to 1e-12: the per-gate
+    baseline of the speed-up figures is checked against the reference's GPU
+    path, not only its CPU kernels."""
+    from oracle import gpusim_ref
+    if not gpusim_ref.available():
+        pytest.skip("oracle/_ref/libgpusim_ref.so not built (the reference is not mounted where it was built)")
+    c = helpers.build_circuit(key)
+    ref = helpers.golden_states()[key]
+    gs = gpusim_ref.GpuState(c.get_qubit_count())
+    gs.apply(c._gates)
+    g = gs.get_vector()
+    assert np.abs(g - ref).max() < F64_TOL
+    for pergate in (True, False):
+        assert np.abs(_dense_run(qulacs_mod, c, pergate=pergate) - g).max() < F64_TOL
+
+
+@pytest.mark.parametrize("n,seed", [(12, 51), (16, 52)])
+def test_reference_gpusim_matches_random_circuits(qulacs_mod, n, seed):
+    from oracle import gpusim_ref
+    if not gpusim_ref.available():
+        pytest.skip("oracle/_ref/libgpusim_ref.so not built")
+    c = helpers.random_circuit(n, 120, seed)
+    gs = gpusim_ref.GpuState(n)
+    gs.apply(c._gates)
+    g = gs.get_vector()
+    assert np.abs(g - csim_ref.run_circuit(n, c._gates)).max() < F64_TOL
+    assert np.abs(_dense_run(qulacs_mod, c, pergate=True) - g).max() < F64_TOL
