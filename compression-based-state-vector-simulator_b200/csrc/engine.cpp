@@ -2076,6 +2076,177 @@ qs_status qs_get_stats(qs_state *h, qs_stats *out) {
     return QS_OK;
 }
 
+// tf32 rounding of x (10 mantissa bits, to nearest, ties away from zero):
+// the hi part of the 3xTF32 split of the gate operand.
+static float tf32_round(float x) {
+    uint32_t b;
+    std::memcpy(&b, &x, 4);
+    if ((b & 0x7f800000u) != 0x7f800000u) b = (b + 0x1000u) & 0xffffe000u;
+    float r;
+    std::memcpy(&r, &b, 4);
+    return r;
+}
+
+qs_status qs_apply_dense_gate(qs_state *h, const uint32_t *targets, uint32_t k, const double *matrix) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    if (!targets || !matrix) return fail(h, QS_ERR_ARG, "NULL argument");
+    if (k < (uint32_t)qs::kMinDenseK || k > (uint32_t)qs::kMaxDenseK)
+        return fail(h, QS_ERR_UNSUPPORTED_GATE, "dense gates act on 4 or 5 qubits (fused by optimize(block_size=k))");
+    if (!h->staged) return fail(h, QS_ERR_UNSUPPORTED_GATE, "dense k-qubit passes need HBM arenas (not the host store)");
+    const int C = (int)h->C, n = (int)h->n, B = (int)h->B;
+    if (n < qs::kDenseTileLog2) return fail(h, QS_ERR_ARG, "dense k-qubit passes need at least 12 qubits");
+    for (uint32_t i = 0; i < k; ++i) {
+        if (targets[i] >= h->n) return fail(h, QS_ERR_ARG, "gate target index out of range");
+        for (uint32_t t = 0; t < i; ++t)
+            if (targets[t] == targets[i]) return fail(h, QS_ERR_ARG, "duplicated qubit index in gate");
+    }
+    // tile: the chunk bits, the gate's qubits above them, padded with other
+    // in-block qubits up to 2^12 amplitudes (every block of a tile then lies
+    // in one group of this one-gate stage)
+    const int jt = qs::kDenseTileLog2 - C;
+    std::set<int> tq;
+    for (uint32_t i = 0; i < k; ++i)
+        if ((int)targets[i] >= C) tq.insert((int)targets[i]);
+    if ((int)tq.size() > jt)
+        return fail(h, QS_ERR_UNSUPPORTED_GATE, "a dense gate has more qubits above the chunk than a tile holds");
+    for (int q = C; q < B && (int)tq.size() < jt; ++q) tq.insert(q);
+    if ((int)tq.size() < jt) return fail(h, QS_ERR_ARG, "block too small for a dense k-qubit tile");
+    const std::vector<int> tile(tq.begin(), tq.end());
+    qs::DenseKGate dk{};
+    dk.k = (int32_t)k;
+    for (uint32_t i = 0; i < k; ++i) {
+        const int q = (int)targets[i];
+        dk.pos[i] = q < C ? q : C + (int)(std::find(tile.begin(), tile.end(), q) - tile.begin());
+    }
+    // the one-gate stage's groups: blocks differing only in the gate's
+    // qubits at or above the block size (make_block_groups' rule)
+    std::vector<uint32_t> b2g(h->nb);
+    std::vector<int> outer;
+    for (int q = B; q < n; ++q) {
+        bool inner = false;
+        for (uint32_t i = 0; i < k; ++i) inner = inner || (int)targets[i] == q;
+        if (!inner) outer.push_back(q);
+    }
+    for (uint32_t b = 0; b < h->nb; ++b) {
+        uint32_t gid = 0;
+        for (size_t i = 0; i < outer.size(); ++i) gid |= ((b >> (outer[i] - B)) & 1u) << i;
+        b2g[b] = gid;
+    }
+    const uint32_t ngroups = 1u << outer.size();
+    // matrix operands
+    const int K = 1 << k, Kp = 2 * K;
+    std::vector<float> hi, lo;
+    std::vector<double> mat;
+    if (!h->f64) {
+        hi.assign((size_t)Kp * Kp, 0.0f);
+        lo.assign((size_t)Kp * Kp, 0.0f);
+        for (int nrow = 0; nrow < Kp; ++nrow)
+            for (int kc = 0; kc < Kp; ++kc) {
+                const int r = nrow % K, c = kc % K;
+                const double gr = matrix[2 * ((size_t)r * K + c)], gi = matrix[2 * ((size_t)r * K + c) + 1];
+                // [[Gr, -Gi], [Gi, Gr]]: output rows Re y then Im y, input columns Re x then Im x
+                const double v = nrow < K ? (kc < K ? gr : -gi) : (kc < K ? gi : gr);
+                const float vh = tf32_round((float)v);
+                const size_t off = qs::dense_k_operand_offset((uint32_t)nrow, (uint32_t)kc, (uint32_t)Kp) / 4;
+                hi[off] = vh;
+                lo[off] = tf32_round((float)v - vh);
+            }
+    } else {
+        mat.assign(matrix, matrix + 2 * (size_t)K * K);
+    }
+    struct Tmp {
+        std::vector<void *> p;
+        ~Tmp() {
+            for (void *q : p) cudaFree(q);
+        }
+    } tmp;
+    cudaStream_t s = h->stream;
+    uint32_t *db2g = nullptr;
+    CUDA_TRY(h, cudaMalloc(&db2g, h->nb * sizeof(uint32_t)));
+    tmp.p.push_back(db2g);
+    CUDA_TRY(h, cudaMemcpyAsync(db2g, b2g.data(), h->nb * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    if (!h->f64) {
+        float *d = nullptr;
+        CUDA_TRY(h, cudaMalloc(&d, 2 * hi.size() * sizeof(float)));
+        tmp.p.push_back(d);
+        CUDA_TRY(h, cudaMemcpyAsync(d, hi.data(), hi.size() * 4, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(h, cudaMemcpyAsync(d + hi.size(), lo.data(), lo.size() * 4, cudaMemcpyHostToDevice, s));
+        dk.bhi = d;
+        dk.blo = d + hi.size();
+    } else {
+        double *d = nullptr;
+        CUDA_TRY(h, cudaMalloc(&d, mat.size() * sizeof(double)));
+        tmp.p.push_back(d);
+        CUDA_TRY(h, cudaMemcpyAsync(d, mat.data(), mat.size() * 8, cudaMemcpyHostToDevice, s));
+        dk.mat = d;
+    }
+    unsigned long long *dhist = nullptr;  // [0] stage total, [1] active blocks
+    CUDA_TRY(h, cudaMalloc(&dhist, 2 * sizeof(unsigned long long)));
+    tmp.p.push_back(dhist);
+    CUDA_TRY(h, cudaMemsetAsync(dhist, 0, 2 * sizeof(unsigned long long), s));
+    CUDA_TRY(h, cudaMemsetAsync(h->error_dev, 0, sizeof(int32_t), s));
+    CUDA_TRY(h, cudaMemsetAsync(h->counters, 0, 8 * sizeof(unsigned long long), s));
+    CUDA_TRY(h, qs::launch_stage_begin(db2g, h->mask, h->nb, h->group_active, ngroups, h->block_nz, h->block_acc,
+                                       dhist + 1, s));
+    const int out = h->cur ^ 1;
+    qs::PassArgs a{};
+    a.n = n;
+    a.B = B;
+    a.C = C;
+    a.j = jt;
+    for (int i = 0; i < jt; ++i) a.tq[i] = tile[i] - C;
+    a.n_tiles = uint64_t(1) << (n - qs::kDenseTileLog2);
+    a.rb = qs::kRegBits;
+    a.codec = h->codec;
+    a.meta_in = h->meta[h->mcur];
+    a.arena_in = h->arena[h->cur];
+    a.meta_out = h->meta[h->mcur ^ 1];
+    a.arena_out = h->arena[out];
+    a.perm = identity_perm();
+    a.bump = h->counters + out;
+    a.capacity = h->capacity;
+    a.block_to_group = db2g;
+    a.group_active = h->group_active;
+    a.mask = h->mask;
+    a.first_pass = 1;
+    a.final_pass = 1;
+    a.exact_zero = (h->flags & QS_FLAG_EXACT_ZERO_TEST) ? 1 : 0;
+    a.header_batch = 4;
+    a.block_nz = h->block_nz;
+    a.block_bytes = h->block_acc;
+    a.error = h->error_dev;
+    a.stats = h->counters + 2;
+    a.staged = 1;
+    a.dense = dk;
+    CUDA_TRY(h, cudaEventRecord(h->ev[0], s));
+    CUDA_TRY(h, qs::launch_pass(h->f64, a, qs::kDenseTileLog2, s));
+    CUDA_TRY(h, cudaEventRecord(h->ev[1], s));
+    CUDA_TRY(h, qs::launch_stage_end(db2g, h->group_active, h->nb, h->block_nz, h->block_acc, h->mask,
+                                     h->block_bytes, dhist, s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
+    int32_t errflag = 0;
+    unsigned long long ctr[8], hst[2];
+    CUDA_TRY(h, cudaMemcpy(&errflag, h->error_dev, sizeof(errflag), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(ctr, h->counters, sizeof(ctr), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(hst, dhist, sizeof(hst), cudaMemcpyDeviceToHost));
+    float ms = 0;
+    CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
+    h->cur = out;
+    h->mcur ^= 1;
+    if (errflag == 2) return fail(h, QS_ERR_TIMEOUT, "a dense-gate pass gave up a bounded wait; the state is invalid");
+    if (errflag) return fail(h, QS_ERR_CAPACITY, "compressed store overflowed its arena in a dense-gate pass");
+    h->arena_used = ctr[out];
+    h->history.push_back(hst[0]);
+    h->st.bytes_read = ctr[2];
+    h->st.bytes_written = ctr[3];
+    h->st.tiles = ctr[4];
+    h->st.kernel_ms = ms;
+    h->st.apply_ms = ms;
+    h->st.passes = 1;
+    h->st.amp_gate_updates = hst[1] << h->B;
+    return QS_OK;
+}
+
 qs_status qs_set_basis_state(qs_state *h, uint64_t basis) {
     if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
     if (basis >> h->n) return fail(h, QS_ERR_ARG, "basis index out of range");

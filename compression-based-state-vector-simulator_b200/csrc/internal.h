@@ -131,6 +131,34 @@ struct DiagSum {
     int32_t nterms;
 };
 
+// A dense k-qubit gate applied over a whole tile of 2^kDenseTileLog2
+// amplitudes (kMinDenseK <= k <= kMaxDenseK): the tile's 2^(12-k) columns
+// (patterns of its other bits) are the rows of one GEMM y = G x.
+//   complex64:  tensor cores (tcgen05.mma kind::tf32 with a 3xTF32 split):
+//               the gate as the real 2^(k+1) x 2^(k+1) matrix
+//               [[Gr, -Gi], [Gi, Gr]] (row = output: Re y_0.. then Im y_0..;
+//               column = input: Re x_0.. then Im x_0..), split into tf32 hi
+//               and lo parts, each in the K-major unswizzled operand layout
+//               of dense_k_operand_offset
+//   complex128: CUDA cores, the 2^k x 2^k matrix row-major (double2)
+constexpr int kMinDenseK = 4;
+constexpr int kMaxDenseK = 5;
+constexpr int kDenseTileLog2 = 12;
+struct DenseKGate {
+    int32_t k;
+    int32_t pos[kMaxDenseK];    // tile bit position of matrix bit i
+    const float *bhi, *blo;     // complex64 operands (2^(2k+2) floats each)
+    const double *mat;          // complex128 matrix (2^(2k) complex, interleaved)
+};
+
+// Byte offset of element (row, col) of a K-major, unswizzled tcgen05
+// operand with kcols columns: 8-row x 16-byte core matrices, consecutive
+// along K (leading byte offset 128), 8-row groups kcols * 32 bytes apart
+// (stride byte offset).
+__host__ __device__ inline uint32_t dense_k_operand_offset(uint32_t row, uint32_t col, uint32_t kcols) {
+    return (row >> 3) * (kcols * 32u) + (col >> 2) * 128u + (row & 7u) * 16u + (col & 3u) * 4u;
+}
+
 // One fused pass over the compressed store.
 struct PassArgs {
     int32_t n, B, C, j;                 // qubits, block log2, chunk log2, tile qubits above C
@@ -166,6 +194,8 @@ struct PassArgs {
     DiagSum diag;                       // nterms > 0: multiply by a diagonal Pauli sum after the sweeps
     int32_t staged;                     // 1: staged_pass_kernel (payloads prefetched with bulk copies),
                                         // 0: pass_kernel (payloads copied chunk by chunk; the host-store arenas)
+    DenseKGate dense;                   // k > 0: the pass applies this one gate instead of sweeps
+                                        // (staged kernel, 2^kDenseTileLog2-amplitude tiles)
 };
 
 // A pass that only permutes chunk headers: meta_out[perm(c)] = meta_in[c]

@@ -825,7 +825,9 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
 // Shared-memory layout of staged_pass_kernel (byte offsets; every region
 // 128-byte aligned).
 struct StagedLayout {
-    size_t tile, buf0, buf1, hdr0, hdr1, poff0, poff1, base, width, nz, off, act, sto, total;
+    size_t tile, buf0, buf1, hdr0, hdr1, poff0, poff1, base, width, nz, off, act, sto;
+    size_t dense_a, dense_b, dense_dep;  // dense k-qubit passes only
+    size_t total;
 };
 
 __host__ __device__ inline size_t align128(size_t x) { return (x + 127) / 128 * 128; }
@@ -836,7 +838,11 @@ __host__ __device__ inline size_t staged_stage_bytes(int C, int j) {
     return ((size_t)1 << j) * payload_bytes(C, 32) + 128;
 }
 
-__host__ __device__ inline StagedLayout staged_layout(bool f64, int C, int j, uint32_t mask_words) {
+// Dense k-qubit passes add: complex64, the tile as the realified tcgen05 A
+// operand (hi and lo parts, 2 x 4 x 2^(nb+1) bytes) and the gate operand (hi
+// and lo, 2 x 4 x 2^(2k+2) bytes); complex128, the gate matrix (16 x
+// 2^(2k) bytes); both, the tile offsets of the gate's 2^k patterns.
+__host__ __device__ inline StagedLayout staged_layout(bool f64, int C, int j, uint32_t mask_words, int dense_k = 0) {
     StagedLayout L{};
     const size_t nch = (size_t)1 << j;
     size_t o = 0;
@@ -854,16 +860,224 @@ __host__ __device__ inline StagedLayout staged_layout(bool f64, int C, int j, ui
     L.off = o;   o += align128(8 * nch);
     L.act = o;   o += align128(4 * (size_t)mask_words);
     L.sto = o;   o += align128(4 * (size_t)mask_words);
+    if (dense_k > 0) {
+        if (!f64) {
+            L.dense_a = o; o += align128((size_t)2 * 4 * ((size_t)2 << (C + j)));
+            L.dense_b = o; o += align128((size_t)2 * 4 * ((size_t)4 << (2 * dense_k)));
+        } else {
+            L.dense_b = o; o += align128((size_t)16 << (2 * dense_k));
+        }
+        L.dense_dep = o; o += align128(4 * ((size_t)1 << dense_k));
+    }
     L.total = o;
     return L;
 }
 
-template <typename R, bool kCodes>
+// ------------------------------------------------------------ dense k-qubit gate over a tile
+// tcgen05 building blocks (sm_100a): shared-memory operand descriptors,
+// the kind::tf32 MMA, its commit to an mbarrier, TMEM allocation and loads.
+
+// Descriptor of a K-major, unswizzled operand (dense_k_operand_offset) whose
+// first element is at shared address saddr: start >> 4 in bits [0, 14),
+// leading byte offset (128: the next 4 columns) >> 4 in [16, 30), stride
+// byte offset (kcols * 32: the next 8 rows) >> 4 in [32, 46), descriptor
+// version 1 at bit 46, layout type 0 (no swizzle) in bits [61, 64).
+__device__ __forceinline__ uint64_t umma_kmajor_desc(uint32_t saddr, uint32_t kcols) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((128u >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)(((kcols * 32u) >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// Instruction descriptor of kind::tf32, FP32 accumulation, both operands
+// K-major: D format F32 (1) in bits [4, 6), A and B format TF32 (2) in
+// [7, 10) and [10, 13), N >> 3 in [17, 23), M >> 4 in [24, 29).
+__host__ __device__ inline uint32_t umma_tf32_idesc(int M, int N) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n"
+        " .reg .pred p;\n"
+        " setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n"
+        "}\n" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+// 16 consecutive 32-bit columns of this warp's 32 TMEM lanes (lane = thread)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+
+// x rounded to tf32 (10 mantissa bits, round to nearest, ties away)
+__device__ __forceinline__ float to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// TMEM columns of the dense accumulator: 2^(5-k) blocks of 128 rows x
+// 2^(k+1) FP32 columns = 64 columns for every k of a 2^12 tile.
+constexpr uint32_t kDenseTmemCols = 64;
+
+// Tile bit patterns: dep[r] = tile offset of gate pattern r (matrix bit i
+// at pos[i]); base of row o = o deposited into the other tile bits.
+__device__ __forceinline__ uint32_t dense_row_base(uint32_t o, uint32_t gmask, int nb) {
+    uint32_t b = 0;
+    for (int t = 0, i = 0; t < nb; ++t) {
+        if ((gmask >> t) & 1u) continue;
+        b |= ((o >> i) & 1u) << t;
+        ++i;
+    }
+    return b;
+}
+
+// complex64: y = G x for every column of the tile on the tensor cores.
+// aop: the A operand area (hi part, then lo part), bop: the gate operand
+// (hi, lo), dep: pattern offsets, d_tmem: the accumulator, bar: the MMA
+// mbarrier with its phase parity.  Returns false when the MMAs did not
+// complete within the bounded wait.
+__device__ bool tile_dense_k_tc(float2 *tile, int nb, int swm, int k, const int32_t *dep, uint32_t gmask,
+                                float *aop, const float *bop, uint32_t d_tmem, uint64_t *bar, uint32_t parity) {
+    const int K = 1 << k;              // complex patterns
+    const int Kp = 2 * K;              // realified columns
+    const int rows = 1 << (nb - k);    // tile columns = GEMM rows
+    const int nblk = rows >> 7;        // 128-row blocks
+    const size_t half = (size_t)rows * Kp;   // floats per operand part
+    float *ahi = aop, *alo = aop + half;
+    const float *bhi = bop, *blo = bop + (size_t)Kp * Kp;
+    // stage the tile as A = X^T (row o: Re x then Im x), tf32 hi and lo
+    for (int o = threadIdx.x; o < rows; o += blockDim.x) {
+        const uint32_t base = dense_row_base((uint32_t)o, gmask, nb);
+        const int blk = o >> 7, m = o & 127;
+        const size_t boff = (size_t)blk * 128 * Kp * 4;
+        for (int r4 = 0; r4 < K; r4 += 4) {
+            float re[4], im[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const float2 v = tile[swz<float>((int)(base | (uint32_t)dep[r4 + i]), swm)];
+                re[i] = v.x;
+                im[i] = v.y;
+            }
+            float4 h, l;
+            h = make_float4(to_tf32(re[0]), to_tf32(re[1]), to_tf32(re[2]), to_tf32(re[3]));
+            l = make_float4(to_tf32(re[0] - h.x), to_tf32(re[1] - h.y), to_tf32(re[2] - h.z), to_tf32(re[3] - h.w));
+            const uint32_t ore = dense_k_operand_offset((uint32_t)m, (uint32_t)r4, (uint32_t)Kp);
+            *reinterpret_cast<float4 *>(reinterpret_cast<char *>(ahi) + boff + ore) = h;
+            *reinterpret_cast<float4 *>(reinterpret_cast<char *>(alo) + boff + ore) = l;
+            h = make_float4(to_tf32(im[0]), to_tf32(im[1]), to_tf32(im[2]), to_tf32(im[3]));
+            l = make_float4(to_tf32(im[0] - h.x), to_tf32(im[1] - h.y), to_tf32(im[2] - h.z), to_tf32(im[3] - h.w));
+            const uint32_t oim = dense_k_operand_offset((uint32_t)m, (uint32_t)(K + r4), (uint32_t)Kp);
+            *reinterpret_cast<float4 *>(reinterpret_cast<char *>(ahi) + boff + oim) = h;
+            *reinterpret_cast<float4 *>(reinterpret_cast<char *>(alo) + boff + oim) = l;
+        }
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        tmem_fence_after();
+        const uint32_t idesc = umma_tf32_idesc(128, Kp);
+        const uint32_t sa_hi = smem_u32(ahi), sa_lo = smem_u32(alo), sb_hi = smem_u32(bhi), sb_lo = smem_u32(blo);
+        for (int b = 0; b < nblk; ++b) {
+            const uint32_t d = d_tmem + (uint32_t)(b * Kp);
+            const uint32_t boff = (uint32_t)b * 128u * (uint32_t)Kp * 4u;
+            for (int st = 0; st < Kp / 8; ++st) {
+                const uint32_t so = (uint32_t)st * 256u;   // 8 columns = two 4-column core matrices
+                const uint64_t ah = umma_kmajor_desc(sa_hi + boff + so, (uint32_t)Kp);
+                const uint64_t al = umma_kmajor_desc(sa_lo + boff + so, (uint32_t)Kp);
+                const uint64_t bh = umma_kmajor_desc(sb_hi + so, (uint32_t)Kp);
+                const uint64_t bl = umma_kmajor_desc(sb_lo + so, (uint32_t)Kp);
+                umma_tf32(d, ah, bh, idesc, st > 0 ? 1u : 0u);
+                umma_tf32(d, ah, bl, idesc, 1u);
+                umma_tf32(d, al, bh, idesc, 1u);
+            }
+        }
+        umma_commit(bar);
+    }
+    const bool mine = mbar_wait_bounded(bar, parity);
+    const bool ok = __syncthreads_and(mine) != 0;
+    if (!ok) return false;
+    tmem_fence_after();
+    // read back: warp w reads TMEM lanes 32 (w % 4) .. of blocks w / 4, w / 4 + 2, ...
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    for (int b = warp >> 2; b < nblk; b += nwarps >> 2) {
+        const int o = b * 128 + 32 * (warp & 3) + lane;
+        const uint32_t base = dense_row_base((uint32_t)o, gmask, nb);
+        const uint32_t taddr = d_tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(b * Kp);
+        for (int c0 = 0; c0 < K; c0 += 16) {
+            // Re y[c0 .. c0+15] at columns c0.., Im at K + c0 ..
+            float re[16], im[16];
+            tmem_ld16(taddr + (uint32_t)c0, re);
+            tmem_ld16(taddr + (uint32_t)(K + c0), im);
+            tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                if (c0 + i < K) tile[swz<float>((int)(base | (uint32_t)dep[c0 + i]), swm)] = make_float2(re[i], im[i]);
+        }
+    }
+    tmem_fence_before();
+    __syncthreads();
+    return true;
+}
+
+// complex128: y = G x per tile column on the CUDA cores (G in shared memory).
+__device__ void tile_dense_k_f64(double2 *tile, int nb, int swm, int k, const int32_t *dep, uint32_t gmask,
+                                 const double2 *g) {
+    const int K = 1 << k;
+    const int rows = 1 << (nb - k);
+    for (int o = threadIdx.x; o < rows; o += blockDim.x) {
+        const uint32_t base = dense_row_base((uint32_t)o, gmask, nb);
+        double2 x[1 << kMaxDenseK];
+#pragma unroll
+        for (int c = 0; c < (1 << kMaxDenseK); ++c)
+            if (c < K) x[c] = tile[swz<double>((int)(base | (uint32_t)dep[c]), swm)];
+        for (int r = 0; r < K; ++r) {
+            double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int c = 0; c < (1 << kMaxDenseK); ++c)
+                if (c < K) acc = cfma(g[r * K + c], x[c], acc);
+            tile[swz<double>((int)(base | (uint32_t)dep[r]), swm)] = acc;
+        }
+    }
+    __syncthreads();
+}
+
+// kDense: the pass applies the dense k-qubit gate a.dense over every tile
+// (tile_dense_k_tc / tile_dense_k_f64) instead of the register sweeps.
+template <typename R, bool kCodes, bool kDense>
 __global__ void __launch_bounds__(kStagedThreads, 1) staged_pass_kernel(const PassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(128) unsigned char staged_smem[];
     unsigned char *smem = staged_smem;
     __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ __align__(8) uint64_t s_mma;   // dense complex64: MMA completion
+    __shared__ uint32_t s_tmem;               // dense complex64: TMEM base address
     __shared__ unsigned long long s_tile_off, s_next, s_slab_end;
     __shared__ int s_flag;
     __shared__ int32_t s_tq[kMaxTileQubits];
@@ -879,7 +1093,7 @@ __global__ void __launch_bounds__(kStagedThreads, 1) staged_pass_kernel(const Pa
     const uint32_t nblk = 1u << (a.n - a.B);
     const bool smask = nblk <= kMaxSmemBlocks;
     const uint32_t mask_words = smask ? (nblk + 31) / 32 : 0;
-    const StagedLayout Ly = staged_layout(sizeof(R) == 8, C, j, mask_words);
+    const StagedLayout Ly = staged_layout(sizeof(R) == 8, C, j, mask_words, kDense ? a.dense.k : 0);
 
     T *tile = reinterpret_cast<T *>(smem + Ly.tile);
     // the two slots of each double-buffered region, by pointer arithmetic
@@ -915,7 +1129,48 @@ __global__ void __launch_bounds__(kStagedThreads, 1) staged_pass_kernel(const Pa
             s_sto[b0 >> 5] = ws;
         }
     }
+    // dense gate: its pattern offsets and matrix operands into shared memory;
+    // complex64 also allocates the TMEM accumulator (warp 0)
+    int32_t *dense_dep = nullptr;
+    uint32_t dense_gmask = 0, mma_phase = 0;
+    bool mma_stuck = false;      // a bounded MMA wait gave up: wait again before freeing TMEM
+    if constexpr (kDense) {
+        const int K = 1 << a.dense.k;
+        dense_dep = reinterpret_cast<int32_t *>(smem + Ly.dense_dep);
+        for (int r = threadIdx.x; r < K; r += blockDim.x) {
+            int32_t d = 0;
+            for (int i = 0; i < a.dense.k; ++i) d |= ((r >> i) & 1) << a.dense.pos[i];
+            dense_dep[r] = d;
+        }
+        for (int i = 0; i < a.dense.k; ++i) dense_gmask |= 1u << a.dense.pos[i];
+        if constexpr (sizeof(R) == 4) {
+            const size_t nf = (size_t)4 << (2 * a.dense.k);  // floats per operand part
+            float *bop = reinterpret_cast<float *>(smem + Ly.dense_b);
+            for (size_t i = threadIdx.x; i < nf; i += blockDim.x) {
+                bop[i] = a.dense.bhi[i];
+                bop[nf + i] = a.dense.blo[i];
+            }
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            if (threadIdx.x == 0) {
+                mbar_init(&s_mma, 1);
+                asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+            }
+            if (warp == 0) {
+                asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                                 smem_u32(&s_tmem)),
+                             "r"(kDenseTmemCols)
+                             : "memory");
+                asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+            }
+            tmem_fence_before();
+        } else {
+            const size_t nm = (size_t)2 << (2 * a.dense.k);  // doubles
+            double *g = reinterpret_cast<double *>(smem + Ly.dense_b);
+            for (size_t i = threadIdx.x; i < nm; i += blockDim.x) g[i] = a.dense.mat[i];
+        }
+    }
     __syncthreads();
+    if constexpr (kDense && sizeof(R) == 4) tmem_fence_after();
 
     auto block_active = [&](uint64_t blk) -> bool {
         return smask ? ((s_act[blk >> 5] >> (blk & 31)) & 1u) != 0 : a.group_active[a.block_to_group[blk]] != 0;
@@ -1025,12 +1280,30 @@ __global__ void __launch_bounds__(kStagedThreads, 1) staged_pass_kernel(const Pa
         if (nxt2 != ~0ull) load_headers(nxt2, slot);
 
         // ---- gates
-        tile_sweeps<R, kRegBits>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool),
-                                 outer_word(chunk_base << C, s_oq, a.nouter));
-        if constexpr (!kCodes) {
-            // buf(slot) is free here: it holds the tile's term coefficients
-            if (a.diag.nterms)
-                tile_diag_sum<R>(tile, nb, swm, a.diag, chunk_base << C, reinterpret_cast<double *>(buf(slot)));
+        if constexpr (kDense) {
+            if constexpr (sizeof(R) == 4) {
+                const bool done = tile_dense_k_tc(reinterpret_cast<float2 *>(tile), nb, swm, a.dense.k, dense_dep,
+                                                  dense_gmask, reinterpret_cast<float *>(smem + Ly.dense_a),
+                                                  reinterpret_cast<const float *>(smem + Ly.dense_b), s_tmem,
+                                                  &s_mma, mma_phase);
+                if (!done) {
+                    mma_stuck = true;
+                    if (threadIdx.x == 0) atomicExch(a.error, 2);
+                    break;
+                }
+                mma_phase ^= 1u;
+            } else {
+                tile_dense_k_f64(reinterpret_cast<double2 *>(tile), nb, swm, a.dense.k, dense_dep, dense_gmask,
+                                 reinterpret_cast<const double2 *>(smem + Ly.dense_b));
+            }
+        } else {
+            tile_sweeps<R, kRegBits>(tile, nb, swm, a.sweeps, a.nsweeps, a.ops, reinterpret_cast<const T *>(a.pool),
+                                     outer_word(chunk_base << C, s_oq, a.nouter));
+            if constexpr (!kCodes) {
+                // buf(slot) is free here: it holds the tile's term coefficients
+                if (a.diag.nterms)
+                    tile_diag_sum<R>(tile, nb, swm, a.diag, chunk_base << C, reinterpret_cast<double *>(buf(slot)));
+            }
         }
 
         // ---- quantise (codes replace values in shared memory)
@@ -1117,6 +1390,16 @@ __global__ void __launch_bounds__(kStagedThreads, 1) staged_pass_kernel(const Pa
     for (int s = 0; s < 2; ++s)
         if ((pending >> s) & 1u) (void)mbar_wait_bounded(&s_bar[s], (phase >> s) & 1u);
     __syncthreads();
+    if constexpr (kDense && sizeof(R) == 4) {
+        // every MMA was waited for (or its bounded wait gave up and the loop
+        // stopped); the accumulator is freed by the warp that allocated it
+        if (mma_stuck) (void)mbar_wait_bounded(&s_mma, mma_phase);
+        tmem_fence_after();
+        if (warp == 0)
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(s_tmem),
+                         "r"(kDenseTmemCols)
+                         : "memory");
+    }
     if (rd) atomicAdd(&a.stats[0], rd);
     if (threadIdx.x == 0) {
         if (wr) atomicAdd(&a.stats[1], wr);
@@ -2039,16 +2322,17 @@ static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-template <typename R, bool kCodes>
+template <typename R, bool kCodes, bool kDense = false>
 static cudaError_t launch_staged_t(const PassArgs &a, cudaStream_t s) {
     const uint32_t nblk = 1u << (a.n - a.B);
     const uint32_t mask_words = nblk <= kMaxSmemBlocks ? (nblk + 31) / 32 : 0;
-    const size_t smem = staged_layout(sizeof(R) == 8, a.C, a.j, mask_words).total;
-    cudaError_t e = cudaFuncSetAttribute(staged_pass_kernel<R, kCodes>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    const size_t smem = staged_layout(sizeof(R) == 8, a.C, a.j, mask_words, kDense ? a.dense.k : 0).total;
+    cudaError_t e = cudaFuncSetAttribute(staged_pass_kernel<R, kCodes, kDense>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, staged_pass_kernel<R, kCodes>, kStagedThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, staged_pass_kernel<R, kCodes, kDense>, kStagedThreads,
+                                                      smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t grid = (uint64_t)per_sm * sm_count();
@@ -2058,7 +2342,7 @@ static cudaError_t launch_staged_t(const PassArgs &a, cudaStream_t s) {
     const char *env = std::getenv("QOMPSIM_SLAB_BYTES");
     const uint64_t slab = env ? (uint64_t)std::strtoull(env, nullptr, 10) : (uint64_t)kArenaSlabBytes;
     b.slab = (slab && a.capacity / grid >= 8 * slab) ? (slab + 127) / 128 * 128 : 0;
-    staged_pass_kernel<R, kCodes><<<(unsigned)grid, kStagedThreads, smem, s>>>(b);
+    staged_pass_kernel<R, kCodes, kDense><<<(unsigned)grid, kStagedThreads, smem, s>>>(b);
     return cudaGetLastError();
 }
 
@@ -2070,6 +2354,15 @@ cudaError_t launch_pass(bool f64, const PassArgs &a, int, cudaStream_t s) {
     if (a.rb != kRegBits || a.C + a.j < kRegBits || a.diag.nterms > kMaxDiagTerms) return cudaErrorInvalidValue;
     if (a.code_moves && a.diag.nterms) return cudaErrorInvalidValue;
     if (a.header_batch != 4 && a.header_batch != 8) return cudaErrorInvalidValue;
+    if (a.dense.k) {
+        // one dense k-qubit gate over 2^kDenseTileLog2-amplitude tiles (staged kernel only)
+        if (a.dense.k < kMinDenseK || a.dense.k > kMaxDenseK || a.C + a.j != kDenseTileLog2 || a.code_moves ||
+            a.diag.nterms || !a.staged)
+            return cudaErrorInvalidValue;
+        for (int i = 0; i < a.dense.k; ++i)
+            if (a.dense.pos[i] < 0 || a.dense.pos[i] >= kDenseTileLog2) return cudaErrorInvalidValue;
+        return f64 ? launch_staged_t<double, false, true>(a, s) : launch_staged_t<float, false, true>(a, s);
+    }
     if (a.staged) {
         if (f64) return a.code_moves ? launch_staged_t<double, true>(a, s) : launch_staged_t<double, false>(a, s);
         return a.code_moves ? launch_staged_t<float, true>(a, s) : launch_staged_t<float, false>(a, s);

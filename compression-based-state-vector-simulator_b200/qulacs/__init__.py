@@ -577,6 +577,49 @@ class CompressedQuantumState:
                                                          ca.view(np.float64).ctypes.data_as(_n.ct.POINTER(_n.ct.c_double)),
                                                          len(za)))
 
+    def apply_dense_gate(self, targets, matrix) -> None:
+        """Apply one dense gate on 4 or 5 qubits (matrix bit i <-> targets[i])
+        at once as a stage of its own (qs_apply_dense_gate): complex64 on the
+        tensor cores, complex128 on the CUDA cores."""
+        t = [int(q) for q in targets]
+        m = np.ascontiguousarray(np.asarray(matrix, dtype=np.complex128).reshape(1 << len(t), 1 << len(t)))
+        ta = (_n.ct.c_uint32 * len(t))(*t)
+        self._check(_n.lib().qs_apply_dense_gate(self._h, ta, len(t),
+                                                 m.reshape(-1).view(np.float64).ctypes.data_as(
+                                                     _n.ct.POINTER(_n.ct.c_double))))
+
+    def apply_gates(self, gates: Sequence[QuantumGateBase], inner_size: int = 4) -> None:
+        """Apply a gate list that may hold fused gates on 3 to 5 qubits
+        (QuantumCircuitOptimizer.optimize(c, block_size=k)): every run of
+        gates on at most two qubits is registered and applied as a circuit
+        (the reference's stages), every larger gate as one dense pass; a
+        3-qubit gate is widened to 4 qubits with an idle qubit.  The
+        reference's compressed engine rejects gates on more than two qubits."""
+        from ._gates import full_matrix
+        run: List[QuantumGateBase] = []
+
+        def flush():
+            if run:
+                c = QuantumCircuit(self._n)
+                c._gates = list(run)
+                self.partition_and_register_circuit(c, inner_size, 0)
+                self.apply_circuit()
+                run.clear()
+
+        for g in gates:
+            qs = g.full_qubits()
+            if len(qs) <= 2:
+                run.append(g)
+                continue
+            flush()
+            m, order = full_matrix(g)
+            if len(order) == 3:
+                extra = next(q for q in range(self._n) if q not in order)
+                order = list(order) + [extra]
+                m = np.kron(np.eye(2), m)
+            self.apply_dense_gate(order, m)
+        flush()
+
     def load_pauli_sum(self, source: "CompressedQuantumState", xs, zs, coefs) -> None:
         """self := (sum_t coefs[t] X^{xs[t]} Z^{zs[t]}) source for general
         Pauli strings, with any i^{ny} of Y factors folded into coefs

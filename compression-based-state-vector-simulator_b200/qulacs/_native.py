@@ -116,6 +116,7 @@ SIGNATURES = [
     ("qs_transition_pauli", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),
     ("qs_apply_diagonal_pauli_sum", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_D), ct.c_size_t]),
     ("qs_apply_pauli_sum", ct.c_int, [_P, _P, ct.POINTER(_U64), ct.POINTER(_U64), ct.POINTER(_D), ct.c_size_t]),
+    ("qs_apply_dense_gate", ct.c_int, [_P, ct.POINTER(_U32), _U32, ct.POINTER(_D)]),
     ("qs_adjoint", ct.c_int, [_P, _P, _P, ct.POINTER(_I32), ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t,
                               ct.POINTER(_D), _U32]),
     ("qs_dense_expectation_pauli", ct.c_int, [_P, ct.POINTER(_U64), ct.POINTER(_U64), ct.c_size_t, ct.POINTER(_D)]),

@@ -286,6 +286,19 @@ qs_status qs_apply_pauli_sum(qs_state *out, qs_state *in, const uint64_t *x_mask
 qs_status qs_adjoint(qs_state *psi, qs_state *lam, const qs_gate *gates, const int32_t *slots, const uint64_t *gen_x,
                      const uint64_t *gen_z, size_t count, double *out, uint32_t nslots);
 
+/* One dense k-qubit gate (k = 4 or 5: the gates optimize(c, block_size=k)
+ * fuses; matrix bit i <-> targets[i], row-major 2^k x 2^k complex128,
+ * interleaved) applied to the compressed state at once, as a stage of its
+ * own: groups of blocks differing in the gate's qubits >= block_size, the
+ * reference's zero-mask rule at the end.  One fused pass over tiles of 2^12
+ * amplitudes (at most 12 - chunk_log2 of the targets above the chunk):
+ * complex64 multiplies each tile by the gate on the tensor cores (tcgen05
+ * tf32 MMAs with a 3xTF32 split, FP32 accumulation), complex128 on the CUDA
+ * cores.  The reference's compressed engine rejects gates on more than two
+ * qubits (compressed_state.hpp:1003-1007); this is an extension.  The
+ * statistics describe this pass (qs_get_stats). */
+qs_status qs_apply_dense_gate(qs_state *h, const uint32_t *targets, uint32_t k, const double *matrix);
+
 /* Zero-block mask: out[b] = 1 when block b is stored (the reference's
  * block_pointers[b] != nullptr, compressed_state.hpp:18-19, 319-325). */
 qs_status qs_get_zero_mask(qs_state *h, uint8_t *out);

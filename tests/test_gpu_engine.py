@@ -666,3 +666,61 @@ def test_reference_gpusim_matches_random_circuits(qulacs_mod, n, seed):
     g = gs.get_vector()
     assert np.abs(g - csim_ref.run_circuit(n, c._gates)).max() < F64_TOL
     assert np.abs(_dense_run(qulacs_mod, c, pergate=True) - g).max() < F64_TOL
+
+
+# ------------------------------------------------------------ dense k-qubit gates (tensor cores)
+def _haar(k, rng):
+    z = rng.normal(size=(1 << k, 1 << k)) + 1j * rng.normal(size=(1 << k, 1 << k))
+    q, r = np.linalg.qr(z)
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+@pytest.mark.parametrize("dtype,tol", [("complex128", 1e-9), ("complex64", 3e-5)])
+@pytest.mark.parametrize("targets", [[0, 3, 9, 11, 12], [12, 2, 13, 7], [10, 11, 12, 13, 1]])
+def test_dense_gate_pass_matches_csim(qulacs_mod, dtype, tol, targets):
+    """One dense 4- or 5-qubit gate over the compressed state
+    (qs_apply_dense_gate: complex64 on the tensor cores with a 3xTF32 split,
+    complex128 on the CUDA cores), targets below and above the chunk and the
+    block, against the reference's csim multi-qubit kernel applied to the
+    decoded input state (tight codec bounds); the gate's one-gate stage
+    stores the blocks it reaches."""
+    from qulacs import gate as G
+    n, B = 14, 12
+    rng = np.random.default_rng(sum(targets))
+    c = helpers.optimized(helpers.random_circuit(n, 40, seed=61), B)
+    kw = dict(dtype=dtype, eps_rel=2.0 ** -22 if dtype == "complex128" else 2.0 ** -20, eps_abs=1e-13)
+    cq = _compressed(qulacs_mod, c, B, 3, **kw)
+    v0 = cq.get_vector(renormalize=False)
+    u = _haar(len(targets), rng)
+    cq.apply_dense_gate(targets, u)
+    got = cq.get_vector(renormalize=False)
+    ref = csim_ref.run_circuit(n, [G.DenseMatrix(targets, u)], init=v0)
+    assert np.abs(got - ref).max() < tol
+    assert cq.get_zero_mask().all()
+    assert cq.get_stats()["passes"] == 1
+
+
+@pytest.mark.parametrize("dtype,tol", [("complex128", 1e-8), ("complex64", 1e-4)])
+def test_fused_k_circuit_matches_csim(qulacs_mod, dtype, tol):
+    """A random circuit fused by optimize(block_size=5) into gates on up to
+    five qubits: apply_gates runs the small gates as registered circuits and
+    the fused ones as dense passes; the state matches csim on the same fused
+    gates (tight codec bounds)."""
+    from qulacs.circuit import QuantumCircuitOptimizer
+    n, B = 14, 12
+    c = helpers.random_circuit(n, 120, seed=62)
+    QuantumCircuitOptimizer(sv_block_size=B).optimize(c, block_size=5)
+    big = [g for g in c._gates if len(g.full_qubits()) > 2]
+    assert big
+    ref = csim_ref.run_circuit(n, c._gates)
+    from qulacs import _native
+    cq = qulacs_mod.CompressedQuantumState(n, B, dtype=dtype, flags=_native.QS_FLAG_QUIET,
+                                           eps_rel=2.0 ** -22 if dtype == "complex128" else 2.0 ** -20,
+                                           eps_abs=1e-13)
+    try:
+        cq.apply_gates(c._gates, inner_size=3)
+    except _native.QompsimError as e:
+        # a fused gate with more qubits above the chunk than a tile holds
+        assert e.status == _native.QS_ERR_UNSUPPORTED_GATE
+        pytest.skip(str(e))
+    assert np.abs(cq.get_vector(renormalize=False) - ref).max() < tol
