@@ -900,7 +900,8 @@ struct qs_state {
     uint32_t *arena[2] = {nullptr, nullptr};
     uint64_t capacity = 0;
     bool host_store = false;   // arenas in pinned, device-mapped host memory (QS_FLAG_HOST_STORE)
-    bool staged = true;        // tile passes prefetch payloads with bulk copies (staged_pass_kernel)
+    bool staged = false;       // tile passes prefetch payloads with bulk copies (staged_pass_kernel)
+    bool staged_ok = true;     // the staged kernel can run (HBM arenas): dense k-qubit passes
     unsigned long long *counters = nullptr;  // [0..1] bump, [2..4] stats, [5] init scratch, [6] header-pass bytes, [7] diagonal-pass total
     uint8_t *mask = nullptr;
     uint32_t *block_nz = nullptr;
@@ -1057,9 +1058,17 @@ qs_status qs_create(qs_state **out, uint32_t n, uint32_t block_size, qs_dtype dt
     if (env_int("QOMPSIM_HOST_STORE", 0)) flags |= QS_FLAG_HOST_STORE;
     h->flags = flags;
     h->host_store = (flags & QS_FLAG_HOST_STORE) != 0;
-    // the host-store arenas are read chunk by chunk with cp.async (pass_kernel);
-    // QOMPSIM_STAGED_PASS=0 selects that kernel for HBM stores too
-    h->staged = !h->host_store && env_int("QOMPSIM_STAGED_PASS", 1) != 0;
+    // Tile passes run pass_kernel (three 4-warp CTAs per SM, payloads copied
+    // chunk by chunk with cp.async) unless QOMPSIM_STAGED_PASS=1 selects
+    // staged_pass_kernel (payloads of the next tile prefetched with bulk
+    // copies), which measured 1.3-1.8x slower per pass on the QFT: its
+    // registers leave one 8-warp CTA per SM, and the passes are bound by
+    // the latency of their decode / sweep / quantise phases, not by memory.
+    // Dense k-qubit passes always use the staged kernel (it holds the tensor
+    // core operands); so that they can run, the host-store arenas (read with
+    // cp.async) are excluded from it.
+    h->staged = !h->host_store && env_int("QOMPSIM_STAGED_PASS", 0) != 0;
+    h->staged_ok = !h->host_store;
     h->merge_tail = env_int("QOMPSIM_MERGE_TAIL", 1) != 0;
     h->tile_log2 = env_int("QOMPSIM_TILE_LOG2", h->f64 ? 12 : 13);
     h->tile_log2 = std::max<int>(h->tile_log2, (int)h->C + 2);
@@ -2092,7 +2101,8 @@ qs_status qs_apply_dense_gate(qs_state *h, const uint32_t *targets, uint32_t k, 
     if (!targets || !matrix) return fail(h, QS_ERR_ARG, "NULL argument");
     if (k < (uint32_t)qs::kMinDenseK || k > (uint32_t)qs::kMaxDenseK)
         return fail(h, QS_ERR_UNSUPPORTED_GATE, "dense gates act on 4 or 5 qubits (fused by optimize(block_size=k))");
-    if (!h->staged) return fail(h, QS_ERR_UNSUPPORTED_GATE, "dense k-qubit passes need HBM arenas (not the host store)");
+    if (!h->staged_ok)
+        return fail(h, QS_ERR_UNSUPPORTED_GATE, "dense k-qubit passes need HBM arenas (not the host store)");
     const int C = (int)h->C, n = (int)h->n, B = (int)h->B;
     if (n < qs::kDenseTileLog2) return fail(h, QS_ERR_ARG, "dense k-qubit passes need at least 12 qubits");
     for (uint32_t i = 0; i < k; ++i) {

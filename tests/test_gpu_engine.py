@@ -724,3 +724,22 @@ def test_fused_k_circuit_matches_csim(qulacs_mod, dtype, tol):
         assert e.status == _native.QS_ERR_UNSUPPORTED_GATE
         pytest.skip(str(e))
     assert np.abs(cq.get_vector(renormalize=False) - ref).max() < tol
+
+
+@pytest.mark.parametrize("dtype", ["complex128", "complex64"])
+@pytest.mark.parametrize("circ", ["qft", "random"])
+def test_staged_kernel_bit_identical(qulacs_mod, monkeypatch, dtype, circ):
+    """The staged pass kernel (QOMPSIM_STAGED_PASS=1: next tile's payloads
+    prefetched with bulk copies) runs the same decode, sweeps and quantiser as
+    the default kernel: same decoded state, masks and byte totals."""
+    from qompsim import circuits as C
+    n, B = 16, 9
+    c = helpers.optimized(C.qft_basis(n, 5) if circ == "qft" else helpers.random_circuit(n, 120, seed=71), B)
+    out = []
+    for staged in ("0", "1"):
+        monkeypatch.setenv("QOMPSIM_STAGED_PASS", staged)
+        cq = _compressed(qulacs_mod, c, B, 3, dtype=dtype)
+        out.append((cq.get_vector(renormalize=False), cq.get_zero_mask(), cq.get_SV_bytes_history()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
