@@ -429,6 +429,18 @@ def brickwork_leg(torch, n: int = 32, layers: int = 20, B: int = 22, I: int = 4)
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
+    # the reference's own plain complex128 GPU path (src/gpusim) first, on
+    # its own 64 GiB state, freed before the states below
+    from oracle import gpusim_ref
+    if gpusim_ref.available():
+        gs = gpusim_ref.GpuState(n)
+        recs = gs.prepare(gates)
+        gs.sync()
+        t0 = time.perf_counter()
+        gs.apply_prepared(recs)
+        gs.sync()
+        res["pergate_reference_gpusim_c128_ms"] = (time.perf_counter() - t0) * 1e3
+        del gs
     ds = qulacs.QuantumState(n, dtype="complex128")
     ds.set_computational_basis(0)
     res["pergate_c128_ms"] = timed(lambda: ds._apply_gates(gates, pergate=True))
@@ -460,8 +472,55 @@ def brickwork_leg(torch, n: int = 32, layers: int = 20, B: int = 22, I: int = 4)
                       "max_sv_bytes": cq.get_max_SV_bytes(),
                       "fidelity": float(acc.abs().item()), "max_abs_err": float(err.item()),
                       "speedup_vs_pergate_c128": res["pergate_c128_ms"] / ms}
+        if "pergate_reference_gpusim_c128_ms" in res:
+            res[dtype]["speedup_vs_reference_gpusim_c128"] = res["pergate_reference_gpusim_c128_ms"] / ms
         del cq
     del ds
+    return res
+
+
+def dense_gate_leg(torch, n: int = 30, B: int = 20, reps: int = 5):
+    """One dense 5-qubit gate (Haar random, targets 0, 1, 2, 3 and 8) over a
+    dense compressed state of n qubits (the QFT of a basis state, default
+    bounds): the pass of qs_apply_dense_gate -- complex64 on the tensor cores
+    (tcgen05 kind::tf32, 3xTF32), complex128 on the CUDA cores -- timed with
+    CUDA events, the best of `reps`.  Reported: its time, the tensor-core
+    arithmetic rate (3 MMAs of 2^(k+1) x 2^(k+1) per tile row, 2 flops per
+    multiply-add) and the compressed bytes moved per second."""
+    import numpy as np
+    import qulacs
+    from qulacs import _native
+    from qompsim import circuits as C
+    rng = np.random.default_rng(5)
+    z = rng.normal(size=(32, 32)) + 1j * rng.normal(size=(32, 32))
+    q, r = np.linalg.qr(z)
+    u = q * (np.diag(r) / np.abs(np.diag(r)))
+    targets = [0, 1, 2, 3, 8]
+    res = {"workload": f"dense 5-qubit gate on qubits {targets} of a compressed n={n} state (QFT output), "
+                       f"block_size={B}", "k": 5}
+    c = C.qft_basis(n, seed=0)
+    from qulacs.circuit import QuantumCircuitOptimizer
+    QuantumCircuitOptimizer(sv_block_size=B).optimize(c, block_size=2)
+    for dtype in ("complex64", "complex128"):
+        cq = qulacs.CompressedQuantumState(n, B, dtype=dtype, flags=_native.QS_FLAG_QUIET)
+        cq.partition_and_register_circuit(c, 4, 0)
+        cq.apply_circuit()
+        best = None
+        for _ in range(reps):
+            cq.apply_dense_gate(targets, u)
+            st = cq.get_stats()
+            if best is None or st["kernel_ms"] < best["kernel_ms"]:
+                best = dict(st)
+        ms = best["kernel_ms"]
+        amps = 1 << n
+        # complex64: 3 products of 64 x 64 real MACs per 32 amplitudes = 384 MACs per amplitude;
+        # complex128: 32 complex MACs (4 real FMAs each) per amplitude
+        flops = 2 * 384 * amps if dtype == "complex64" else 2 * 4 * 32 * amps
+        moved = best["bytes_read"] + best["bytes_written"]
+        res[dtype] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12,
+                      "unit_note": "tensor-core TF/s (3xTF32)" if dtype == "complex64" else "FP64 TF/s (CUDA cores)",
+                      "gb_per_s": moved / (ms * 1e-3) / 1e9, "bytes": int(moved)}
+        del cq
     return res
 
 
@@ -658,6 +717,7 @@ def run_ours(args, spec):
             extra["complex64"]["speedup_vs_pergate_c128"] = (dense["pergate_c128"]["ms_per_step"]
                                                              / extra["complex64"]["ms_per_step"])
         extra["adjoint"] = adjoint_leg(torch)
+        extra["dense_gate"] = dense_gate_leg(torch)
         if not args.no_brickwork:
             extra["brickwork32"] = brickwork_leg(torch)
 
@@ -725,7 +785,15 @@ def main():
     ap.add_argument("--no-dense", action="store_true", help="skip the uncompressed per-gate comparison leg")
     ap.add_argument("--no-legs", action="store_true", help="skip the complex64, adjoint-gradient and brickwork legs")
     ap.add_argument("--no-brickwork", action="store_true", help="skip the brickwork n=32 leg")
+    ap.add_argument("--leg", choices=["dense_gate"], default=None,
+                    help="run only this leg and print its JSON (for profiling)")
+    ap.add_argument("--leg-n", type=int, default=None, help="qubits of the --leg workload")
     args = ap.parse_args()
+    if args.leg == "dense_gate":
+        import torch
+        n = args.leg_n or 30
+        print(json.dumps(dense_gate_leg(torch, n=n, B=min(20, n - 4), reps=2)))
+        return
     spec = workload_spec(args.workload)
     if args.impl == "reference":
         run_reference(args, spec)

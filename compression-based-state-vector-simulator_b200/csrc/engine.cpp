@@ -2676,7 +2676,13 @@ static qs_status dual_check(qs_state *A, const qs_state *B) {
     return QS_OK;
 }
 
-constexpr int kDualTileLog2 = 12;
+// Tiles of the two-store passes: 2^12 amplitudes (two value tiles of 64 KB
+// in complex128, 32 KB in complex64); QOMPSIM_DUAL_TILE_LOG2 = 13 doubles
+// them (complex64 only), halving the passes of a gate sequence's qubits.
+static int dual_tile_log2(const qs_state *h) {
+    const int t = env_int("QOMPSIM_DUAL_TILE_LOG2", 12);
+    return (t == 13 && !h->f64) ? 13 : 12;
+}
 
 qs_status qs_apply_pauli_sum(qs_state *out, qs_state *in, const uint64_t *x_masks, const uint64_t *z_masks,
                              const double *coefs, size_t nterms) {
@@ -2689,7 +2695,7 @@ qs_status qs_apply_pauli_sum(qs_state *out, qs_state *in, const uint64_t *x_mask
     const uint64_t full = n >= 64 ? ~0ull : ((1ull << n) - 1);
     for (size_t t = 0; t < nterms; ++t)
         if ((x_masks[t] | z_masks[t]) & ~full) return fail(out, QS_ERR_ARG, "Pauli term acts outside the register");
-    const int jmax = std::min(kDualTileLog2 - C, n - C);
+    const int jmax = std::min(dual_tile_log2(in) - C, n - C);
     // terms in order, grouped so that each group's flip qubits >= C fit a tile
     std::vector<std::vector<size_t>> groups;
     std::vector<std::set<int>> gq;
@@ -2776,7 +2782,7 @@ qs_status qs_adjoint(qs_state *psi, qs_state *lam, const qs_gate *gates, const i
         }
         if (gen_x[i] & ~covered) return fail(psi, QS_ERR_ARG, "a generator flips a qubit its gate does not act on");
     }
-    const int jmax = std::min(kDualTileLog2 - C, n - C);
+    const int jmax = std::min(dual_tile_log2(psi) - C, n - C);
     std::vector<uint32_t> ids(count);
     for (size_t i = 0; i < count; ++i) ids[i] = (uint32_t)i;
     auto pl = plan_passes(ids, cg, C, jmax, jmax, C, n);

@@ -283,17 +283,21 @@ __device__ __forceinline__ void tile_sweeps_body(typename Cplx<R>::T *tile, int 
     const uint32_t wo = ow << nb;
     for (int w = 0; w < nsweeps; ++w) {
         const Sweep sw = sweeps[w];
-        int sb[RB];
+        int sb[RB], bm[RB];
 #pragma unroll
-        for (int k = 0; k < RB; ++k) sb[k] = sw.sbits[k];
-        int off[NS];
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
+        for (int k = 0; k < RB; ++k) {
+            sb[k] = sw.sbits[k];
+            bm[k] = 1 << sb[k];
+        }
+        // offset of group element s: the OR of the masks of its set bits (s is
+        // a compile-time index, so each offset is a few ORs, no table)
+        auto off = [&](int s) {
             int o = 0;
 #pragma unroll
-            for (int k = 0; k < RB; ++k) o |= ((s >> k) & 1) << sb[k];
-            off[s] = o;
-        }
+            for (int k = 0; k < RB; ++k)
+                if ((s >> k) & 1) o |= bm[k];
+            return o;
+        };
         for (int grp = threadIdx.x; grp < groups; grp += blockDim.x) {
             int base = grp;
 #pragma unroll
@@ -304,7 +308,7 @@ __device__ __forceinline__ void tile_sweeps_body(typename Cplx<R>::T *tile, int 
             const uint32_t W = (uint32_t)base | wo;
             T v[NS];
 #pragma unroll
-            for (int s = 0; s < NS; ++s) v[s] = tile[swz<R>(base | off[s], swm)];
+            for (int s = 0; s < NS; ++s) v[s] = tile[swz<R>(base | off(s), swm)];
             T z = c_one<T>();
             for (int k = sw.g0; k < sw.g1; ++k) {
                 const ROp o = ops[k];
@@ -315,7 +319,7 @@ __device__ __forceinline__ void tile_sweeps_body(typename Cplx<R>::T *tile, int 
                 for (int s = 0; s < NS; ++s) v[s] = cmul(z, v[s]);
             }
 #pragma unroll
-            for (int s = 0; s < NS; ++s) tile[swz<R>(base | off[s], swm)] = v[s];
+            for (int s = 0; s < NS; ++s) tile[swz<R>(base | off(s), swm)] = v[s];
         }
         __syncthreads();
     }
