@@ -785,7 +785,7 @@ def main():
     ap.add_argument("--no-dense", action="store_true", help="skip the uncompressed per-gate comparison leg")
     ap.add_argument("--no-legs", action="store_true", help="skip the complex64, adjoint-gradient and brickwork legs")
     ap.add_argument("--no-brickwork", action="store_true", help="skip the brickwork n=32 leg")
-    ap.add_argument("--leg", choices=["dense_gate"], default=None,
+    ap.add_argument("--leg", choices=["dense_gate", "adjoint"], default=None,
                     help="run only this leg and print its JSON (for profiling)")
     ap.add_argument("--leg-n", type=int, default=None, help="qubits of the --leg workload")
     args = ap.parse_args()
@@ -793,6 +793,10 @@ def main():
         import torch
         n = args.leg_n or 30
         print(json.dumps(dense_gate_leg(torch, n=n, B=min(20, n - 4), reps=2)))
+        return
+    if args.leg == "adjoint":
+        import torch
+        print(json.dumps(adjoint_leg(torch, n=args.leg_n or 24)))
         return
     spec = workload_spec(args.workload)
     if args.impl == "reference":

@@ -349,95 +349,136 @@ std::vector<qs::Sweep> plan_sweeps(const std::vector<qs::KGate> &kg, size_t g0, 
 // A register op before its final encoding: kind, register bits, selector
 // sources (< 64: tile bit, >= 64: outer qubit + 64) and its variants in the
 // pool (variant v at mat + v * vstride).
-enum RawKind : uint8_t { RK_SCALAR = 0, RK_D2 = 1, RK_M2 = 2, RK_D4 = 3, RK_M4 = 4 };
+// RK_SUM (two-store sweeps): a derivative sum, xs / zs its register masks,
+// slot its local slot, one +-1 sign per variant (vstride 1).
+enum RawKind : uint8_t { RK_SCALAR = 0, RK_D2 = 1, RK_M2 = 2, RK_D4 = 3, RK_M4 = 4, RK_SUM = 5 };
 struct RawOp {
     uint8_t kind = RK_SCALAR;
     uint8_t k0 = 0, k1 = 0;
     uint8_t nsel = 0;
     uint8_t sel[qs::kMaxSel] = {};
     uint32_t mat = 0, vstride = 0;
+    uint8_t xs = 0, zs = 0;
+    int32_t slot = -1;
 };
+
+void build_gate_op(const qs::KGate &g, const qs::Sweep &sw, int RB, std::vector<RawOp> *ops, std::vector<cplx> *pool);
 
 void build_ops(const std::vector<qs::KGate> &kg, size_t g0, const std::vector<qs::Sweep> &sweeps, int RB,
                std::vector<RawOp> *ops, std::vector<cplx> *pool) {
-    for (const auto &sw : sweeps) {
-        for (int gi = sw.g0; gi < sw.g1; ++gi) {
-            const qs::KGate &g = kg[g0 + gi];
-            int reg[2] = {-1, -1}, src[2] = {0, 0};
-            std::vector<int> fixed;  // gate-qubit indices that select a variant
-            for (int i = 0; i < g.nq; ++i) {
-                const int p = g.tpos[i];
-                int k = -1;
-                for (int kk = 0; kk < RB; ++kk)
-                    if (p >= 0 && sw.sbits[kk] == p) k = kk;
-                if (k >= 0) {
-                    reg[i] = k;
-                } else {
-                    src[i] = p >= 0 ? p : 64 + g.q[i];
-                    fixed.push_back(i);
-                }
-            }
-            const int dim = 1 << g.nq;
-            auto M = [&](int r, int c) { return cplx(g.m[2 * (r * dim + c)], g.m[2 * (r * dim + c) + 1]); };
-            std::vector<int> regs;
-            for (int i = 0; i < g.nq; ++i)
-                if (reg[i] >= 0) regs.push_back(i);
-            RawOp op{};
-            op.nsel = (uint8_t)fixed.size();
-            for (size_t j = 0; j < fixed.size(); ++j) op.sel[j] = (uint8_t)src[fixed[j]];
-            op.mat = (uint32_t)pool->size();
-            const int nvar = 1 << fixed.size();
-            // full-matrix index of register pattern x under variant v
-            auto full = [&](int x, int v) {
-                int idx = 0;
-                for (size_t r = 0; r < regs.size(); ++r)
-                    if ((x >> r) & 1) idx |= 1 << regs[r];
-                for (size_t j = 0; j < fixed.size(); ++j)
-                    if ((v >> j) & 1) idx |= 1 << fixed[j];
-                return idx;
-            };
-            const int rd = 1 << regs.size();
-            bool diag = true;
-            for (int v = 0; v < nvar; ++v)
-                for (int x = 0; x < rd; ++x)
-                    for (int y = 0; y < rd; ++y)
-                        if (x != y && M(full(x, v), full(y, v)) != cplx(0, 0)) diag = false;
-            if (regs.empty()) {
-                op.kind = RK_SCALAR;
-                op.vstride = 1;
-                for (int v = 0; v < nvar; ++v) pool->push_back(M(full(0, v), full(0, v)));
-            } else if (regs.size() == 1) {
-                op.k0 = (uint8_t)reg[regs[0]];
-                if (diag) {
-                    op.kind = RK_D2;
-                    op.vstride = 2;
-                    for (int v = 0; v < nvar; ++v) {
-                        pool->push_back(M(full(0, v), full(0, v)));
-                        pool->push_back(M(full(1, v), full(1, v)));
-                    }
-                } else {
-                    op.kind = RK_M2;
-                    op.vstride = 4;
-                    for (int v = 0; v < nvar; ++v)
-                        for (int x = 0; x < 2; ++x)
-                            for (int y = 0; y < 2; ++y) pool->push_back(M(full(x, v), full(y, v)));
-                }
-            } else {
-                op.k0 = (uint8_t)reg[0];
-                op.k1 = (uint8_t)reg[1];
-                if (diag) {
-                    op.kind = RK_D4;
-                    op.vstride = 4;
-                    for (int x = 0; x < 4; ++x) pool->push_back(M(x, x));
-                } else {
-                    op.kind = RK_M4;
-                    op.vstride = 16;
-                    for (int x = 0; x < 16; ++x) pool->push_back(M(x / 4, x % 4));
-                }
-            }
-            ops->push_back(op);
+    for (const auto &sw : sweeps)
+        for (int gi = sw.g0; gi < sw.g1; ++gi) build_gate_op(kg[g0 + gi], sw, RB, ops, pool);
+}
+
+// The derivative sum of a gate whose generator has flip mask gx and Z mask gz
+// (global qubits), as a register op of sweep sw: flips must lie on register
+// bits; Z factors on other qubits select a +-1 variant.  tile: the pass's
+// tile qubits >= C.  False when a flip qubit is not a register bit.
+bool build_sum_op(uint64_t gx, uint64_t gz, int slot, const qs::Sweep &sw, int RB, const std::vector<int> &tile, int C,
+                  std::vector<RawOp> *ops, std::vector<cplx> *pool) {
+    RawOp op{};
+    op.kind = RK_SUM;
+    op.slot = slot;
+    op.vstride = 1;
+    for (int q = 0; q < 64; ++q) {
+        const bool xb = (gx >> q) & 1, zb = (gz >> q) & 1;
+        if (!xb && !zb) continue;
+        int p = q < C ? q : -1;
+        if (q >= C) {
+            auto it = std::find(tile.begin(), tile.end(), q);
+            if (it != tile.end()) p = C + (int)(it - tile.begin());
+        }
+        int k = -1;
+        for (int kk = 0; kk < RB; ++kk)
+            if (p >= 0 && sw.sbits[kk] == p) k = kk;
+        if (k >= 0) {
+            op.xs |= (uint8_t)(xb << k);
+            op.zs |= (uint8_t)(zb << k);
+        } else {
+            if (xb || op.nsel >= qs::kMaxSel) return false;
+            op.sel[op.nsel++] = (uint8_t)(p >= 0 ? p : 64 + q);
         }
     }
+    op.mat = (uint32_t)pool->size();
+    for (int v = 0; v < (1 << op.nsel); ++v) pool->push_back(cplx((__builtin_popcount(v) & 1) ? -1.0 : 1.0, 0.0));
+    ops->push_back(op);
+    return true;
+}
+
+void build_gate_op(const qs::KGate &g, const qs::Sweep &sw, int RB, std::vector<RawOp> *ops, std::vector<cplx> *pool) {
+    int reg[2] = {-1, -1}, src[2] = {0, 0};
+    std::vector<int> fixed;  // gate-qubit indices that select a variant
+    for (int i = 0; i < g.nq; ++i) {
+        const int p = g.tpos[i];
+        int k = -1;
+        for (int kk = 0; kk < RB; ++kk)
+            if (p >= 0 && sw.sbits[kk] == p) k = kk;
+        if (k >= 0) {
+            reg[i] = k;
+        } else {
+            src[i] = p >= 0 ? p : 64 + g.q[i];
+            fixed.push_back(i);
+        }
+    }
+    const int dim = 1 << g.nq;
+    auto M = [&](int r, int c) { return cplx(g.m[2 * (r * dim + c)], g.m[2 * (r * dim + c) + 1]); };
+    std::vector<int> regs;
+    for (int i = 0; i < g.nq; ++i)
+        if (reg[i] >= 0) regs.push_back(i);
+    RawOp op{};
+    op.nsel = (uint8_t)fixed.size();
+    for (size_t j = 0; j < fixed.size(); ++j) op.sel[j] = (uint8_t)src[fixed[j]];
+    op.mat = (uint32_t)pool->size();
+    const int nvar = 1 << fixed.size();
+    // full-matrix index of register pattern x under variant v
+    auto full = [&](int x, int v) {
+        int idx = 0;
+        for (size_t r = 0; r < regs.size(); ++r)
+            if ((x >> r) & 1) idx |= 1 << regs[r];
+        for (size_t j = 0; j < fixed.size(); ++j)
+            if ((v >> j) & 1) idx |= 1 << fixed[j];
+        return idx;
+    };
+    const int rd = 1 << regs.size();
+    bool diag = true;
+    for (int v = 0; v < nvar; ++v)
+        for (int x = 0; x < rd; ++x)
+            for (int y = 0; y < rd; ++y)
+                if (x != y && M(full(x, v), full(y, v)) != cplx(0, 0)) diag = false;
+    if (regs.empty()) {
+        op.kind = RK_SCALAR;
+        op.vstride = 1;
+        for (int v = 0; v < nvar; ++v) pool->push_back(M(full(0, v), full(0, v)));
+    } else if (regs.size() == 1) {
+        op.k0 = (uint8_t)reg[regs[0]];
+        if (diag) {
+            op.kind = RK_D2;
+            op.vstride = 2;
+            for (int v = 0; v < nvar; ++v) {
+                pool->push_back(M(full(0, v), full(0, v)));
+                pool->push_back(M(full(1, v), full(1, v)));
+            }
+        } else {
+            op.kind = RK_M2;
+            op.vstride = 4;
+            for (int v = 0; v < nvar; ++v)
+                for (int x = 0; x < 2; ++x)
+                    for (int y = 0; y < 2; ++y) pool->push_back(M(full(x, v), full(y, v)));
+        }
+    } else {
+        op.k0 = (uint8_t)reg[0];
+        op.k1 = (uint8_t)reg[1];
+        if (diag) {
+            op.kind = RK_D4;
+            op.vstride = 4;
+            for (int x = 0; x < 4; ++x) pool->push_back(M(x, x));
+        } else {
+            op.kind = RK_M4;
+            op.vstride = 16;
+            for (int x = 0; x < 16; ++x) pool->push_back(M(x / 4, x % 4));
+        }
+    }
+    ops->push_back(op);
 }
 
 // Merge runs of diagonal ops: a SCALAR or D2 op followed by SCALAR / D2 ops
@@ -562,6 +603,12 @@ bool finalize_ops(const std::vector<RawOp> &raw, const std::vector<cplx> &rpool,
         const bool flip = r.k0 > r.k1;  // canonical index: bit 0 <-> the lower register bit
         auto canon = [&](int x) { return flip ? (((x & 1) << 1) | (x >> 1)) : x; };
         switch (r.kind) {
+            case RK_SUM:
+                o.code = qs::OPC_SUM;
+                o.vstride = (uint8_t)r.slot;
+                o.pad = (uint8_t)((r.xs << 4) | r.zs);
+                for (int v = 0; v < nvar; ++v) pool->push_back(E(v, 0));
+                break;
             case RK_SCALAR:
                 o.code = qs::OPC_SCALAR;
                 o.vstride = 1;
@@ -2579,11 +2626,30 @@ qs_status qs_apply_diagonal_pauli_sum(qs_state *out, const qs_state *in, const u
 // One launch of dual_pass_kernel over A and B with the tile qubits `tile`;
 // ops and sums already on the device.  Written stores switch to their other
 // arena; afterwards every block of a written store is stored.
+// Register sweeps of a two-store launch (device pointers; see DualPassArgs).
+struct DualSweepRef {
+    const qs::Sweep *sweeps = nullptr;
+    int nsweeps = 0, rb = 0;
+    const qs::ROp *rops = nullptr;
+    const void *pool = nullptr;
+    const std::vector<int> *outer = nullptr;
+};
+
 static qs_status dual_launch(qs_state *A, qs_state *B, const std::vector<int> &tile, const qs::DualOp *ops,
-                             int nops, bool write_a, bool b_zero, double *sums, int nslots) {
+                             int nops, bool write_a, bool b_zero, double *sums, int nslots,
+                             const DualSweepRef *sw = nullptr) {
     cudaStream_t s = A->stream;
     const int C = (int)A->C;
     qs::DualPassArgs d{};
+    if (sw && sw->nsweeps > 0) {
+        d.sweeps = sw->sweeps;
+        d.nsweeps = sw->nsweeps;
+        d.rb = sw->rb;
+        d.rops = sw->rops;
+        d.pool = sw->pool;
+        d.nouter = (int32_t)sw->outer->size();
+        for (int i = 0; i < d.nouter; ++i) d.outer_q[i] = (int8_t)(*sw->outer)[i];
+    }
     d.n = (int)A->n;
     d.B = (int)A->B;
     d.C = C;
@@ -2785,13 +2851,25 @@ qs_status qs_adjoint(qs_state *psi, qs_state *lam, const qs_gate *gates, const i
     const int jmax = std::min(dual_tile_log2(psi) - C, n - C);
     std::vector<uint32_t> ids(count);
     for (size_t i = 0; i < count; ++i) ids[i] = (uint32_t)i;
-    auto pl = plan_passes(ids, cg, C, jmax, jmax, C, n);
+    // Commuting gates may change places here too: a gate G moved across the
+    // derivative sum of gate k commutes with U_k, so it shares with U_k only
+    // qubits on which neither mixes, and there P_k is I or Z (its flip qubits
+    // count as mixing qubits of gate k above); then G commutes with P_k and
+    // <G^-1 lam| P_k |G^-1 psi> = <lam| P_k |psi>.
+    auto pl = env_int("QOMPSIM_DAG_PLAN", 1) ? plan_passes_dag(ids, cg, C, jmax, jmax, C, n)
+                                             : plan_passes(ids, cg, C, jmax, jmax, C, n);
     // launches: a pass's gates, split so that each launch has at most
     // kMaxDualSlots derivative sums
     struct Launch {
         std::vector<int> tile;
         size_t op_off, nops, out_off;
         std::vector<int32_t> local_to_global;
+        std::vector<uint32_t> gates;
+        // register sweeps over both stores (fused = false: one shared-memory
+        // sweep per DualOp instead)
+        bool fused = false;
+        size_t sw_off = 0, nsw = 0, rop_off = 0;
+        std::vector<int> outer;
     };
     std::vector<qs::DualOp> ops;
     std::vector<Launch> launches;
@@ -2818,11 +2896,69 @@ qs_status qs_adjoint(qs_state *psi, qs_state *lam, const qs_gate *gates, const i
                 o.kind = qs::DOP_GATE_AB;
                 o.g = to_kgate(cg[gi], p.tile, C);
                 ops.push_back(o);
+                L.gates.push_back(gi);
             }
             L.nops = ops.size() - L.op_off;
             nout += L.local_to_global.size();
             launches.push_back(std::move(L));
             g0 = g1;
+        }
+    }
+    // Register sweeps for every launch: the launch's gates in order, each
+    // parametric gate's derivative sum placed just before it (a pseudo-gate
+    // with the gate's qubits and mixing bits, so that the two share a sweep
+    // and the generator's flip qubits are register bits).
+    const int RB = psi->f64 ? qs::kDualRegBitsF64 : qs::kDualRegBitsF32;
+    std::vector<qs::Sweep> all_sw;
+    std::vector<qs::ROp> all_rops;
+    std::vector<cplx> all_pool;
+    if (env_int("QOMPSIM_DUAL_SWEEPS", 1)) {
+        for (Launch &L : launches) {
+            const int nb = C + (int)L.tile.size();
+            if (nb < RB) continue;
+            std::vector<qs::KGate> kg;
+            std::vector<int32_t> sum_slot;
+            std::vector<uint32_t> gid;
+            int32_t ls = 0;
+            for (uint32_t gi : L.gates) {
+                const qs::KGate g = to_kgate(cg[gi], L.tile, C);
+                if (slots[gi] >= 0) {
+                    kg.push_back(g);
+                    sum_slot.push_back(ls++);
+                    gid.push_back(gi);
+                }
+                kg.push_back(g);
+                sum_slot.push_back(-1);
+                gid.push_back(gi);
+            }
+            const auto sweeps = plan_sweeps(kg, 0, kg.size(), nb, RB);
+            std::vector<RawOp> raw;
+            std::vector<cplx> rpool;
+            bool ok = true;
+            for (const auto &sw : sweeps)
+                for (int i = sw.g0; i < sw.g1 && ok; ++i) {
+                    if (sum_slot[i] >= 0)
+                        ok = build_sum_op(gen_x[gid[i]], gen_z[gid[i]], sum_slot[i], sw, RB, L.tile, C, &raw, &rpool);
+                    else
+                        build_gate_op(kg[i], sw, RB, &raw, &rpool);
+                }
+            if (!ok) continue;
+            std::vector<qs::Sweep> msw;
+            merge_diagonal_ops(sweeps, 0, &raw, &rpool, &msw);
+            std::vector<qs::ROp> rops;
+            std::vector<int> outer;
+            const size_t pool0 = all_pool.size();
+            if (!finalize_ops(raw, rpool, nb, &outer, &rops, &all_pool)) {
+                all_pool.resize(pool0);
+                continue;
+            }
+            L.fused = true;
+            L.sw_off = all_sw.size();
+            L.nsw = msw.size();
+            L.rop_off = all_rops.size();
+            L.outer = outer;
+            all_sw.insert(all_sw.end(), msw.begin(), msw.end());
+            all_rops.insert(all_rops.end(), rops.begin(), rops.end());
         }
     }
     qs::DualOp *dops = nullptr;
@@ -2832,13 +2968,44 @@ qs_status qs_adjoint(qs_state *psi, qs_state *lam, const qs_gate *gates, const i
     CUDA_TRY(psi, cudaMalloc(&dsum, std::max<size_t>(1, 2 * nout) * sizeof(double)));
     Free f2{dsum};
     cudaStream_t s = psi->stream;
+    qs::Sweep *dsw = nullptr;
+    qs::ROp *drops = nullptr;
+    void *dpool = nullptr;
+    const size_t pool_bytes = all_pool.size() * (psi->f64 ? 16 : 8);
+    CUDA_TRY(psi, cudaMalloc(&dsw, std::max<size_t>(1, all_sw.size()) * sizeof(qs::Sweep)));
+    Free f3{dsw};
+    CUDA_TRY(psi, cudaMalloc(&drops, std::max<size_t>(1, all_rops.size()) * sizeof(qs::ROp)));
+    Free f4{drops};
+    CUDA_TRY(psi, cudaMalloc(&dpool, std::max<size_t>(16, pool_bytes)));
+    Free f5{dpool};
+    std::vector<float> pool_f;
+    std::vector<double> pool_d;
+    if (psi->f64) pool_d = pool_as<double>(all_pool);
+    else pool_f = pool_as<float>(all_pool);
+    if (!all_sw.empty())
+        CUDA_TRY(psi, cudaMemcpyAsync(dsw, all_sw.data(), all_sw.size() * sizeof(qs::Sweep), cudaMemcpyHostToDevice, s));
+    if (!all_rops.empty())
+        CUDA_TRY(psi, cudaMemcpyAsync(drops, all_rops.data(), all_rops.size() * sizeof(qs::ROp), cudaMemcpyHostToDevice,
+                                      s));
+    if (pool_bytes)
+        CUDA_TRY(psi, cudaMemcpyAsync(dpool, psi->f64 ? (const void *)pool_d.data() : (const void *)pool_f.data(),
+                                      pool_bytes, cudaMemcpyHostToDevice, s));
     if (!ops.empty())
         CUDA_TRY(psi, cudaMemcpyAsync(dops, ops.data(), ops.size() * sizeof(qs::DualOp), cudaMemcpyHostToDevice, s));
     CUDA_TRY(psi, cudaMemsetAsync(dsum, 0, std::max<size_t>(1, 2 * nout) * sizeof(double), s));
     CUDA_TRY(psi, cudaMemsetAsync(psi->error_dev, 0, sizeof(int32_t), s));
     for (const Launch &L : launches) {
+        DualSweepRef ref{};
+        if (L.fused) {
+            ref.sweeps = dsw + L.sw_off;
+            ref.nsweeps = (int)L.nsw;
+            ref.rb = RB;
+            ref.rops = drops + L.rop_off;
+            ref.pool = dpool;
+            ref.outer = &L.outer;
+        }
         st = dual_launch(psi, lam, L.tile, dops + L.op_off, (int)L.nops, true, false, dsum + 2 * L.out_off,
-                         (int)L.local_to_global.size());
+                         (int)L.local_to_global.size(), L.fused ? &ref : nullptr);
         if (st != QS_OK) return st;
     }
     std::vector<double> h(2 * nout);
@@ -3157,7 +3324,8 @@ qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) 
     if ((int)h->n < RB) return qs_dense_apply_gates_pergate(h, gates, count);
     std::vector<uint32_t> ids(count);
     for (size_t i = 0; i < count; ++i) ids[i] = (uint32_t)i;
-    auto pl = plan_passes(ids, cg, C, jmax, std::min(jmax, 3), C, (int)h->n);
+    auto pl = env_int("QOMPSIM_DAG_PLAN", 1) ? plan_passes_dag(ids, cg, C, jmax, std::min(jmax, 3), C, (int)h->n)
+                                             : plan_passes(ids, cg, C, jmax, std::min(jmax, 3), C, (int)h->n);
     std::vector<qs::KGate> kg;
     std::vector<qs::Sweep> sw;
     std::vector<qs::ROp> ops;
@@ -3471,7 +3639,9 @@ qs_status qs_dense_adjoint(qs_dense *psi, qs_dense *lam, const qs_gate *gates, c
     }
     std::vector<uint32_t> ids(count);
     for (size_t i = 0; i < count; ++i) ids[i] = (uint32_t)i;
-    auto pl = plan_passes(ids, cg, C, jmax, std::min(jmax, 3), C, n);
+    // commuting gates may change places (the argument at qs_adjoint holds here)
+    auto pl = env_int("QOMPSIM_DAG_PLAN", 1) ? plan_passes_dag(ids, cg, C, jmax, std::min(jmax, 3), C, n)
+                                             : plan_passes(ids, cg, C, jmax, std::min(jmax, 3), C, n);
     // every launch's gate records (at most 128 parametric gates each) are
     // built first and uploaded at once; the launches then run back to back
     // and their slot sums are read back with one copy at the end

@@ -83,10 +83,17 @@ constexpr int kSweepThreads = 128;
 //   OPC_D4H + (a*8+b)    diag(1, m0, m1, m2) on bits a < b
 //   OPC_M4  + (a*8+b)    4x4 matrix m0..m15 on bits a < b
 //   OPC_SWAP + (a*8+b)   exchange bits a and b (no arithmetic)
+//   OPC_SUM              two-store sweeps only: derivative sum, see below
 enum : uint8_t {
     OPC_SCALAR = 0, OPC_D2 = 8, OPC_D2H = 16, OPC_M2 = 24, OPC_X = 32,
-    OPC_D4 = 64, OPC_D4H = 96, OPC_M4 = 128, OPC_SWAP = 160
+    OPC_D4 = 64, OPC_D4H = 96, OPC_M4 = 128, OPC_SWAP = 160, OPC_SUM = 224
 };
+// OPC_SUM in a two-store sweep (groups v of store A and w of store B at the
+// same tile positions): sums[slot] += f * sum_s conj(w[s ^ xs]) (-1)^{|s & zs|} v[s],
+// xs / zs = the generator's flip / Z qubits among the register bits
+// (ROp.pad = xs << 4 | zs), slot = ROp.vstride, and f = +-1 (variant real
+// part) the sign of its Z qubits among the selector bits.  The stores' lazy
+// scalar factors enter as conj(zB) zA.
 constexpr int kMaxSel = 8;
 constexpr uint8_t kSelNone = 31;
 struct ROp {
@@ -299,6 +306,10 @@ struct DualOp {
     int32_t slot;
 };
 constexpr int kMaxDualSlots = 128;
+// Register bits of the two-store sweeps: two groups (one per store) of
+// 2^rb amplitudes are held at once.
+constexpr int kDualRegBitsF32 = 4;
+constexpr int kDualRegBitsF64 = 3;
 struct DualStore {
     const ChunkMeta *meta_in;   // NULL: the store starts the pass at zero (B only)
     const uint32_t *arena_in;
@@ -315,6 +326,15 @@ struct DualPassArgs {
     uint64_t n_tiles;
     const DualOp *ops;
     int32_t nops;
+    // register sweeps over both stores (nsweeps > 0: used instead of ops):
+    // gates as ROps applied to both groups, derivative sums as OPC_SUM
+    const Sweep *sweeps;
+    int32_t nsweeps;
+    int32_t rb;                 // register bits: kDualRegBitsF32 / kDualRegBitsF64
+    const ROp *rops;
+    const void *pool;           // variants, complex of the store's precision
+    int8_t outer_q[kMaxOuterSel];
+    int32_t nouter;
     CodecParams codec;
     DualStore a, b;
     double *sums;               // 2 doubles per slot

@@ -2107,7 +2107,12 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_pass_kernel(const AdjPass
 // B), and each written store is re-encoded into its output arena with one
 // reservation per tile.  Blocks not stored at the start of the pass read as
 // zeros; every chunk of a written store is written.
+// Threads of a two-store pass CTA: 8 warps for tiles of 2^12 amplitudes (two
+// CTAs per SM), 16 warps for 2^13-amplitude complex64 tiles, whose two value
+// tiles (128 KB) leave room for one CTA per SM.
 constexpr int kDualThreads = 256;
+constexpr int kDualThreadsWide = 512;
+inline int dual_threads(int nb) { return nb >= 13 ? kDualThreadsWide : kDualThreads; }
 
 template <typename R>
 __device__ void dual_decode_tile(const DualStore &st, int C, int j, int blk_shift, uint64_t chunk_base,
@@ -2181,8 +2186,125 @@ __device__ bool dual_encode_tile(const DualStore &st, int C, int j, int blk_shif
     return true;
 }
 
+// sum_s conj(w[s ^ X]) (-1)^{|s & zs|} v[s] over a register group, X a
+// compile-time flip mask (the caller dispatches on the op's mask).
+template <int NS, int X, typename T>
+__device__ __forceinline__ void group_pauli_sum(const T (&v)[NS], const T (&w)[NS], int zs, double &re, double &im) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const T a = v[s], b = w[s ^ X];
+        double pr = (double)b.x * (double)a.x + (double)b.y * (double)a.y;
+        double pi = (double)b.x * (double)a.y - (double)b.y * (double)a.x;
+        const double sg = (__popc(s & zs) & 1) ? -1.0 : 1.0;
+        re = fma(sg, pr, re);
+        im = fma(sg, pi, im);
+    }
+}
+
+template <int RB, typename T>
+__device__ __forceinline__ void group_pauli_sum_any(const T (&v)[1 << RB], const T (&w)[1 << RB], int xs, int zs,
+                                                    double &re, double &im) {
+    constexpr int NS = 1 << RB;
+#define QS_GS(X) \
+    case X:      \
+        if constexpr ((X) < NS) group_pauli_sum<NS, (X)>(v, w, zs, re, im); \
+        break;
+    switch (xs) {
+        QS_GS(0) QS_GS(1) QS_GS(2) QS_GS(3) QS_GS(4) QS_GS(5) QS_GS(6) QS_GS(7)
+        QS_GS(8) QS_GS(9) QS_GS(10) QS_GS(11) QS_GS(12) QS_GS(13) QS_GS(14) QS_GS(15)
+        default: break;
+    }
+#undef QS_GS
+}
+
+// Register sweeps over the two tiles of a two-store pass: each thread holds
+// the group of store A (v) and the group of store B (w) at the same 2^RB tile
+// positions, applies every gate op of the sweep to both, and at each OPC_SUM
+// adds the group's share of the derivative sum to s_acc (warp sums, one
+// shared-memory atomic per warp).  Tiles are in the linear layout.  The
+// group loop runs the same trip count in every warp, so that the warp sums
+// see all 32 lanes.
+template <typename R, int RB>
+__device__ void dual_tile_sweeps(typename Cplx<R>::T *tA, typename Cplx<R>::T *tB, int nb, const Sweep *__restrict__ sweeps,
+                                 int nsweeps, const ROp *__restrict__ ops, const typename Cplx<R>::T *__restrict__ pool,
+                                 uint32_t ow, double *s_acc, int lane) {
+    using T = typename Cplx<R>::T;
+    constexpr int NS = 1 << RB;
+    const int groups = 1 << (nb - RB);
+    const uint32_t wo = ow << nb;
+    for (int sidx = 0; sidx < nsweeps; ++sidx) {
+        const Sweep sw = sweeps[sidx];
+        int sb[RB], bm[RB];
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+            sb[k] = sw.sbits[k];
+            bm[k] = 1 << sb[k];
+        }
+        auto off = [&](int s) {
+            int o = 0;
+#pragma unroll
+            for (int k = 0; k < RB; ++k)
+                if ((s >> k) & 1) o |= bm[k];
+            return o;
+        };
+        for (int g0 = 0; g0 < groups; g0 += blockDim.x) {
+            const int grp = g0 + threadIdx.x;
+            const bool live = grp < groups;
+            int base = live ? grp : 0;
+#pragma unroll
+            for (int k = 0; k < RB; ++k) {
+                const int t = sb[k];
+                base = ((base >> t) << (t + 1)) | (base & ((1 << t) - 1));
+            }
+            const uint32_t W = (uint32_t)base | wo;
+            T v[NS], w[NS];
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                v[s] = live ? tA[base | off(s)] : make_c<T, R>(0.0, 0.0);
+                w[s] = live ? tB[base | off(s)] : make_c<T, R>(0.0, 0.0);
+            }
+            T za = c_one<T>(), zb = c_one<T>();
+            for (int k = sw.g0; k < sw.g1; ++k) {
+                const ROp o = ops[k];
+                if (o.code == OPC_SUM) {
+                    const T f = pool[o.mat + rop_variant(o, W)];
+                    double re = 0.0, im = 0.0;
+                    group_pauli_sum_any<RB>(v, w, o.pad >> 4, o.pad & 15, re, im);
+                    // conj(zb) za f (re + i im)
+                    const double cr = (double)zb.x * (double)za.x + (double)zb.y * (double)za.y;
+                    const double ci = (double)zb.x * (double)za.y - (double)zb.y * (double)za.x;
+                    const double fr = (double)f.x;
+                    double sr = fr * (cr * re - ci * im), si = fr * (cr * im + ci * re);
+#pragma unroll
+                    for (int d = 16; d > 0; d >>= 1) {
+                        sr += __shfl_xor_sync(0xffffffffu, sr, d);
+                        si += __shfl_xor_sync(0xffffffffu, si, d);
+                    }
+                    if (lane == 0) {
+                        atomicAdd(&s_acc[2 * o.vstride], sr);
+                        atomicAdd(&s_acc[2 * o.vstride + 1], si);
+                    }
+                } else {
+                    const T *m = pool + o.mat + rop_variant(o, W) * o.vstride;
+                    apply_rop<RB>(v, za, o.code, m);
+                    apply_rop<RB>(w, zb, o.code, m);
+                }
+            }
+            if (live) {
+                const bool sa = za.x != R(1) || za.y != R(0), sbz = zb.x != R(1) || zb.y != R(0);
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    tA[base | off(s)] = sa ? cmul(za, v[s]) : v[s];
+                    tB[base | off(s)] = sbz ? cmul(zb, w[s]) : w[s];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 template <typename R>
-__global__ void __launch_bounds__(kDualThreads) dual_pass_kernel(const DualPassArgs a) {
+__global__ void __launch_bounds__(kDualThreadsWide) dual_pass_kernel(const DualPassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char dual_smem[];
     __shared__ double s_acc[2 * kMaxDualSlots];
@@ -2210,7 +2332,17 @@ __global__ void __launch_bounds__(kDualThreads) dual_pass_kernel(const DualPassA
         dual_decode_tile<R>(a.b, C, j, blk_shift, chunk_base, s_tq, a.codec, reinterpret_cast<R *>(tB), wstage,
                             warp, nwarps, lane);
         __syncthreads();
-        for (int k = 0; k < a.nops; ++k) {
+        if (a.nsweeps > 0) {
+            uint32_t ow = 0;
+            for (int i = 0; i < a.nouter; ++i) ow |= (uint32_t)((base_amp >> a.outer_q[i]) & 1u) << i;
+            if constexpr (sizeof(R) == 4)
+                dual_tile_sweeps<R, kDualRegBitsF32>(tA, tB, nb, a.sweeps, a.nsweeps, a.rops,
+                                                     reinterpret_cast<const T *>(a.pool), ow, s_acc, lane);
+            else
+                dual_tile_sweeps<R, kDualRegBitsF64>(tA, tB, nb, a.sweeps, a.nsweeps, a.rops,
+                                                     reinterpret_cast<const T *>(a.pool), ow, s_acc, lane);
+        }
+        for (int k = 0; k < (a.nsweeps > 0 ? 0 : a.nops); ++k) {
             const DualOp &op = a.ops[k];
             if (op.kind == DOP_SUM) {
                 const int outer = __popcll(base_amp & op.term.zo) & 1;
@@ -2263,7 +2395,7 @@ __global__ void __launch_bounds__(kDualThreads) dual_pass_kernel(const DualPassA
 size_t dual_pass_smem_bytes(bool f64, int C, int j) {
     const size_t nch = (size_t)1 << j;
     // two value tiles, the warps' staging areas, then base, width and offset per chunk
-    return ((size_t)2 * (f64 ? 16 : 8) << (C + j)) + (size_t)(kDualThreads / 32) * kStageWords * 4 + 16 * nch;
+    return ((size_t)2 * (f64 ? 16 : 8) << (C + j)) + (size_t)(dual_threads(C + j) / 32) * kStageWords * 4 + 16 * nch;
 }
 
 // Imported stores: the header of every chunk of an unstored block is set to
@@ -2522,17 +2654,21 @@ uint64_t noalloc_scratch_words() { return kNoAllocScratchWords; }
 template <typename R>
 static cudaError_t launch_dual_t(const DualPassArgs &a, cudaStream_t s) {
     if (a.nslots > kMaxDualSlots) return cudaErrorInvalidValue;
+    if (a.nsweeps > 0 && (a.rb != (sizeof(R) == 8 ? kDualRegBitsF64 : kDualRegBitsF32) || a.C + a.j < a.rb ||
+                          a.nouter < 0 || a.nouter > kMaxOuterSel || !a.sweeps || !a.rops || !a.pool))
+        return cudaErrorInvalidValue;
     const size_t smem = dual_pass_smem_bytes(sizeof(R) == 8, a.C, a.j);
     cudaError_t e = cudaFuncSetAttribute(dual_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dual_pass_kernel<R>, kDualThreads, smem);
+    const int threads = dual_threads(a.C + a.j);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dual_pass_kernel<R>, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t grid = (uint64_t)per_sm * sm_count();
     if (grid > a.n_tiles) grid = a.n_tiles;
     if (grid == 0) grid = 1;
-    dual_pass_kernel<R><<<(unsigned)grid, kDualThreads, smem, s>>>(a);
+    dual_pass_kernel<R><<<(unsigned)grid, threads, smem, s>>>(a);
     return cudaGetLastError();
 }
 

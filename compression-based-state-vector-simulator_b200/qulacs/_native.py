@@ -224,9 +224,9 @@ def make_gate_array(gates):
             rec.controls[k] = c
             rec.control_values[k] = v
         m = np.ascontiguousarray(g.get_matrix(), dtype=np.complex128).reshape(-1)
-        flat = m.view(np.float64)
-        for k in range(flat.size):
-            rec.matrix[k] = flat[k]
+        if m.size > 16:
+            raise QompsimError(QS_ERR_UNSUPPORTED_GATE, f"gate {i} ({g.get_name()}): matrix larger than 4x4")
+        ct.memmove(ct.addressof(rec) + qs_gate.matrix.offset, m.ctypes.data, m.nbytes)
     return arr
 
 

@@ -351,3 +351,46 @@ def test_compressed_adjoint_hea(qulacs_mod, dtype, ckpt):
         fd = _fd(circ, obs, "complex128")
         assert abs(e - e_ref) < 3e-3
         assert np.max(np.abs(g - fd)) < 3e-3
+
+
+@pytest.mark.parametrize("dtype", ["complex128", "complex64"])
+def test_compressed_adjoint_register_sweeps_match_op_path(qulacs_mod, dtype, monkeypatch):
+    """The backward passes as register sweeps over both stores (the default:
+    derivative sums inside the sweeps) against one shared-memory sweep per
+    gate and per sum (QOMPSIM_DUAL_SWEEPS=0), on a circuit whose generators
+    flip one or two qubits (RX, RY, XX, YZ rotations), are diagonal (RZ, ZZ)
+    or have Z factors on qubits outside the register bits, and an observable
+    with X, Y and Z strings; and both against the FP64 adjoint."""
+    from qulacs.torch import compressed_adjoint_gradient, energy_and_gradient
+    n, B = 11, 7
+    rng = np.random.default_rng(12)
+    c = qulacs_mod.ParametricQuantumCircuit(n)
+    for q in range(n):
+        c.add_H_gate(q)
+    for layer in range(2):
+        for q in range(n):
+            c.add_parametric_RY_gate(q, rng.uniform(0, 2 * np.pi))
+            c.add_parametric_RX_gate(q, rng.uniform(0, 2 * np.pi))
+        for q in range(0, n - 1, 2):
+            c.add_parametric_multi_Pauli_rotation_gate([q, q + 1], [3, 3], rng.uniform(0, 2 * np.pi))
+        for q in range(1, n - 1, 2):
+            c.add_parametric_multi_Pauli_rotation_gate([q, q + 1], [1, 1], rng.uniform(0, 2 * np.pi))
+        for q in range(0, n - 3, 3):
+            c.add_parametric_multi_Pauli_rotation_gate([q, q + 3], [2, 3], rng.uniform(0, 2 * np.pi))
+            c.add_CNOT_gate(q, q + 2)
+        for q in range(n):
+            c.add_parametric_RZ_gate(q, rng.uniform(0, 2 * np.pi))
+    obs = hea_observable(qulacs_mod, n)
+    obs.add_operator(0.3, "X 2 Z 9")
+    obs.add_operator(-0.2, "Y 8 Y 10")
+    e_ref, g_ref = energy_and_gradient(c, obs, "complex128")
+    tight = dtype == "complex128"
+    kw = dict(eps_rel=2.0 ** -22, eps_abs=1e-13) if tight else dict(eps_rel=2.0 ** -14, eps_abs=1e-9)
+    monkeypatch.setenv("QOMPSIM_DUAL_SWEEPS", "1")
+    e1, g1 = compressed_adjoint_gradient(c, obs, B, 3, dtype, checkpoint_every=8, **kw)
+    monkeypatch.setenv("QOMPSIM_DUAL_SWEEPS", "0")
+    e0, g0 = compressed_adjoint_gradient(c, obs, B, 3, dtype, checkpoint_every=8, **kw)
+    tol = 1e-6 if tight else 2e-3
+    assert abs(e1 - e0) < 1e-12   # the forward pass is the same; reductions may add in another order
+    assert np.max(np.abs(g1 - g0)) < tol
+    assert np.max(np.abs(g1 - g_ref)) < tol
