@@ -2127,6 +2127,11 @@ qs_status qs_get_total_times(qs_state *h, double out[10]) {
 qs_status qs_get_stats(qs_state *h, qs_stats *out) {
     if (!h || !out) return fail(h, QS_ERR_ARG, "NULL argument");
     *out = h->st;
+    // the state's geometry and codec hold before any apply
+    out->mantissa_bits = h->codec.m;
+    out->linear_exp = h->codec.L;
+    out->chunk_log2 = (int32_t)h->C;
+    out->tile_log2 = h->tile_log2;
     out->arena_capacity = h->capacity;
     out->host_store = h->host_store ? 1 : 0;
     return QS_OK;
@@ -3188,6 +3193,173 @@ qs_status qs_import_store(qs_state *h, const void *buf, uint64_t size) {
     uint64_t total = 0;
     for (uint64_t v : bb) total += v;
     h->history.assign(1, total);
+    return QS_OK;
+}
+
+qs_status qs_set_zero_vector(qs_state *h) {
+    if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
+    cudaStream_t s = h->stream;
+    CUDA_TRY(h, cudaMemsetAsync(h->mask, 0, h->nb, s));
+    CUDA_TRY(h, cudaMemsetAsync(h->block_bytes, 0, h->nb * sizeof(unsigned long long), s));
+    CUDA_TRY(h, cudaMemsetAsync(h->meta[h->mcur], 0, h->nchunks * sizeof(qs::ChunkMeta), s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
+    h->arena_used = 0;
+    h->history.assign(1, 0);
+    return QS_OK;
+}
+
+// ---- exchange of half a store across the rank boundary
+// Packed layout (device memory): this 128-byte header, the half's chunk
+// headers (16 bytes each), one stored flag per chunk (padded to 128 bytes),
+// then the payloads (128-byte aligned, offsets in the packed headers are
+// relative to the payload start).
+struct HalfHeader {
+    char magic[8];
+    uint32_t n, B, C, f64;
+    int32_t m, L;
+    uint32_t qubit, value;
+    uint64_t nhalf, payload_bytes;
+    uint8_t pad[72];
+};
+static_assert(sizeof(HalfHeader) == 128, "half header is 128 bytes");
+
+static uint64_t half_layout(uint64_t nhalf, uint64_t payload, uint64_t *meta_off, uint64_t *flags_off,
+                            uint64_t *payload_off) {
+    *meta_off = sizeof(HalfHeader);
+    *flags_off = *meta_off + nhalf * sizeof(qs::ChunkMeta);
+    *payload_off = *flags_off + (nhalf + 127) / 128 * 128;
+    return *payload_off + payload;
+}
+
+static qs_status half_args(qs_state *h, uint32_t qubit, uint32_t value, qs::HalfChunks *a) {
+    if (qubit < h->C || qubit >= h->n) return fail(h, QS_ERR_ARG, "exchanged qubit must lie in [chunk bits, n)");
+    if (value > 1) return fail(h, QS_ERR_ARG, "half value must be 0 or 1");
+    if (h->host_store) return fail(h, QS_ERR_ARG, "the exchange needs HBM arenas");
+    a->bit = (int32_t)(qubit - h->C);
+    a->value = value;
+    a->cshift = (int32_t)(h->B - h->C);
+    a->C = (int32_t)h->C;
+    a->nhalf = h->nchunks / 2;
+    return QS_OK;
+}
+
+}  // extern "C"
+
+// A device allocation freed when it goes out of scope.
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+};
+
+extern "C" {
+
+qs_status qs_export_half(qs_state *h, uint32_t qubit, uint32_t value, void *dev_buf, uint64_t cap, uint64_t *size) {
+    if (!h || !size) return fail(h, QS_ERR_ARG, "NULL argument");
+    qs::HalfChunks a{};
+    qs_status st = half_args(h, qubit, value, &a);
+    if (st != QS_OK) return st;
+    cudaStream_t s = h->stream;
+    DevBuf<uint64_t> sizes, scratch;
+    DevBuf<uint8_t> flags;
+    CUDA_TRY(h, cudaMalloc(&sizes.p, std::max<uint64_t>(1, a.nhalf) * 8));
+    CUDA_TRY(h, cudaMalloc(&flags.p, std::max<uint64_t>(1, a.nhalf)));
+    CUDA_TRY(h, cudaMalloc(&scratch.p, (qs::half_scan_scratch_words(a.nhalf) + 1) * 8));
+    uint64_t *total_dev = scratch.p + qs::half_scan_scratch_words(a.nhalf);
+    CUDA_TRY(h, qs::launch_half_sizes(a, h->meta[h->mcur], h->mask, sizes.p, flags.p, s));
+    CUDA_TRY(h, qs::launch_half_scan(sizes.p, a.nhalf, scratch.p, total_dev, s));
+    uint64_t payload = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&payload, total_dev, 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
+    uint64_t mo, fo, po;
+    *size = half_layout(a.nhalf, payload, &mo, &fo, &po);
+    if (!dev_buf) return QS_OK;
+    if (cap < *size) return fail(h, QS_ERR_ARG, "export buffer too small");
+    if ((reinterpret_cast<uintptr_t>(dev_buf) & 127) != 0) return fail(h, QS_ERR_ARG, "export buffer must be 128-byte aligned");
+    HalfHeader hd{};
+    std::memcpy(hd.magic, "QSHALF01", 8);
+    hd.n = h->n; hd.B = h->B; hd.C = h->C; hd.f64 = h->f64;
+    hd.m = h->codec.m; hd.L = h->codec.L;
+    hd.qubit = qubit; hd.value = value;
+    hd.nhalf = a.nhalf; hd.payload_bytes = payload;
+    char *b = (char *)dev_buf;
+    CUDA_TRY(h, cudaMemcpyAsync(b, &hd, sizeof(hd), cudaMemcpyHostToDevice, s));
+    if (a.nhalf) CUDA_TRY(h, cudaMemcpyAsync(b + fo, flags.p, a.nhalf, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(h, qs::launch_half_pack(a, h->meta[h->mcur], h->arena[h->cur], flags.p, sizes.p,
+                                     reinterpret_cast<qs::ChunkMeta *>(b + mo), reinterpret_cast<uint32_t *>(b + po),
+                                     false, s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
+    return QS_OK;
+}
+
+qs_status qs_import_half(qs_state *h, uint32_t qubit, uint32_t value, const void *dev_buf, uint64_t size) {
+    if (!h || !dev_buf) return fail(h, QS_ERR_ARG, "NULL argument");
+    qs::HalfChunks a{};
+    qs_status st = half_args(h, qubit, value, &a);
+    if (st != QS_OK) return st;
+    if (size < sizeof(HalfHeader)) return fail(h, QS_ERR_CORRUPT, "exchange buffer shorter than its header");
+    if ((reinterpret_cast<uintptr_t>(dev_buf) & 127) != 0) return fail(h, QS_ERR_ARG, "exchange buffer must be 128-byte aligned");
+    cudaStream_t s = h->stream;
+    HalfHeader hd{};
+    CUDA_TRY(h, cudaMemcpyAsync(&hd, dev_buf, sizeof(hd), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
+    if (std::memcmp(hd.magic, "QSHALF01", 8) != 0 || hd.n != h->n || hd.B != h->B || hd.C != h->C ||
+        hd.f64 != (uint32_t)h->f64 || hd.m != h->codec.m || hd.L != h->codec.L || hd.qubit != qubit ||
+        hd.nhalf != a.nhalf || (hd.payload_bytes & 127) != 0)
+        return fail(h, QS_ERR_CORRUPT, "exchange buffer does not match this state's geometry, codec or qubit");
+    uint64_t mo, fo, po;
+    if (half_layout(a.nhalf, hd.payload_bytes, &mo, &fo, &po) != size)
+        return fail(h, QS_ERR_CORRUPT, "exchange buffer length does not match its header");
+    const char *b = (const char *)dev_buf;
+    const auto *in_meta = reinterpret_cast<const qs::ChunkMeta *>(b + mo);
+    const auto *in_flags = reinterpret_cast<const uint8_t *>(b + fo);
+    // every received header of a stored chunk must point inside the received payload
+    CUDA_TRY(h, qs::launch_half_check(a, in_meta, in_flags, hd.payload_bytes, h->error_dev, s));
+    int32_t bad = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&bad, h->error_dev, sizeof(bad), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
+    CUDA_TRY(h, cudaMemsetAsync(h->error_dev, 0, sizeof(int32_t), s));
+    if (bad) return fail(h, QS_ERR_CORRUPT, "received chunk header outside the received payload");
+    // The new store goes to the other arena: first the kept half (bit !=
+    // value) compacted, then the received payloads; the replaced half's
+    // payloads are left behind with the old arena.
+    qs::HalfChunks kept = a;
+    kept.value = value ^ 1u;
+    DevBuf<uint64_t> sizes, scratch;
+    DevBuf<uint8_t> flags;
+    CUDA_TRY(h, cudaMalloc(&sizes.p, std::max<uint64_t>(1, a.nhalf) * 8));
+    CUDA_TRY(h, cudaMalloc(&flags.p, std::max<uint64_t>(1, a.nhalf)));
+    CUDA_TRY(h, cudaMalloc(&scratch.p, (qs::half_scan_scratch_words(a.nhalf) + 1) * 8));
+    uint64_t *total_dev = scratch.p + qs::half_scan_scratch_words(a.nhalf);
+    CUDA_TRY(h, qs::launch_half_sizes(kept, h->meta[h->mcur], h->mask, sizes.p, flags.p, s));
+    CUDA_TRY(h, qs::launch_half_scan(sizes.p, a.nhalf, scratch.p, total_dev, s));
+    uint64_t kept_bytes = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&kept_bytes, total_dev, 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
+    if (kept_bytes + hd.payload_bytes > h->capacity)
+        return fail(h, QS_ERR_CAPACITY, "the store after the exchange does not fit the arena; set QOMPSIM_ARENA_BYTES larger");
+    const int nc = h->cur ^ 1, nm = h->mcur ^ 1;
+    CUDA_TRY(h, qs::launch_half_pack(kept, h->meta[h->mcur], h->arena[h->cur], flags.p, sizes.p, h->meta[nm],
+                                     h->arena[nc], true, s));
+    if (hd.payload_bytes)
+        CUDA_TRY(h, cudaMemcpyAsync(reinterpret_cast<char *>(h->arena[nc]) + kept_bytes, b + po, hd.payload_bytes,
+                                    cudaMemcpyDeviceToDevice, s));
+    // received chunks: the kept half's blocks keep their stored flags (a
+    // chunk-level qubit) and gain the received ones
+    CUDA_TRY(h, qs::launch_half_unpack(a, in_meta, in_flags, kept_bytes, h->meta[nm], h->mask, s));
+    CUDA_TRY(h, qs::launch_block_bytes(h->meta[nm], h->mask, h->nb, (int)(h->B - h->C), (int)h->C,
+                                       h->block_bytes, s));
+    DevBuf<unsigned long long> tot;
+    CUDA_TRY(h, cudaMalloc(&tot.p, sizeof(unsigned long long)));
+    CUDA_TRY(h, cudaMemsetAsync(tot.p, 0, sizeof(unsigned long long), s));
+    CUDA_TRY(h, qs::launch_sum_mask_bytes(h->mask, h->block_bytes, h->nb, tot.p, s));
+    unsigned long long total = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&total, tot.p, sizeof(total), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
+    h->cur = nc;
+    h->mcur = nm;
+    h->arena_used = kept_bytes + hd.payload_bytes;
+    h->history.push_back(total);
     return QS_OK;
 }
 

@@ -417,6 +417,45 @@ uint64_t noalloc_scratch_words();
 cudaError_t launch_zero_unstored_headers(ChunkMeta *meta, const uint8_t *mask, uint64_t nchunks, int cshift,
                                          cudaStream_t stream);
 
+// ---- chunk exchange between ranks (qubit swap across the rank boundary)
+// The half of a store whose chunk-index bit `bit` (= qubit - C) equals v, in
+// the order of the other index bits ("half index" k).  Export packs its
+// headers (offsets relative to the packed payload, width 0 and base 0 for
+// chunks of unstored blocks, flag 1 for stored ones) and payloads; import
+// writes received chunks to the same positions of another store.
+struct HalfChunks {
+    int32_t bit;          // chunk-index bit of the exchanged qubit
+    uint32_t value;       // the half: chunks whose bit equals value
+    int32_t cshift;       // B - C: chunk index >> cshift = block
+    int32_t C;
+    uint64_t nhalf;       // chunks in the half
+};
+// sizes[k] = payload bytes of half chunk k (0 for unstored blocks), flags[k] = stored
+cudaError_t launch_half_sizes(const HalfChunks &h, const ChunkMeta *meta, const uint8_t *mask, uint64_t *sizes,
+                              uint8_t *flags, cudaStream_t stream);
+// In-place exclusive scan of n sizes; *total receives their sum.  scratch:
+// half_scan_scratch_words(n) 8-byte words.
+uint64_t half_scan_scratch_words(uint64_t n);
+cudaError_t launch_half_scan(uint64_t *sizes, uint64_t n, uint64_t *scratch, uint64_t *total, cudaStream_t stream);
+// Packed headers and payloads of the half (offsets[k]: exclusive scan of
+// sizes); headers go to out_meta[k], or with scatter to out_meta[chunk] (a
+// store's own header array: the compaction of the half a rank keeps).
+// Chunks of unstored blocks get zero headers.
+cudaError_t launch_half_pack(const HalfChunks &h, const ChunkMeta *meta, const uint32_t *arena, const uint8_t *flags,
+                             const uint64_t *offsets, ChunkMeta *out_meta, uint32_t *out_payload, bool scatter,
+                             cudaStream_t stream);
+// Import: received headers written to their chunks with offsets rebased by
+// base (bytes into the arena), their blocks marked stored (a block-level
+// qubit: the block's stored flag is the received one).
+cudaError_t launch_half_unpack(const HalfChunks &h, const ChunkMeta *in_meta, const uint8_t *in_flags, uint64_t base,
+                               ChunkMeta *meta, uint8_t *mask, cudaStream_t stream);
+// *bad = 1 when a received stored chunk's header is out of range.
+cudaError_t launch_half_check(const HalfChunks &h, const ChunkMeta *in_meta, const uint8_t *in_flags,
+                              uint64_t payload_bytes_total, int32_t *bad, cudaStream_t stream);
+// block_bytes[b] = stored ? sum over its chunks of payload + 16 : 0.
+cudaError_t launch_block_bytes(const ChunkMeta *meta, const uint8_t *mask, uint32_t nb, int cshift, int C,
+                               unsigned long long *block_bytes, cudaStream_t stream);
+
 int sm_count();
 
 }  // namespace qs

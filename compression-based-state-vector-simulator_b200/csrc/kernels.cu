@@ -2407,6 +2407,167 @@ __global__ void zero_unstored_headers_kernel(ChunkMeta *meta, const uint8_t *mas
         if (!mask[k >> cshift]) meta[k] = ChunkMeta{0, 0, 0};
 }
 
+// ------------------------------------------------------------ chunk exchange
+// Chunk index of half index k: bit `bit` of the chunk index set to v.
+__device__ __forceinline__ uint64_t half_chunk(uint64_t k, int bit, uint32_t v) {
+    const uint64_t lo = k & ((uint64_t(1) << bit) - 1);
+    return ((k >> bit) << (bit + 1)) | ((uint64_t)v << bit) | lo;
+}
+
+__global__ void half_sizes_kernel(const HalfChunks h, const ChunkMeta *meta, const uint8_t *mask, uint64_t *sizes,
+                                  uint8_t *flags) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < h.nhalf;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = half_chunk(k, h.bit, h.value);
+        const bool st = mask[c >> h.cshift] != 0;
+        const uint32_t w = st ? min(meta[c].width, 32u) : 0u;
+        sizes[k] = st ? payload_bytes(h.C, w) : 0;
+        flags[k] = st ? 1 : 0;
+    }
+}
+
+// Block-wide inclusive sum of one value per thread (blockDim.x = 1024).
+__device__ __forceinline__ uint64_t block_inclusive_scan(uint64_t x, uint64_t *s_warp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t t = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += t;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint64_t y = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t t = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += t;
+        }
+        s_warp[lane] = y;
+    }
+    __syncthreads();
+    const uint64_t r = x + (warp > 0 ? s_warp[warp - 1] : 0);
+    __syncthreads();
+    return r;
+}
+
+constexpr int kScanThreads = 1024, kScanPerThread = 4, kScanPerBlock = kScanThreads * kScanPerThread;
+
+// Per-CTA exclusive scan of kScanPerBlock values in place; the CTA's total to totals[cta].
+__global__ void __launch_bounds__(kScanThreads) half_scan_blocks_kernel(uint64_t *v, uint64_t n, uint64_t *totals) {
+    __shared__ uint64_t s_warp[32];
+    const uint64_t i0 = (uint64_t)blockIdx.x * kScanPerBlock + (uint64_t)threadIdx.x * kScanPerThread;
+    uint64_t a[kScanPerThread], sum = 0;
+#pragma unroll
+    for (int t = 0; t < kScanPerThread; ++t) {
+        a[t] = i0 + t < n ? v[i0 + t] : 0;
+        sum += a[t];
+    }
+    const uint64_t incl = block_inclusive_scan(sum, s_warp);
+    uint64_t run = incl - sum;
+#pragma unroll
+    for (int t = 0; t < kScanPerThread; ++t) {
+        if (i0 + t < n) v[i0 + t] = run;
+        run += a[t];
+    }
+    if (threadIdx.x == blockDim.x - 1) totals[blockIdx.x] = incl;
+}
+
+// One CTA: exclusive scan of the m CTA totals in place, grand total to *total.
+__global__ void __launch_bounds__(kScanThreads) half_scan_totals_kernel(uint64_t *totals, uint64_t m, uint64_t *total) {
+    __shared__ uint64_t s_warp[32];
+    const uint64_t per = (m + kScanThreads - 1) / kScanThreads;
+    const uint64_t i0 = (uint64_t)threadIdx.x * per;
+    uint64_t sum = 0;
+    for (uint64_t i = i0; i < i0 + per && i < m; ++i) sum += totals[i];
+    const uint64_t incl = block_inclusive_scan(sum, s_warp);
+    uint64_t run = incl - sum;
+    for (uint64_t i = i0; i < i0 + per && i < m; ++i) {
+        const uint64_t t = totals[i];
+        totals[i] = run;
+        run += t;
+    }
+    if (threadIdx.x == blockDim.x - 1) *total = incl;
+}
+
+__global__ void half_scan_add_kernel(uint64_t *v, uint64_t n, const uint64_t *totals) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        v[i] += totals[i / kScanPerBlock];
+}
+
+// One warp per half chunk: its packed header, then its payload copied in
+// 16-byte words (payloads are 128-byte aligned on both sides).
+__global__ void half_pack_kernel(const HalfChunks h, const ChunkMeta *meta, const uint32_t *arena,
+                                 const uint8_t *flags, const uint64_t *offsets, ChunkMeta *out_meta,
+                                 uint32_t *out_payload, bool scatter) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t k = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; k < h.nhalf; k += warps) {
+        const uint64_t c = half_chunk(k, h.bit, h.value);
+        ChunkMeta md{0, 0, 0};
+        if (flags[k]) {
+            md = meta[c];
+            md.width = min(md.width, 32u);
+        }
+        const uint64_t bytes = flags[k] ? payload_bytes(h.C, md.width) : 0;
+        const uint4 *src = reinterpret_cast<const uint4 *>(arena + (md.offset >> 2));
+        uint4 *dst = reinterpret_cast<uint4 *>(out_payload + (offsets[k] >> 2));
+        for (uint64_t w = lane; w < bytes / 16; w += 32) dst[w] = src[w];
+        if (lane == 0)
+            out_meta[scatter ? c : k] = flags[k] ? ChunkMeta{offsets[k], md.base, md.width} : ChunkMeta{0, 0, 0};
+    }
+}
+
+__global__ void half_unpack_kernel(const HalfChunks h, const ChunkMeta *in_meta, const uint8_t *in_flags,
+                                   uint64_t base, ChunkMeta *meta, uint8_t *mask) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < h.nhalf;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = half_chunk(k, h.bit, h.value);
+        ChunkMeta md = in_meta[k];
+        if (in_flags[k]) {
+            md.offset += base;
+            md.width = min(md.width, 32u);
+            mask[c >> h.cshift] = 1;
+        } else {
+            md = ChunkMeta{0, 0, 0};
+            // a block-level qubit moves whole blocks: an unstored one stays unstored
+            if (h.bit >= h.cshift) mask[c >> h.cshift] = 0;
+        }
+        meta[c] = md;
+    }
+}
+
+// Received headers: stored chunks must have a 128-byte aligned offset, a
+// width of at most 32 and a payload inside the received payload bytes.
+__global__ void half_check_kernel(const HalfChunks h, const ChunkMeta *in_meta, const uint8_t *in_flags,
+                                  uint64_t payload_bytes_total, int32_t *bad) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < h.nhalf;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        if (!in_flags[k]) continue;
+        const ChunkMeta md = in_meta[k];
+        const uint64_t pb = payload_bytes(h.C, md.width & 63u);
+        if (md.width > 32 || (md.offset & 127) || md.offset > payload_bytes_total || pb > payload_bytes_total - md.offset)
+            atomicOr(bad, 1);
+    }
+}
+
+// One warp per block.
+__global__ void block_bytes_kernel(const ChunkMeta *meta, const uint8_t *mask, uint32_t nb, int cshift, int C,
+                                   unsigned long long *block_bytes) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint64_t cpb = uint64_t(1) << cshift;
+    for (uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; b < nb; b += warps) {
+        unsigned long long s = 0;
+        if (mask[b])
+            for (uint64_t k = lane; k < cpb; k += 32)
+                s += payload_bytes(C, min(meta[(b << cshift) + k].width, 32u)) + sizeof(ChunkMeta);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) block_bytes[b] = mask[b] ? s : 0;
+    }
+}
+
 int g_sm_count = 0;
 
 // Scratch of the allocation-free codec round trip (qs_codec_roundtrip_noalloc):
@@ -2680,6 +2841,55 @@ cudaError_t launch_zero_unstored_headers(ChunkMeta *meta, const uint8_t *mask, u
                                          cudaStream_t s) {
     const unsigned grid = grid_for(nchunks, 256, 8);
     zero_unstored_headers_kernel<<<grid, 256, 0, s>>>(meta, mask, nchunks, cshift);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_half_sizes(const HalfChunks &h, const ChunkMeta *meta, const uint8_t *mask, uint64_t *sizes,
+                              uint8_t *flags, cudaStream_t s) {
+    if (h.nhalf == 0) return cudaSuccess;
+    half_sizes_kernel<<<grid_for(h.nhalf, 256, 8), 256, 0, s>>>(h, meta, mask, sizes, flags);
+    return cudaGetLastError();
+}
+
+uint64_t half_scan_scratch_words(uint64_t n) { return (n + kScanPerBlock - 1) / kScanPerBlock + 1; }
+
+cudaError_t launch_half_scan(uint64_t *sizes, uint64_t n, uint64_t *scratch, uint64_t *total, cudaStream_t s) {
+    const uint64_t m = (n + kScanPerBlock - 1) / kScanPerBlock;
+    if (m == 0) return cudaMemsetAsync(total, 0, sizeof(uint64_t), s);
+    half_scan_blocks_kernel<<<(unsigned)m, kScanThreads, 0, s>>>(sizes, n, scratch);
+    half_scan_totals_kernel<<<1, kScanThreads, 0, s>>>(scratch, m, total);
+    half_scan_add_kernel<<<grid_for(n, 256, 8), 256, 0, s>>>(sizes, n, scratch);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_half_pack(const HalfChunks &h, const ChunkMeta *meta, const uint32_t *arena, const uint8_t *flags,
+                             const uint64_t *offsets, ChunkMeta *out_meta, uint32_t *out_payload, bool scatter,
+                             cudaStream_t s) {
+    if (h.nhalf == 0) return cudaSuccess;
+    half_pack_kernel<<<grid_for(h.nhalf * 32, 256, 8), 256, 0, s>>>(h, meta, arena, flags, offsets, out_meta,
+                                                                    out_payload, scatter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_half_unpack(const HalfChunks &h, const ChunkMeta *in_meta, const uint8_t *in_flags, uint64_t base,
+                               ChunkMeta *meta, uint8_t *mask, cudaStream_t s) {
+    if (h.nhalf == 0) return cudaSuccess;
+    half_unpack_kernel<<<grid_for(h.nhalf, 256, 8), 256, 0, s>>>(h, in_meta, in_flags, base, meta, mask);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_half_check(const HalfChunks &h, const ChunkMeta *in_meta, const uint8_t *in_flags,
+                              uint64_t payload_bytes_total, int32_t *bad, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(bad, 0, sizeof(int32_t), s);
+    if (e != cudaSuccess || h.nhalf == 0) return e;
+    half_check_kernel<<<grid_for(h.nhalf, 256, 8), 256, 0, s>>>(h, in_meta, in_flags, payload_bytes_total, bad);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_block_bytes(const ChunkMeta *meta, const uint8_t *mask, uint32_t nb, int cshift, int C,
+                               unsigned long long *block_bytes, cudaStream_t s) {
+    if (nb == 0) return cudaSuccess;
+    block_bytes_kernel<<<grid_for((uint64_t)nb * 32, 256, 8), 256, 0, s>>>(meta, mask, nb, cshift, C, block_bytes);
     return cudaGetLastError();
 }
 

@@ -134,6 +134,9 @@ SIGNATURES = [
     ("qs_get_stats", ct.c_int, [_P, ct.POINTER(qs_stats)]),
     ("qs_export_store", ct.c_int, [_P, _P, _U64, ct.POINTER(_U64)]),
     ("qs_import_store", ct.c_int, [_P, _P, _U64]),
+    ("qs_export_half", ct.c_int, [_P, _U32, _U32, _P, _U64, ct.POINTER(_U64)]),
+    ("qs_import_half", ct.c_int, [_P, _U32, _U32, _P, _U64]),
+    ("qs_set_zero_vector", ct.c_int, [_P]),
     ("qs_checkpoint", ct.c_int, [_P, _U32]),
     ("qs_restore", ct.c_int, [_P, _U32]),
     ("qs_free_checkpoint", ct.c_int, [_P, _U32]),

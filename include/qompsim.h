@@ -329,6 +329,25 @@ qs_status qs_get_stats(qs_state *h, qs_stats *out);
 qs_status qs_export_store(qs_state *h, void *buf, uint64_t cap, uint64_t *size);
 qs_status qs_import_store(qs_state *h, const void *buf, uint64_t size);
 
+/* Multi-rank exchange (replaces apply_fused_swap's compressed block
+ * send/recv, compressed_state.hpp:1396-1546, for one swapped qubit pair):
+ * a rank holding global qubit bit b swaps it with its local qubit `qubit`
+ * (chunk bits <= qubit < n) by sending the half of its store whose
+ * amplitude-index bit `qubit` equals 1-b and receiving the partner's half
+ * into the same positions.  qs_export_half packs the half whose bit equals
+ * `value` (chunk headers and compressed payloads, no decoding) into a
+ * 128-byte aligned DEVICE buffer; with dev_buf == NULL it only reports the
+ * size.  qs_import_half writes a packed half received from a partner of the
+ * same geometry and codec into the positions whose bit equals `value`
+ * (payloads appended to the current arena, headers rewritten, blocks marked
+ * stored, per-block bytes recomputed); QS_ERR_CORRUPT when the buffer does
+ * not match or a header points outside it.  Both synchronise the stream.
+ * qs_set_zero_vector makes the state the zero vector (every block unstored):
+ * the initial store of ranks that do not hold |0...0>. */
+qs_status qs_export_half(qs_state *h, uint32_t qubit, uint32_t value, void *dev_buf, uint64_t cap, uint64_t *size);
+qs_status qs_import_half(qs_state *h, uint32_t qubit, uint32_t value, const void *dev_buf, uint64_t size);
+qs_status qs_set_zero_vector(qs_state *h);
+
 /* Device-side checkpoints of the compressed store (zero mask, per-block
  * bytes, chunk headers and the payload in use): qs_checkpoint copies the
  * current store into slot (0..63, allocated on first use, regrown when the
