@@ -479,6 +479,95 @@ def brickwork_leg(torch, n: int = 32, layers: int = 20, B: int = 22, I: int = 4)
     return res
 
 
+def qaoa_leg(torch, n: int = 34, p: int = 4, B: int = 24, I: int = 4):
+    """QAOA MaxCut (seeded 3-regular graph, p layers of RZZ(gamma) per edge
+    and RX(beta) per qubit from |+>^n), complex64 at the default bounds: the
+    compressed forward pass (CUDA events) and its cut energy sum_edges
+    <Z_a Z_b> (FP64 reductions on the compressed store), against this
+    package's fused uncompressed complex64 state of the same gates (energy,
+    and the fidelity and largest amplitude error in 2^24-amplitude slices
+    when both states fit the GPU together; at n=34 the 137 GB uncompressed
+    state runs first and is freed before the compressed one)."""
+    import numpy as np
+    import qulacs
+    from qulacs import _native
+    from qompsim import circuits as C
+    from qulacs.circuit import QuantumCircuitOptimizer
+    c = C.qaoa_maxcut(n, p, seed=0)
+    QuantumCircuitOptimizer(sv_block_size=B).optimize(c, block_size=2)
+    obs = qulacs.Observable(n)
+    for a, b in C.regular_graph_edges(n, 3, 0):
+        obs.add_operator(1.0, f"Z {a} Z {b}")
+    res = {"workload": f"qaoa maxcut: n={n} p={p} 3-regular, block_size={B}, inner_size={I}, complex64, "
+                       f"eps_rel=1e-3, eps_abs=1e-7", "gates": len(c._gates)}
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    ds = qulacs.QuantumState(n, dtype="complex64")
+    ds.set_computational_basis(0)
+    res["fused_dense_c64_ms"] = timed(lambda: ds._apply_gates(list(c._gates), pergate=False))
+    e_dense = obs.get_expectation_value(ds)
+    res["energy_dense_c64"] = e_dense
+    cq = None
+    try:
+        cq = qulacs.CompressedQuantumState(n, B, dtype="complex64", eps_rel=1e-3, eps_abs=1e-7,
+                                           flags=_native.QS_FLAG_QUIET)
+        cq.partition_and_register_circuit(c, I, 0)
+        ms = timed(cq.apply_circuit)
+        both = True
+    except _native.QompsimError:
+        # the two compressed arenas did not fit beside the dense state
+        both = False
+        cq = None
+        torch.cuda.empty_cache()
+    if not both:
+        e_keep = e_dense
+        del ds
+        ds = None
+        cq = qulacs.CompressedQuantumState(n, B, dtype="complex64", eps_rel=1e-3, eps_abs=1e-7,
+                                           flags=_native.QS_FLAG_QUIET)
+        cq.partition_and_register_circuit(c, I, 0)
+        ms = timed(cq.apply_circuit)
+        e_dense = e_keep
+    st = cq.get_stats()
+    e = obs.get_expectation_value(cq)
+    res["compressed_c64"] = {"ms": ms, "passes": int(st["passes"]), "stages": int(st["stages"]),
+                             "amp_gate_updates": int(st["amp_gate_updates"]),
+                             "updates_per_s": st["amp_gate_updates"] / (ms * 1e-3),
+                             "max_sv_bytes": cq.get_max_SV_bytes(), "arena_capacity": int(st["arena_capacity"]),
+                             "energy": e, "energy_err_vs_dense_c64": abs(e - e_dense),
+                             "speedup_vs_fused_dense_c64": res["fused_dense_c64_ms"] / ms}
+    if ds is not None:
+        scale = 1.0 / math.sqrt(cq.get_squared_norm())
+        cnt = 1 << SLICE_LOG2
+        rbuf = torch.empty(2 * cnt, dtype=torch.float64, device="cuda")
+        pbuf = torch.empty(2 * cnt, dtype=torch.float64, device="cuda")
+        acc = torch.zeros((), dtype=torch.complex128, device="cuda")
+        err = torch.zeros((), dtype=torch.float64, device="cuda")
+        nref = torch.zeros((), dtype=torch.float64, device="cuda")
+        for first in range(0, 1 << n, cnt):
+            cq.get_amplitudes_to(pbuf.data_ptr(), first, cnt, renormalize=False)
+            psi = torch.view_as_complex(pbuf.view(-1, 2)) * scale
+            ds.get_amplitudes_to(rbuf.data_ptr(), first, cnt)
+            ref = torch.view_as_complex(rbuf.view(-1, 2))
+            acc += torch.vdot(ref, psi)
+            nref += (ref.abs() ** 2).sum()
+            err = torch.maximum(err, (ref - psi).abs().max())
+        res["compressed_c64"]["fidelity_vs_dense_c64"] = float(acc.abs().item() / math.sqrt(nref.item()))
+        res["compressed_c64"]["max_abs_err_vs_dense_c64"] = float(err.item())
+    del cq, ds
+    torch.cuda.empty_cache()
+    del np
+    return res
+
+
 def dense_gate_leg(torch, n: int = 30, B: int = 20, reps: int = 5):
     """One dense 5-qubit gate (Haar random, targets 0, 1, 2, 3 and 8) over a
     dense compressed state of n qubits (the QFT of a basis state, default
@@ -785,7 +874,7 @@ def main():
     ap.add_argument("--no-dense", action="store_true", help="skip the uncompressed per-gate comparison leg")
     ap.add_argument("--no-legs", action="store_true", help="skip the complex64, adjoint-gradient and brickwork legs")
     ap.add_argument("--no-brickwork", action="store_true", help="skip the brickwork n=32 leg")
-    ap.add_argument("--leg", choices=["dense_gate", "adjoint"], default=None,
+    ap.add_argument("--leg", choices=["dense_gate", "adjoint", "qaoa"], default=None,
                     help="run only this leg and print its JSON (for profiling)")
     ap.add_argument("--leg-n", type=int, default=None, help="qubits of the --leg workload")
     args = ap.parse_args()
@@ -793,6 +882,10 @@ def main():
         import torch
         n = args.leg_n or 30
         print(json.dumps(dense_gate_leg(torch, n=n, B=min(20, n - 4), reps=2)))
+        return
+    if args.leg == "qaoa":
+        import torch
+        print(json.dumps(qaoa_leg(torch, n=args.leg_n or 34)))
         return
     if args.leg == "adjoint":
         import torch
