@@ -479,6 +479,68 @@ def brickwork_leg(torch, n: int = 32, layers: int = 20, B: int = 22, I: int = 4)
     return res
 
 
+def sharded_leg(torch, n: int = 28, P: int = 2, B: int = 20, I: int = 4):
+    """QFT n=28 (complex128, default bounds) on P ranks of the sharded
+    compressed state (qulacs.distributed), the ranks run as threads of this
+    process on one GPU: each rank's store holds n - log2(P) qubits and every
+    exchange is a packed half-store (compressed chunks) handed over on the
+    device (across GPUs it is an NCCL send).  Reported: the slowest rank's
+    apply time (wall clock, synchronised), the exchanges and their
+    compressed bytes per rank, and the fidelity of the gathered state against
+    the analytic QFT state."""
+    import threading
+    from qompsim import circuits as C
+    from qulacs import distributed as D
+    from qulacs.circuit import QuantumCircuitOptimizer
+    c = C.qft_basis(n, seed=0)
+    x = C.qft_input(n, 0)
+    QuantumCircuitOptimizer(sv_block_size=B).optimize(c, block_size=2)
+    hub = D.ThreadExchange(P, timeout=600)
+    start = threading.Barrier(P)
+    out, errs = {}, []
+
+    def rank(r):
+        try:
+            torch.cuda.set_device(0)
+            st = D.ShardedCompressedQuantumState(n, B, dtype="complex128", exchange=hub.endpoint(r))
+            st.partition_and_register_circuit(c, I)
+            start.wait()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st.apply_circuit()
+            torch.cuda.synchronize()
+            out[r] = (time.perf_counter() - t0, st.exchanges, st.exchanged_bytes, st.get_local_vector())
+        except Exception as e:  # noqa: BLE001
+            errs.append(repr(e))
+            start.abort()
+
+    th = [threading.Thread(target=rank, args=(r,)) for r in range(P)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=900)
+    if errs or len(out) != P:
+        return {"error": errs[:2] or ["a rank did not finish"]}
+    nl = n - (P.bit_length() - 1)
+    amp = 1.0 / math.sqrt(float(1 << n))
+    acc = 0j
+    nrm = 0.0
+    err = 0.0
+    for r in range(P):
+        v = torch.from_numpy(out[r][3]).cuda()
+        k = torch.arange(r << nl, (r + 1) << nl, dtype=torch.int64, device="cuda")
+        ph = ((k * x) & ((1 << n) - 1)).to(torch.float64) * (2.0 * math.pi / float(1 << n))
+        ref = torch.polar(torch.full_like(ph, amp), ph)
+        acc += complex(torch.vdot(ref, v).item())
+        nrm += float((v.abs() ** 2).sum().item())
+        err = max(err, float((ref - v).abs().max().item()))
+        del v, k, ph, ref
+    return {"workload": f"qft: n={n} complex128 on {P} ranks (threads on one GPU), block_size={B}, inner_size={I}",
+            "apply_ms_slowest_rank": 1e3 * max(o[0] for o in out.values()),
+            "exchanges_per_rank": out[0][1], "exchanged_bytes_per_rank": out[0][2],
+            "fidelity": abs(acc) / math.sqrt(nrm), "max_abs_err_unnormalised": err}
+
+
 def qaoa_leg(torch, n: int = 34, p: int = 4, B: int = 24, I: int = 4):
     """QAOA MaxCut (seeded 3-regular graph, p layers of RZZ(gamma) per edge
     and RX(beta) per qubit from |+>^n), complex64 at the default bounds: the
@@ -807,6 +869,7 @@ def run_ours(args, spec):
                                                              / extra["complex64"]["ms_per_step"])
         extra["adjoint"] = adjoint_leg(torch)
         extra["dense_gate"] = dense_gate_leg(torch)
+        extra["sharded"] = sharded_leg(torch)
         if not args.no_brickwork:
             extra["brickwork32"] = brickwork_leg(torch)
 
@@ -874,7 +937,7 @@ def main():
     ap.add_argument("--no-dense", action="store_true", help="skip the uncompressed per-gate comparison leg")
     ap.add_argument("--no-legs", action="store_true", help="skip the complex64, adjoint-gradient and brickwork legs")
     ap.add_argument("--no-brickwork", action="store_true", help="skip the brickwork n=32 leg")
-    ap.add_argument("--leg", choices=["dense_gate", "adjoint", "qaoa"], default=None,
+    ap.add_argument("--leg", choices=["dense_gate", "adjoint", "qaoa", "sharded"], default=None,
                     help="run only this leg and print its JSON (for profiling)")
     ap.add_argument("--leg-n", type=int, default=None, help="qubits of the --leg workload")
     args = ap.parse_args()
@@ -882,6 +945,10 @@ def main():
         import torch
         n = args.leg_n or 30
         print(json.dumps(dense_gate_leg(torch, n=n, B=min(20, n - 4), reps=2)))
+        return
+    if args.leg == "sharded":
+        import torch
+        print(json.dumps(sharded_leg(torch, n=args.leg_n or 28)))
         return
     if args.leg == "qaoa":
         import torch
