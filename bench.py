@@ -676,12 +676,12 @@ def dense_gate_leg(torch, n: int = 30, B: int = 20, reps: int = 5):
 
 
 def adjoint_leg(torch, n: int = 24, depth: int = 8, reps: int = 5):
-    import numpy as np
     """Hardware-efficient ansatz n=24, depth 8 (RY RZ per qubit + CNOT ladder,
     384 parameters), H = sum Z_i Z_i+1 + 0.5 sum X_i: wall time of the energy
     alone and of energy + adjoint gradient through the public API, each call
     synchronised; the best of `reps` calls of each (the calls include host
     planning, whose time varies with the host's load)."""
+    import numpy as np
     import qulacs
     from qompsim import circuits as C
     from qulacs.torch import energy, energy_and_gradient
@@ -711,12 +711,14 @@ def adjoint_leg(torch, n: int = 24, depth: int = 8, reps: int = 5):
 
 
 def compressed_adjoint_leg(torch, circ, obs, n: int, B: int = 18, I: int = 4, reps: int = 3):
-    import numpy as np
     """The same ansatz with both states compressed (complex64, FP64
     reductions, eps_rel 1e-3 / eps_abs 1e-7), device checkpoints after every
     layer's 48 parameters: device times (CUDA events) of the forward pass with
     its energy, of lambda = H psi and of the backward sweep, the best of
-    `reps` calls; gradient error against the uncompressed FP64 adjoint."""
+    `reps` calls -- as stream windows (host planning between launches
+    included) and as the engine's launch spans alone (`*_launches_ms`,
+    `ratio_launches`); gradient error against the uncompressed FP64 adjoint."""
+    import numpy as np
     from qulacs.torch import compressed_adjoint_gradient, energy_and_gradient
     e_ref, g_ref = energy_and_gradient(circ, obs, "complex128")
     best = None
@@ -727,9 +729,13 @@ def compressed_adjoint_leg(torch, circ, obs, n: int, B: int = 18, I: int = 4, re
             best = (tm, e, g)
     tm, e, g = best
     fwd = tm["forward_ms"]
+    fk = tm["forward_launches_ms"]
     return {"block_size": B, "inner_size": I, "dtype": "complex64", "checkpoint_every": 2 * n,
             "forward_ms": fwd, "lambda_ms": tm["lambda_ms"], "backward_ms": tm["backward_ms"],
             "ratio": (fwd + tm["lambda_ms"] + tm["backward_ms"]) / fwd,
+            "forward_launches_ms": fk, "lambda_launches_ms": tm["lambda_launches_ms"],
+            "backward_launches_ms": tm["backward_launches_ms"],
+            "ratio_launches": (fk + tm["lambda_launches_ms"] + tm["backward_launches_ms"]) / fk,
             "energy_err": abs(e - e_ref), "grad_max_abs_err_vs_fp64": float(np.max(np.abs(g - g_ref))),
             "grad_max_abs": float(np.max(np.abs(g_ref)))}
 

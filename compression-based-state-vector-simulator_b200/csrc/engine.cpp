@@ -682,6 +682,23 @@ std::vector<Real> pool_as(const std::vector<cplx> &pool) {
     return out;
 }
 
+// Register sweeps over two stores for one launch of a backward pass: the
+// gates `gl` (indices into cg) in order, the derivative sum of each
+// parametric one (slots[gi] >= 0; local slots numbered in order) placed just
+// before it as a pseudo-gate with the gate's qubits and mixing bits, so that
+// the two share a sweep and the generator's flip qubits are register bits.
+// Appends sweeps (op ranges relative to *rop_off), ops and variants; false
+// (nothing appended) when a flip qubit is not a register bit or the pass
+// needs too many outer selector qubits.
+struct DualSweepPlan {
+    size_t sw_off = 0, nsw = 0, rop_off = 0;
+    std::vector<int> outer;
+};
+bool plan_dual_sweeps(const std::vector<CGate> &cg, const std::vector<uint32_t> &gl, const int32_t *slots,
+                      const uint64_t *gen_x, const uint64_t *gen_z, const std::vector<int> &tile, int C, int RB,
+                      std::vector<qs::Sweep> *all_sw, std::vector<qs::ROp> *all_rops, std::vector<cplx> *all_pool,
+                      DualSweepPlan *out);
+
 struct PassPlan {
     std::vector<int> tile;        // tile qubits >= C, ascending
     std::vector<uint32_t> gates;  // indices into the gate list
@@ -842,6 +859,57 @@ std::vector<PassPlan> plan_passes_dag(const std::vector<uint32_t> &gate_ids, con
         pp.tile.assign(s2.begin(), s2.end());
     }
     return out;
+}
+
+bool plan_dual_sweeps(const std::vector<CGate> &cg, const std::vector<uint32_t> &gl, const int32_t *slots,
+                      const uint64_t *gen_x, const uint64_t *gen_z, const std::vector<int> &tile, int C, int RB,
+                      std::vector<qs::Sweep> *all_sw, std::vector<qs::ROp> *all_rops, std::vector<cplx> *all_pool,
+                      DualSweepPlan *out) {
+    const int nb = C + (int)tile.size();
+    if (nb < RB) return false;
+    std::vector<qs::KGate> kg;
+    std::vector<int32_t> sum_slot;
+    std::vector<uint32_t> gid;
+    int32_t ls = 0;
+    for (uint32_t gi : gl) {
+        const qs::KGate g = to_kgate(cg[gi], tile, C);
+        if (slots[gi] >= 0) {
+            kg.push_back(g);
+            sum_slot.push_back(ls++);
+            gid.push_back(gi);
+        }
+        kg.push_back(g);
+        sum_slot.push_back(-1);
+        gid.push_back(gi);
+    }
+    const auto sweeps = plan_sweeps(kg, 0, kg.size(), nb, RB);
+    std::vector<RawOp> raw;
+    std::vector<cplx> rpool;
+    for (const auto &sw : sweeps)
+        for (int i = sw.g0; i < sw.g1; ++i) {
+            if (sum_slot[i] >= 0) {
+                if (!build_sum_op(gen_x[gid[i]], gen_z[gid[i]], sum_slot[i], sw, RB, tile, C, &raw, &rpool))
+                    return false;
+            } else {
+                build_gate_op(kg[i], sw, RB, &raw, &rpool);
+            }
+        }
+    std::vector<qs::Sweep> msw;
+    merge_diagonal_ops(sweeps, 0, &raw, &rpool, &msw);
+    std::vector<qs::ROp> rops;
+    std::vector<int> outer;
+    const size_t pool0 = all_pool->size();
+    if (!finalize_ops(raw, rpool, nb, &outer, &rops, all_pool)) {
+        all_pool->resize(pool0);
+        return false;
+    }
+    out->sw_off = all_sw->size();
+    out->nsw = msw.size();
+    out->rop_off = all_rops->size();
+    out->outer = outer;
+    all_sw->insert(all_sw->end(), msw.begin(), msw.end());
+    all_rops->insert(all_rops->end(), rops.begin(), rops.end());
+    return true;
 }
 
 std::string format_size(unsigned long long size) {
@@ -2817,13 +2885,23 @@ qs_status qs_apply_pauli_sum(qs_state *out, qs_state *in, const uint64_t *x_mask
         CUDA_TRY(out, cudaMemcpyAsync(dops, ops.data(), ops.size() * sizeof(qs::DualOp), cudaMemcpyHostToDevice,
                                       out->stream));
     CUDA_TRY(out, cudaMemsetAsync(in->error_dev, 0, sizeof(int32_t), out->stream));
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    CUDA_TRY(out, cudaEventCreate(&ev0));
+    struct EvFree { cudaEvent_t &a, &b; ~EvFree() { if (a) cudaEventDestroy(a); if (b) cudaEventDestroy(b); } } evf{ev0, ev1};
+    CUDA_TRY(out, cudaEventCreate(&ev1));
+    CUDA_TRY(out, cudaEventRecord(ev0, out->stream));
     for (size_t g = 0; g < tiles.size(); ++g) {
         st = dual_launch(in, out, tiles[g], dops + op_off[g], (int)(op_off[g + 1] - op_off[g]), false, g == 0,
                          nullptr, 0);
         if (st != QS_OK) return fail(out, st, in->err);
     }
+    CUDA_TRY(out, cudaEventRecord(ev1, out->stream));
     st = dual_finish(in, out, false);
     if (st != QS_OK) return fail(out, st, in->err);
+    {
+        float pm = 0.f;
+        if (cudaEventElapsedTime(&pm, ev0, ev1) == cudaSuccess) out->st.pair_ms = pm;
+    }
     return QS_OK;
 }
 
@@ -2919,51 +2997,14 @@ qs_status qs_adjoint(qs_state *psi, qs_state *lam, const qs_gate *gates, const i
     std::vector<cplx> all_pool;
     if (env_int("QOMPSIM_DUAL_SWEEPS", 1)) {
         for (Launch &L : launches) {
-            const int nb = C + (int)L.tile.size();
-            if (nb < RB) continue;
-            std::vector<qs::KGate> kg;
-            std::vector<int32_t> sum_slot;
-            std::vector<uint32_t> gid;
-            int32_t ls = 0;
-            for (uint32_t gi : L.gates) {
-                const qs::KGate g = to_kgate(cg[gi], L.tile, C);
-                if (slots[gi] >= 0) {
-                    kg.push_back(g);
-                    sum_slot.push_back(ls++);
-                    gid.push_back(gi);
-                }
-                kg.push_back(g);
-                sum_slot.push_back(-1);
-                gid.push_back(gi);
-            }
-            const auto sweeps = plan_sweeps(kg, 0, kg.size(), nb, RB);
-            std::vector<RawOp> raw;
-            std::vector<cplx> rpool;
-            bool ok = true;
-            for (const auto &sw : sweeps)
-                for (int i = sw.g0; i < sw.g1 && ok; ++i) {
-                    if (sum_slot[i] >= 0)
-                        ok = build_sum_op(gen_x[gid[i]], gen_z[gid[i]], sum_slot[i], sw, RB, L.tile, C, &raw, &rpool);
-                    else
-                        build_gate_op(kg[i], sw, RB, &raw, &rpool);
-                }
-            if (!ok) continue;
-            std::vector<qs::Sweep> msw;
-            merge_diagonal_ops(sweeps, 0, &raw, &rpool, &msw);
-            std::vector<qs::ROp> rops;
-            std::vector<int> outer;
-            const size_t pool0 = all_pool.size();
-            if (!finalize_ops(raw, rpool, nb, &outer, &rops, &all_pool)) {
-                all_pool.resize(pool0);
+            DualSweepPlan dp;
+            if (!plan_dual_sweeps(cg, L.gates, slots, gen_x, gen_z, L.tile, C, RB, &all_sw, &all_rops, &all_pool, &dp))
                 continue;
-            }
             L.fused = true;
-            L.sw_off = all_sw.size();
-            L.nsw = msw.size();
-            L.rop_off = all_rops.size();
-            L.outer = outer;
-            all_sw.insert(all_sw.end(), msw.begin(), msw.end());
-            all_rops.insert(all_rops.end(), rops.begin(), rops.end());
+            L.sw_off = dp.sw_off;
+            L.nsw = dp.nsw;
+            L.rop_off = dp.rop_off;
+            L.outer = dp.outer;
         }
     }
     qs::DualOp *dops = nullptr;
@@ -2999,6 +3040,11 @@ qs_status qs_adjoint(qs_state *psi, qs_state *lam, const qs_gate *gates, const i
         CUDA_TRY(psi, cudaMemcpyAsync(dops, ops.data(), ops.size() * sizeof(qs::DualOp), cudaMemcpyHostToDevice, s));
     CUDA_TRY(psi, cudaMemsetAsync(dsum, 0, std::max<size_t>(1, 2 * nout) * sizeof(double), s));
     CUDA_TRY(psi, cudaMemsetAsync(psi->error_dev, 0, sizeof(int32_t), s));
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    CUDA_TRY(psi, cudaEventCreate(&ev0));
+    struct EvFree { cudaEvent_t &a, &b; ~EvFree() { if (a) cudaEventDestroy(a); if (b) cudaEventDestroy(b); } } evf{ev0, ev1};
+    CUDA_TRY(psi, cudaEventCreate(&ev1));
+    CUDA_TRY(psi, cudaEventRecord(ev0, s));
     for (const Launch &L : launches) {
         DualSweepRef ref{};
         if (L.fused) {
@@ -3013,9 +3059,14 @@ qs_status qs_adjoint(qs_state *psi, qs_state *lam, const qs_gate *gates, const i
                          (int)L.local_to_global.size(), L.fused ? &ref : nullptr);
         if (st != QS_OK) return st;
     }
+    CUDA_TRY(psi, cudaEventRecord(ev1, s));
     std::vector<double> h(2 * nout);
     if (nout) CUDA_TRY(psi, cudaMemcpyAsync(h.data(), dsum, 2 * nout * sizeof(double), cudaMemcpyDeviceToHost, s));
     st = dual_finish(psi, lam, true);
+    {
+        float pm = 0.f;
+        if (cudaEventElapsedTime(&pm, ev0, ev1) == cudaSuccess) psi->st.pair_ms = pm;
+    }
     if (st != QS_OK) return st;
     std::vector<double> acc(2 * (size_t)nslots, 0.0);
     for (const Launch &L : launches)
@@ -3822,6 +3873,10 @@ qs_status qs_dense_adjoint(qs_dense *psi, qs_dense *lam, const qs_gate *gates, c
         int32_t tq[qs::kMaxTileQubits];
         size_t gate_off, ngates, out_off;
         std::vector<int32_t> local_to_global;
+        std::vector<int> tile;
+        std::vector<uint32_t> gates;
+        bool fused = false;
+        DualSweepPlan sweeps;
     };
     std::vector<qs::AdjGate> ag;
     std::vector<Launch> launches;
@@ -3831,6 +3886,7 @@ qs_status qs_dense_adjoint(qs_dense *psi, qs_dense *lam, const qs_gate *gates, c
             Launch L{};
             L.j = (int)p.tile.size();
             for (int k = 0; k < L.j; ++k) L.tq[k] = p.tile[k] - C;
+            L.tile = p.tile;
             L.gate_off = ag.size();
             L.out_off = nout;
             size_t g1 = g0;
@@ -3862,6 +3918,7 @@ qs_status qs_dense_adjoint(qs_dense *psi, qs_dense *lam, const qs_gate *gates, c
                     a.gen.zo = zo;
                 }
                 ag.push_back(a);
+                L.gates.push_back(gi);
             }
             L.ngates = ag.size() - L.gate_off;
             nout += L.local_to_global.size();
@@ -3869,17 +3926,56 @@ qs_status qs_dense_adjoint(qs_dense *psi, qs_dense *lam, const qs_gate *gates, c
             g0 = g1;
         }
     }
+    // register sweeps over both tiles (the shared-memory op path stays for
+    // launches the sweeps cannot express, and behind QOMPSIM_DUAL_SWEEPS=0)
+    const int RB = psi->f64 ? qs::kDualRegBitsF64 : qs::kDualRegBitsF32;
+    std::vector<qs::Sweep> all_sw;
+    std::vector<qs::ROp> all_rops;
+    std::vector<cplx> all_pool;
+    if (env_int("QOMPSIM_DUAL_SWEEPS", 1))
+        for (Launch &L : launches)
+            L.fused = plan_dual_sweeps(cg, L.gates, slots, gen_x, gen_z, L.tile, C, RB, &all_sw, &all_rops, &all_pool,
+                                       &L.sweeps);
     std::vector<double> acc(2 * (size_t)nslots, 0.0);
     double *dout = nullptr;
     qs::AdjGate *dg = nullptr;
+    qs::Sweep *dsw = nullptr;
+    qs::ROp *drops = nullptr;
+    void *dpool = nullptr;
+    const size_t pool_bytes = all_pool.size() * (psi->f64 ? 16 : 8);
+    std::vector<float> pool_f;
+    std::vector<double> pool_d;
+    if (psi->f64) pool_d = pool_as<double>(all_pool);
+    else pool_f = pool_as<float>(all_pool);
     cudaError_t e = cudaMalloc(&dg, std::max<size_t>(1, ag.size()) * sizeof(qs::AdjGate));
     if (e == cudaSuccess) e = cudaMalloc(&dout, std::max<size_t>(1, 2 * nout) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&dsw, std::max<size_t>(1, all_sw.size()) * sizeof(qs::Sweep));
+    if (e == cudaSuccess) e = cudaMalloc(&drops, std::max<size_t>(1, all_rops.size()) * sizeof(qs::ROp));
+    if (e == cudaSuccess) e = cudaMalloc(&dpool, std::max<size_t>(16, pool_bytes));
     if (e == cudaSuccess && !ag.empty())
         e = cudaMemcpyAsync(dg, ag.data(), ag.size() * sizeof(qs::AdjGate), cudaMemcpyHostToDevice, psi->stream);
+    if (e == cudaSuccess && !all_sw.empty())
+        e = cudaMemcpyAsync(dsw, all_sw.data(), all_sw.size() * sizeof(qs::Sweep), cudaMemcpyHostToDevice,
+                            psi->stream);
+    if (e == cudaSuccess && !all_rops.empty())
+        e = cudaMemcpyAsync(drops, all_rops.data(), all_rops.size() * sizeof(qs::ROp), cudaMemcpyHostToDevice,
+                            psi->stream);
+    if (e == cudaSuccess && pool_bytes)
+        e = cudaMemcpyAsync(dpool, psi->f64 ? (const void *)pool_d.data() : (const void *)pool_f.data(), pool_bytes,
+                            cudaMemcpyHostToDevice, psi->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(dout, 0, std::max<size_t>(1, 2 * nout) * sizeof(double), psi->stream);
     for (const Launch &L : launches) {
         if (e != cudaSuccess) break;
         qs::AdjPassArgs a{};
+        if (L.fused) {
+            a.sweeps = dsw + L.sweeps.sw_off;
+            a.nsweeps = (int32_t)L.sweeps.nsw;
+            a.rb = RB;
+            a.rops = drops + L.sweeps.rop_off;
+            a.pool = dpool;
+            a.nouter = (int32_t)L.sweeps.outer.size();
+            for (int i = 0; i < a.nouter; ++i) a.outer_q[i] = (int8_t)L.sweeps.outer[i];
+        }
         a.n = n;
         a.C = C;
         a.j = L.j;
@@ -3905,6 +4001,9 @@ qs_status qs_dense_adjoint(qs_dense *psi, qs_dense *lam, const qs_gate *gates, c
             }
     if (dg) cudaFree(dg);
     if (dout) cudaFree(dout);
+    if (dsw) cudaFree(dsw);
+    if (drops) cudaFree(drops);
+    if (dpool) cudaFree(dpool);
     if (e != cudaSuccess) return dfail(psi, QS_ERR_CUDA, std::string("adjoint: ") + cudaGetErrorString(e));
     for (size_t i = 0; i < acc.size(); ++i) out[i] = acc[i];
     return QS_OK;

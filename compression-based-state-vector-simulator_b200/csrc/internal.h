@@ -286,6 +286,15 @@ struct AdjPassArgs {
     void *lam;
     double *out;
     int32_t nslots;
+    // register sweeps over both tiles (nsweeps > 0: used instead of gates),
+    // as in DualPassArgs
+    const struct Sweep *sweeps;
+    int32_t nsweeps;
+    int32_t rb;
+    const struct ROp *rops;
+    const void *pool;
+    int8_t outer_q[kMaxOuterSel];
+    int32_t nouter;
 };
 
 // A pass over two compressed stores A and B of one geometry (the compressed

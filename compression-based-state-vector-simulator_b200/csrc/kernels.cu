@@ -2038,8 +2038,13 @@ __device__ void smem_apply_gate(typename Cplx<R>::T *t, int nb, const KGate &g, 
 constexpr int kAdjThreads = 256;
 constexpr int kMaxAdjSlots = 128;
 
+template <typename R, int RB>
+__device__ void dual_tile_sweeps(typename Cplx<R>::T *tA, typename Cplx<R>::T *tB, int nb, const Sweep *__restrict__ sweeps,
+                                 int nsweeps, const ROp *__restrict__ ops, const typename Cplx<R>::T *__restrict__ pool,
+                                 uint32_t ow, double *s_acc, int lane);
+
 template <typename R>
-__global__ void __launch_bounds__(kAdjThreads) adjoint_pass_kernel(const AdjPassArgs a) {
+__global__ void __launch_bounds__(kAdjThreads, 2) adjoint_pass_kernel(const AdjPassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double s_acc[2 * kMaxAdjSlots];
@@ -2063,7 +2068,17 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_pass_kernel(const AdjPass
         }
         __syncthreads();
         const uint64_t base_amp = chunk_base << C;
-        for (int k = 0; k < a.ngates; ++k) {
+        if (a.nsweeps > 0) {
+            uint32_t ow = 0;
+            for (int i = 0; i < a.nouter; ++i) ow |= (uint32_t)((base_amp >> a.outer_q[i]) & 1u) << i;
+            if constexpr (sizeof(R) == 4)
+                dual_tile_sweeps<R, kDualRegBitsF32>(tp, tl, nb, a.sweeps, a.nsweeps, a.rops,
+                                                     reinterpret_cast<const T *>(a.pool), ow, s_acc, lane);
+            else
+                dual_tile_sweeps<R, kDualRegBitsF64>(tp, tl, nb, a.sweeps, a.nsweeps, a.rops,
+                                                     reinterpret_cast<const T *>(a.pool), ow, s_acc, lane);
+        }
+        for (int k = 0; k < (a.nsweeps > 0 ? 0 : a.ngates); ++k) {
             const AdjGate &ag = a.gates[k];
             if (ag.slot >= 0) {
                 const int outer = __popcll(base_amp & ag.gen.zo) & 1;
@@ -2896,6 +2911,9 @@ cudaError_t launch_block_bytes(const ChunkMeta *meta, const uint8_t *mask, uint3
 template <typename R>
 static cudaError_t launch_adjoint_pass_t(const AdjPassArgs &a, cudaStream_t s) {
     if (a.nslots > kMaxAdjSlots) return cudaErrorInvalidValue;
+    if (a.nsweeps > 0 && (a.rb != (sizeof(R) == 8 ? kDualRegBitsF64 : kDualRegBitsF32) || a.C + a.j < a.rb ||
+                          a.nouter < 0 || a.nouter > kMaxOuterSel || !a.sweeps || !a.rops || !a.pool))
+        return cudaErrorInvalidValue;
     const int nb = a.C + a.j;
     const size_t smem = (size_t)(4 * sizeof(R)) << nb;
     cudaError_t e = cudaFuncSetAttribute(adjoint_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

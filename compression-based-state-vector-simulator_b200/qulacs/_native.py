@@ -80,6 +80,7 @@ class qs_stats(ct.Structure):
         ("host_store", ct.c_uint64),
         ("merged_from", ct.c_int64),
         ("tail_passes", ct.c_uint64),
+        ("pair_ms", ct.c_double),
     ]
 
 

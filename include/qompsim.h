@@ -118,6 +118,8 @@ typedef struct qs_stats {
                                     once every block is stored, the remaining stages' gates share
                                     passes (no stage boundary can change the mask any more) */
     uint64_t tail_passes;        /* device passes of that merged tail                   */
+    double pair_ms;              /* device time (CUDA events) of the launches of the
+                                    last qs_apply_pauli_sum / qs_adjoint on this state */
 } qs_stats;
 
 /* ---------------------------------------------------------------- errors */
