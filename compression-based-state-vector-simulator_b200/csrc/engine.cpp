@@ -574,6 +574,61 @@ void merge_diagonal_ops(const std::vector<qs::Sweep> &sweeps, size_t op0, std::v
 // whose bit-0 factor is exactly 1 in every variant touch only the bit-1
 // amplitudes; exact X and SWAP matrices become register moves.  Appends to
 // ops/pool; false when the pass needs more than kMaxOuterSel outer qubits.
+// When an op's selector bits form at most two runs of consecutive positions
+// of W, its variants are renumbered so that variant bit j is the j-th
+// selector in ascending position, and the op carries the runs instead of the
+// bit list (sel[0] = kSelRuns | start1, sel[1] = length1, sel[2] = start2,
+// sel[3] = length2): the device then computes the variant with two shifts
+// and masks instead of one extract per selector.  stride: pool entries per
+// variant, starting at o->mat (the op's entries are the last ones appended).
+void encode_selector_runs(qs::ROp *o, int stride, std::vector<cplx> *pool) {
+    const int ns = o->nsel;
+    if (ns == 0 || stride == 0) return;
+    std::vector<int> order(ns);
+    for (int j = 0; j < ns; ++j) order[j] = j;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return o->sel[a] < o->sel[b]; });
+    int runs = 1, start[2] = {o->sel[order[0]], 0}, len[2] = {1, 0};
+    for (int j = 1; j < ns; ++j) {
+        if (o->sel[order[j]] == o->sel[order[j - 1]] + 1) {
+            ++len[runs - 1];
+        } else {
+            if (++runs > 2) return;
+            start[1] = o->sel[order[j]];
+            len[1] = 1;
+        }
+    }
+    const size_t nvar = size_t(1) << ns;
+    std::vector<cplx> old(pool->begin() + o->mat, pool->begin() + o->mat + nvar * stride);
+    for (size_t vn = 0; vn < nvar; ++vn) {
+        size_t vo = 0;
+        for (int j = 0; j < ns; ++j)
+            if ((vn >> j) & 1) vo |= size_t(1) << order[j];
+        for (int e = 0; e < stride; ++e) (*pool)[o->mat + vn * stride + e] = old[vo * stride + e];
+    }
+    for (int j = 0; j < qs::kMaxSel; ++j) o->sel[j] = 0;
+    o->sel[0] = (uint8_t)(qs::kSelRuns | start[0]);
+    o->sel[1] = (uint8_t)len[0];
+    o->sel[2] = (uint8_t)start[1];
+    o->sel[3] = (uint8_t)len[1];
+}
+
+// Runs of half-diagonal ops on one register bit inside a sweep (phases that
+// the diagonal merge could not join because their selectors are too many):
+// every op but the last only multiplies a pending factor (OPC_ACC), the last
+// (OPC_D2HP) applies the product once.  ops[op0 + sweep.g0 .. g1) per sweep.
+void fuse_half_chains(std::vector<qs::ROp> *ops, size_t op0, const std::vector<qs::Sweep> &sweeps) {
+    for (const auto &sw : sweeps)
+        for (int k = sw.g0 + 1; k < sw.g1; ++k) {
+            qs::ROp &prev = (*ops)[op0 + k - 1], &cur = (*ops)[op0 + k];
+            if (cur.code < qs::OPC_D2H || cur.code >= qs::OPC_D2H + 8) continue;
+            const int bit = cur.code - qs::OPC_D2H;
+            const bool chained = prev.code == qs::OPC_D2H + bit || prev.code == qs::OPC_D2HP + bit;
+            if (!chained) continue;
+            prev.code = qs::OPC_ACC;
+            cur.code = (uint8_t)(qs::OPC_D2HP + bit);
+        }
+}
+
 bool finalize_ops(const std::vector<RawOp> &raw, const std::vector<cplx> &rpool, int nb, std::vector<int> *outer,
                   std::vector<qs::ROp> *ops, std::vector<cplx> *pool) {
     const cplx one(1.0, 0.0), zero(0.0, 0.0);
@@ -667,6 +722,7 @@ bool finalize_ops(const std::vector<RawOp> &raw, const std::vector<cplx> &rpool,
                 break;
             }
         }
+        encode_selector_runs(&o, r.kind == RK_SUM ? 1 : o.vstride, pool);
         ops->push_back(o);
     }
     return true;
@@ -903,6 +959,7 @@ bool plan_dual_sweeps(const std::vector<CGate> &cg, const std::vector<uint32_t> 
         all_pool->resize(pool0);
         return false;
     }
+    fuse_half_chains(&rops, 0, msw);
     out->sw_off = all_sw->size();
     out->nsw = msw.size();
     out->rop_off = all_rops->size();
@@ -1424,6 +1481,7 @@ static qs_status emit_passes(qs_state *h, uint32_t stage, const std::vector<CGat
         std::vector<int> outer;
         if (!finalize_ops(raw, rpool, C + dp.j, &outer, &ops, &pool))
             return fail(h, QS_ERR_ARG, "a pass needs more outer selector qubits than the planner allows");
+        fuse_half_chains(&ops, op0, swp);
         dp.nouter = (int)outer.size();
         for (size_t i = 0; i < outer.size(); ++i) dp.outer_q[i] = (int8_t)outer[i];
         dp.op_off = (uint32_t)op0;
@@ -1438,12 +1496,14 @@ static qs_status emit_passes(qs_state *h, uint32_t stage, const std::vector<CGat
             int kinds[5] = {0, 0, 0, 0, 0}, sel = 0, half = 0, moves = 0;
             for (size_t o = op0; o < ops.size(); ++o) {
                 const int c = ops[o].code;
-                const int kind = c == qs::OPC_SCALAR ? 0 : c < qs::OPC_M2 ? 1 : c < qs::OPC_D4 ? 2
-                               : c < qs::OPC_M4 ? 3 : 4;
+                const int kind = c == qs::OPC_SCALAR ? 0
+                               : (c < qs::OPC_M2 || (c >= qs::OPC_ACC && c < qs::OPC_D4)) ? 1
+                               : c < qs::OPC_D4 ? 2 : c < qs::OPC_M4 ? 3 : 4;
                 ++kinds[kind];
                 sel += ops[o].nsel;
-                half += (c >= qs::OPC_D2H && c < qs::OPC_M2) || (c >= qs::OPC_D4H && c < qs::OPC_M4);
-                moves += (c >= qs::OPC_X && c < qs::OPC_D4) || c >= qs::OPC_SWAP;
+                half += (c >= qs::OPC_D2H && c < qs::OPC_M2) || (c >= qs::OPC_ACC && c < qs::OPC_D4) ||
+                        (c >= qs::OPC_D4H && c < qs::OPC_M4);
+                moves += (c >= qs::OPC_X && c < qs::OPC_X + 8) || (c >= qs::OPC_SWAP && c < qs::OPC_SWAP + 64);
             }
             printf("stage %u pass %zu: j=%d gates=%u sweeps=%zu ops=%zu (scalar %d d2 %d m2 %d d4 %d m4 %d, "
                    "half-diagonal %d, moves %d, selectors %d, outer %d)%s tile=[", stage, p, dp.j, dp.ngates,
@@ -3574,6 +3634,7 @@ qs_status qs_dense_apply_gates(qs_dense *h, const qs_gate *gates, size_t count) 
         std::vector<int> outer;
         if (!finalize_ops(raw, rpool, C + (int)p.tile.size(), &outer, &ops, &pool))
             return dfail(h, QS_ERR_ARG, "a pass needs more outer selector qubits than the planner allows");
+        fuse_half_chains(&ops, op0, swp);
         outers.push_back(outer);
         op_offsets.push_back(op0);
         sweep_ranges.push_back({sw.size(), swp.size()});

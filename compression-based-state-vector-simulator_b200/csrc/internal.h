@@ -83,9 +83,13 @@ constexpr int kSweepThreads = 128;
 //   OPC_D4H + (a*8+b)    diag(1, m0, m1, m2) on bits a < b
 //   OPC_M4  + (a*8+b)    4x4 matrix m0..m15 on bits a < b
 //   OPC_SWAP + (a*8+b)   exchange bits a and b (no arithmetic)
+//   OPC_ACC              zh *= m[0]               (a pending bit-1 factor)
+//   OPC_D2HP + k         diag(1, zh m0) on bit k, then zh = 1: the last of a
+//                        run of half-diagonals on one bit inside a sweep, the
+//                        others of which became OPC_ACC (fuse_half_chains)
 //   OPC_SUM              two-store sweeps only: derivative sum, see below
 enum : uint8_t {
-    OPC_SCALAR = 0, OPC_D2 = 8, OPC_D2H = 16, OPC_M2 = 24, OPC_X = 32,
+    OPC_SCALAR = 0, OPC_D2 = 8, OPC_D2H = 16, OPC_M2 = 24, OPC_X = 32, OPC_ACC = 40, OPC_D2HP = 48,
     OPC_D4 = 64, OPC_D4H = 96, OPC_M4 = 128, OPC_SWAP = 160, OPC_SUM = 224
 };
 // OPC_SUM in a two-store sweep (groups v of store A and w of store B at the
@@ -96,6 +100,10 @@ enum : uint8_t {
 // scalar factors enter as conj(zB) zA.
 constexpr int kMaxSel = 8;
 constexpr uint8_t kSelNone = 31;
+// sel[0] with this bit set: the selectors are given as at most two runs of
+// consecutive W bits (sel[0] & 31 = start of the first, sel[1] its length,
+// sel[2] / sel[3] the second), variant bit j = the j-th selector in order.
+constexpr uint8_t kSelRuns = 0x80;
 struct ROp {
     uint8_t code;
     uint8_t nsel;        // 0..kMaxSel selector bits

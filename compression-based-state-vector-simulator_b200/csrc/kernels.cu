@@ -185,7 +185,7 @@ __device__ __forceinline__ void r_swap(T (&v)[NS]) {
 // One register op on a group (codes in internal.h).  z collects the group's
 // scalar factors and is applied when the group is stored.
 template <int RB, typename T>
-__device__ __forceinline__ void apply_rop(T (&v)[1 << RB], T &z, int code, const T *__restrict__ m) {
+__device__ __forceinline__ void apply_rop(T (&v)[1 << RB], T &z, T &zh, int code, const T *__restrict__ m) {
     constexpr int NS = 1 << RB;
 #define QS_K(BASE, K, ...) \
     case BASE + K:         \
@@ -200,6 +200,7 @@ __device__ __forceinline__ void apply_rop(T (&v)[1 << RB], T &z, int code, const
     F(BASE, 1, 3) F(BASE, 1, 4) F(BASE, 2, 3) F(BASE, 2, 4) F(BASE, 3, 4)
 #define QS_D2(B, K) QS_K(B, K, r_diag2<NS, K>(v, m[0], m[1]))
 #define QS_D2H(B, K) QS_K(B, K, r_half2<NS, K>(v, m[0]))
+#define QS_D2HP(B, K) QS_K(B, K, r_half2<NS, K>(v, cmul(zh, m[0])); zh = c_one<T>())
 #define QS_M2(B, K) QS_K(B, K, r_2x2<NS, K>(v, m[0], m[1], m[2], m[3]))
 #define QS_X(B, K) QS_K(B, K, r_x<NS, K>(v))
 #define QS_D4(B, A, C) QS_P(B, A, C, r_diag4<NS, A, C>(v, m[0], m[1], m[2], m[3]))
@@ -208,8 +209,10 @@ __device__ __forceinline__ void apply_rop(T (&v)[1 << RB], T &z, int code, const
 #define QS_SW(B, A, C) QS_P(B, A, C, r_swap<NS, A, C>(v))
     switch (code) {
         case OPC_SCALAR: z = cmul(z, m[0]); break;
+        case OPC_ACC: zh = cmul(zh, m[0]); break;
         QS_ALLK(OPC_D2, QS_D2)
         QS_ALLK(OPC_D2H, QS_D2H)
+        QS_ALLK(OPC_D2HP, QS_D2HP)
         QS_ALLK(OPC_M2, QS_M2)
         QS_ALLK(OPC_X, QS_X)
         QS_ALLP(OPC_D4, QS_D4)
@@ -224,6 +227,7 @@ __device__ __forceinline__ void apply_rop(T (&v)[1 << RB], T &z, int code, const
 #undef QS_ALLP
 #undef QS_D2
 #undef QS_D2H
+#undef QS_D2HP
 #undef QS_M2
 #undef QS_X
 #undef QS_D4
@@ -235,6 +239,10 @@ __device__ __forceinline__ void apply_rop(T (&v)[1 << RB], T &z, int code, const
 // Variant index of an op for a group with word W (selector bits of W).
 __device__ __forceinline__ uint32_t rop_variant(const ROp &o, uint32_t W) {
     uint32_t var = 0;
+    if (o.sel[0] & kSelRuns) {
+        const uint32_t a = o.sel[0] & 31u, la = o.sel[1], b = o.sel[2], lb = o.sel[3];
+        return ((W >> a) & ((1u << la) - 1u)) | (((W >> b) & ((1u << lb) - 1u)) << la);
+    }
     if (o.nsel) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) var |= ((W >> o.sel[j]) & 1u) << j;
@@ -309,10 +317,10 @@ __device__ __forceinline__ void tile_sweeps_body(typename Cplx<R>::T *tile, int 
             T v[NS];
 #pragma unroll
             for (int s = 0; s < NS; ++s) v[s] = tile[swz<R>(base | off(s), swm)];
-            T z = c_one<T>();
+            T z = c_one<T>(), zh = c_one<T>();
             for (int k = sw.g0; k < sw.g1; ++k) {
                 const ROp o = ops[k];
-                apply_rop<RB>(v, z, o.code, pool + o.mat + rop_variant(o, W) * o.vstride);
+                apply_rop<RB>(v, z, zh, o.code, pool + o.mat + rop_variant(o, W) * o.vstride);
             }
             if (z.x != R(1) || z.y != R(0)) {
 #pragma unroll
@@ -2278,7 +2286,7 @@ __device__ void dual_tile_sweeps(typename Cplx<R>::T *tA, typename Cplx<R>::T *t
                 v[s] = live ? tA[base | off(s)] : make_c<T, R>(0.0, 0.0);
                 w[s] = live ? tB[base | off(s)] : make_c<T, R>(0.0, 0.0);
             }
-            T za = c_one<T>(), zb = c_one<T>();
+            T za = c_one<T>(), zb = c_one<T>(), zha = c_one<T>(), zhb = c_one<T>();
             for (int k = sw.g0; k < sw.g1; ++k) {
                 const ROp o = ops[k];
                 if (o.code == OPC_SUM) {
@@ -2301,8 +2309,8 @@ __device__ void dual_tile_sweeps(typename Cplx<R>::T *tA, typename Cplx<R>::T *t
                     }
                 } else {
                     const T *m = pool + o.mat + rop_variant(o, W) * o.vstride;
-                    apply_rop<RB>(v, za, o.code, m);
-                    apply_rop<RB>(w, zb, o.code, m);
+                    apply_rop<RB>(v, za, zha, o.code, m);
+                    apply_rop<RB>(w, zb, zhb, o.code, m);
                 }
             }
             if (live) {
