@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <climits>
 #include <cstdlib>
+#include <map>
 #include <mutex>
 
 #include "codec.cuh"
@@ -2591,6 +2592,26 @@ __global__ void block_bytes_kernel(const ChunkMeta *meta, const uint8_t *mask, u
     }
 }
 
+// Raises a kernel's dynamic shared-memory limit to at least `smem` bytes on
+// the current device and never lowers it: the limit is per function, shared
+// by every host thread and handle, so a thread that lowered it between
+// another thread's setting and its launch would make that launch fail.
+std::mutex g_smem_attr_mu;
+std::map<std::pair<const void *, int>, size_t> g_smem_attr;
+
+template <typename K>
+cudaError_t ensure_dyn_smem(K *kernel, size_t smem) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(g_smem_attr_mu);
+    size_t &cur = g_smem_attr[{reinterpret_cast<const void *>(kernel), dev}];
+    if (smem <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) cur = smem;
+    return e;
+}
+
 int g_sm_count = 0;
 
 // Scratch of the allocation-free codec round trip (qs_codec_roundtrip_noalloc):
@@ -2623,8 +2644,7 @@ template <typename R, int RB, bool kCodes, int kHB>
 static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
     const int nb = a.C + a.j;
     const size_t smem = pass_smem_bytes(sizeof(R) == 8, nb, a.j);
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, RB, kCodes, kHB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = ensure_dyn_smem(pass_kernel<R, RB, kCodes, kHB>, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<R, RB, kCodes, kHB>, kSweepThreads, smem);
@@ -2647,8 +2667,7 @@ static cudaError_t launch_staged_t(const PassArgs &a, cudaStream_t s) {
     const uint32_t nblk = 1u << (a.n - a.B);
     const uint32_t mask_words = nblk <= kMaxSmemBlocks ? (nblk + 31) / 32 : 0;
     const size_t smem = staged_layout(sizeof(R) == 8, a.C, a.j, mask_words, kDense ? a.dense.k : 0).total;
-    cudaError_t e = cudaFuncSetAttribute(staged_pass_kernel<R, kCodes, kDense>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_dyn_smem(staged_pass_kernel<R, kCodes, kDense>, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, staged_pass_kernel<R, kCodes, kDense>, kStagedThreads,
@@ -2706,7 +2725,7 @@ template <typename R, int RB>
 static cudaError_t launch_dense_pass_t(const DensePassArgs &a, cudaStream_t s) {
     const int nb = a.C + a.j;
     const size_t smem = (size_t)(2 * sizeof(R)) << nb;
-    cudaError_t e = cudaFuncSetAttribute(dense_pass_kernel<R, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_dyn_smem(dense_pass_kernel<R, RB>, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense_pass_kernel<R, RB>, kSweepThreads, smem);
@@ -2842,7 +2861,7 @@ static cudaError_t launch_dual_t(const DualPassArgs &a, cudaStream_t s) {
                           a.nouter < 0 || a.nouter > kMaxOuterSel || !a.sweeps || !a.rops || !a.pool))
         return cudaErrorInvalidValue;
     const size_t smem = dual_pass_smem_bytes(sizeof(R) == 8, a.C, a.j);
-    cudaError_t e = cudaFuncSetAttribute(dual_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_dyn_smem(dual_pass_kernel<R>, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     const int threads = dual_threads(a.C + a.j);
@@ -2924,7 +2943,7 @@ static cudaError_t launch_adjoint_pass_t(const AdjPassArgs &a, cudaStream_t s) {
         return cudaErrorInvalidValue;
     const int nb = a.C + a.j;
     const size_t smem = (size_t)(4 * sizeof(R)) << nb;
-    cudaError_t e = cudaFuncSetAttribute(adjoint_pass_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_dyn_smem(adjoint_pass_kernel<R>, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_pass_kernel<R>, kAdjThreads, smem);
@@ -2986,7 +3005,7 @@ static cudaError_t launch_expect_t(const ExpectArgs &a, cudaStream_t s) {
     const int nb = a.C + a.j;
     const size_t tiles = a.meta_bra ? 2 : 1;
     const size_t smem = tiles * ((size_t)(2 * sizeof(R)) << nb) + (size_t)(kExpectThreads / 32) * kStageWords * 4;
-    cudaError_t e = cudaFuncSetAttribute(expect_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_dyn_smem(expect_kernel<R>, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, expect_kernel<R>, kExpectThreads, smem);
