@@ -19,6 +19,8 @@
  *                QuantumCircuit::update_quantum_state, src/cppsim/circuit.cpp:23-34).
  *
  * Threading: a handle is not re-entrant; use one handle per host thread.
+ * Handles on different threads may run concurrently (the per-kernel launch
+ * settings they share are only ever raised, under a lock).
  * All device work of a handle is ordered on one CUDA stream (qs_set_stream,
  * default: the legacy default stream).  Calls that return host data
  * synchronise that stream.
