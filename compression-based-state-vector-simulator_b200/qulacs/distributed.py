@@ -131,16 +131,21 @@ class _ThreadEndpoint:
     def allgather(self, arr: np.ndarray) -> List[np.ndarray]:
         out = []
         k = self._next(self.rank, -1)
-        self.hub._post((self.rank, -1, k), np.array(arr))
+        # the posted copy carries how many other ranks still have to read it
+        self.hub._post((self.rank, -1, k), [np.array(arr), self.size - 1])
         for r in range(self.size):
             if r == self.rank:
                 out.append(np.array(arr))
-            else:
-                with self.hub._cv:
-                    key = (r, -1, k)
-                    if not self.hub._cv.wait_for(lambda: key in self.hub._box, timeout=self.hub._timeout):
-                        raise TimeoutError(f"allgather {key} timed out")
-                    out.append(np.array(self.hub._box[key]))
+                continue
+            with self.hub._cv:
+                key = (r, -1, k)
+                if not self.hub._cv.wait_for(lambda: key in self.hub._box, timeout=self.hub._timeout):
+                    raise TimeoutError(f"allgather {key} timed out")
+                entry = self.hub._box[key]
+                out.append(np.array(entry[0]))
+                entry[1] -= 1
+                if entry[1] == 0:
+                    del self.hub._box[key]
         return out
 
 
