@@ -3307,6 +3307,24 @@ qs_status qs_import_store(qs_state *h, const void *buf, uint64_t size) {
     return QS_OK;
 }
 
+qs_status qs_selftest_bounded_wait(uint32_t tries, int32_t *gave_up) {
+    if (!gave_up || tries == 0) return fail(nullptr, QS_ERR_ARG, "gave_up must not be NULL and tries > 0");
+    int32_t *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(d, 0xff, sizeof(int32_t));
+    if (e == cudaSuccess) e = qs::launch_bounded_wait_selftest(tries, d, nullptr);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(nullptr);
+    int32_t v = -1;
+    if (e == cudaSuccess) e = cudaMemcpy(&v, d, sizeof(v), cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return fail(nullptr, QS_ERR_CUDA, std::string("bounded-wait self-test: ") + cudaGetErrorString(e));
+    }
+    *gave_up = v;
+    return QS_OK;
+}
+
 qs_status qs_set_zero_vector(qs_state *h) {
     if (!h) return fail(nullptr, QS_ERR_ARG, "NULL handle");
     cudaStream_t s = h->stream;

@@ -473,6 +473,10 @@ cudaError_t launch_half_check(const HalfChunks &h, const ChunkMeta *in_meta, con
 cudaError_t launch_block_bytes(const ChunkMeta *meta, const uint8_t *mask, uint32_t nb, int cshift, int C,
                                unsigned long long *block_bytes, cudaStream_t stream);
 
+// One CTA arms an mbarrier that nothing completes and runs the bounded wait
+// of the staged kernels with `tries` tries; *gave_up = 1 when it gave up.
+cudaError_t launch_bounded_wait_selftest(uint32_t tries, int32_t *gave_up, cudaStream_t stream);
+
 int sm_count();
 
 }  // namespace qs

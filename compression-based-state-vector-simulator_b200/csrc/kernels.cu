@@ -815,11 +815,31 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 }
 
 // Wait for the phase of `bar` with the given parity to complete; false when
-// it has not after kMbarSpinLimit tries.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kMbarSpinLimit; ++i)
+// it has not after `tries` tries.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t tries = kMbarSpinLimit) {
+    for (uint32_t i = 0; i < tries; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
+}
+
+__device__ __forceinline__ void mbar_inval(uint64_t *bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// The bounded wait's give-up path, exercised without any copy: thread 0
+// arms an mbarrier for 16 bytes that nothing will deliver and waits at most
+// `tries` times; *gave_up = 1 when the wait returned false (as it must), 0
+// otherwise.  No asynchronous operation targets the barrier, so the CTA
+// invalidates it and exits cleanly.
+__global__ void bounded_wait_selftest_kernel(uint32_t tries, int32_t *gave_up) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_arrive_expect_tx(&bar, 16);
+        const bool done = mbar_wait_bounded(&bar, 0, tries);
+        mbar_inval(&bar);
+        *gave_up = done ? 0 : 1;
+    }
 }
 
 // 1-D bulk copy global -> this CTA's shared memory, completion (in bytes) on
@@ -2925,6 +2945,11 @@ cudaError_t launch_half_check(const HalfChunks &h, const ChunkMeta *in_meta, con
     cudaError_t e = cudaMemsetAsync(bad, 0, sizeof(int32_t), s);
     if (e != cudaSuccess || h.nhalf == 0) return e;
     half_check_kernel<<<grid_for(h.nhalf, 256, 8), 256, 0, s>>>(h, in_meta, in_flags, payload_bytes_total, bad);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bounded_wait_selftest(uint32_t tries, int32_t *gave_up, cudaStream_t s) {
+    bounded_wait_selftest_kernel<<<1, 32, 0, s>>>(tries, gave_up);
     return cudaGetLastError();
 }
 

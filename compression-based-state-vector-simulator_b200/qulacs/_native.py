@@ -138,6 +138,7 @@ SIGNATURES = [
     ("qs_export_half", ct.c_int, [_P, _U32, _U32, _P, _U64, ct.POINTER(_U64)]),
     ("qs_import_half", ct.c_int, [_P, _U32, _U32, _P, _U64]),
     ("qs_set_zero_vector", ct.c_int, [_P]),
+    ("qs_selftest_bounded_wait", ct.c_int, [_U32, ct.POINTER(ct.c_int32)]),
     ("qs_checkpoint", ct.c_int, [_P, _U32]),
     ("qs_restore", ct.c_int, [_P, _U32]),
     ("qs_free_checkpoint", ct.c_int, [_P, _U32]),

@@ -352,6 +352,13 @@ qs_status qs_export_half(qs_state *h, uint32_t qubit, uint32_t value, void *dev_
 qs_status qs_import_half(qs_state *h, uint32_t qubit, uint32_t value, const void *dev_buf, uint64_t size);
 qs_status qs_set_zero_vector(qs_state *h);
 
+/* Failure-path self-test of the bounded device waits (the staged and dense
+ * tensor-core passes wait on mbarriers with an iteration limit, after which
+ * the pass sets its error flag and the call returns QS_ERR_TIMEOUT): one CTA
+ * arms an mbarrier that nothing completes and waits at most `tries` times.
+ * *gave_up = 1 when the wait gave up, as it must; the context stays usable. */
+qs_status qs_selftest_bounded_wait(uint32_t tries, int32_t *gave_up);
+
 /* Device-side checkpoints of the compressed store (zero mask, per-block
  * bytes, chunk headers and the payload in use): qs_checkpoint copies the
  * current store into slot (0..63, allocated on first use, regrown when the
