@@ -544,8 +544,9 @@ constexpr bool kPrefetchDecode = sizeof(R) == 8;
 // moves, chunk permutations), so the tile holds the quantised codes
 // themselves and the pass skips dequantisation and quantisation.
 // kHB: complex64 chunk headers loaded per warp batch (4 or 8).
-// kC: the chunk log2 when known at compile time, 0 to read it from the args.
-template <typename R, int RB, bool kCodes, int kHB, int kC>
+// kC, kJ: the chunk log2 and the tile qubits above the chunk when known at
+// compile time, 0 to read them from the args.
+template <typename R, int RB, bool kCodes, int kHB, int kC, int kJ>
 __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -561,7 +562,7 @@ __global__ void __launch_bounds__(kSweepThreads, 3) pass_kernel(const PassArgs a
     }
     __syncthreads();
 
-    const int C = kC ? kC : a.C, j = a.j, nb = C + j;
+    const int C = kC ? kC : a.C, j = kJ ? kJ : a.j, nb = C + j;
     const int nchunks = 1 << j;
     const int ncomp = 2 << C;
     const int per_lane = ncomp >> 5;
@@ -2348,7 +2349,9 @@ __device__ void dual_tile_sweeps(typename Cplx<R>::T *tA, typename Cplx<R>::T *t
     }
 }
 
-template <typename R>
+// kC, kJ: chunk log2 and tile qubits above the chunk as compile-time
+// constants (0: read from the args), as for pass_kernel.
+template <typename R, int kC, int kJ>
 __global__ void __launch_bounds__(kDualThreadsWide) dual_pass_kernel(const DualPassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char dual_smem[];
@@ -2356,7 +2359,7 @@ __global__ void __launch_bounds__(kDualThreadsWide) dual_pass_kernel(const DualP
     __shared__ int32_t s_tq[kMaxTileQubits];
     __shared__ unsigned long long s_tile_off;
     __shared__ int s_flag;
-    const int C = a.C, j = a.j, nb = C + j, size = 1 << nb;
+    const int C = kC ? kC : a.C, j = kJ ? kJ : a.j, nb = C + j, size = 1 << nb;
     const int nchunks = 1 << j;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int blk_shift = a.B - C;
@@ -2661,14 +2664,14 @@ int sm_count() {
     return g_sm_count;
 }
 
-template <typename R, int RB, bool kCodes, int kHB, int kC>
+template <typename R, int RB, bool kCodes, int kHB, int kC, int kJ>
 static cudaError_t launch_pass_kc(const PassArgs &a, cudaStream_t s) {
     const int nb = a.C + a.j;
     const size_t smem = pass_smem_bytes(sizeof(R) == 8, nb, a.j);
-    cudaError_t e = ensure_dyn_smem(pass_kernel<R, RB, kCodes, kHB, kC>, smem);
+    cudaError_t e = ensure_dyn_smem(pass_kernel<R, RB, kCodes, kHB, kC, kJ>, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<R, RB, kCodes, kHB, kC>, kSweepThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<R, RB, kCodes, kHB, kC, kJ>, kSweepThreads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t grid = (uint64_t)per_sm * sm_count();
@@ -2679,17 +2682,21 @@ static cudaError_t launch_pass_kc(const PassArgs &a, cudaStream_t s) {
     const char *env = std::getenv("QOMPSIM_SLAB_BYTES");
     const uint64_t slab = env ? (uint64_t)std::strtoull(env, nullptr, 10) : (uint64_t)kArenaSlabBytes;
     b.slab = (slab && a.capacity / grid >= 8 * slab) ? (slab + 127) / 128 * 128 : 0;
-    pass_kernel<R, RB, kCodes, kHB, kC><<<(unsigned)grid, kSweepThreads, smem, s>>>(b);
+    pass_kernel<R, RB, kCodes, kHB, kC, kJ><<<(unsigned)grid, kSweepThreads, smem, s>>>(b);
     return cudaGetLastError();
 }
 
-// The default chunk size (2^8 amplitudes) is a compile-time constant of its
-// instantiation: the per-lane counts, chunk offsets and swizzle mask then
-// fold into the code (measured 8-14 % faster than reading C from the args).
+// The default chunk size (2^8 amplitudes) and the default tile (2^12
+// amplitudes for complex128, 2^13 for complex64, i.e. 4 or 5 tile qubits
+// above the chunk) are compile-time constants of their instantiation: the
+// per-lane counts, chunk and group counts, offsets and swizzle mask then fold
+// into the code (measured 12-19 % faster than reading them from the args).
 template <typename R, int RB, bool kCodes, int kHB>
 static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
-    return a.C == kMaxChunkLog2 ? launch_pass_kc<R, RB, kCodes, kHB, kMaxChunkLog2>(a, s)
-                                : launch_pass_kc<R, RB, kCodes, kHB, 0>(a, s);
+    constexpr int J = sizeof(R) == 8 ? 4 : 5;
+    if (a.C == kMaxChunkLog2 && a.j == J) return launch_pass_kc<R, RB, kCodes, kHB, kMaxChunkLog2, J>(a, s);
+    return a.C == kMaxChunkLog2 ? launch_pass_kc<R, RB, kCodes, kHB, kMaxChunkLog2, 0>(a, s)
+                                : launch_pass_kc<R, RB, kCodes, kHB, 0, 0>(a, s);
 }
 
 template <typename R, bool kCodes, bool kDense = false>
@@ -2884,25 +2891,31 @@ cudaError_t launch_codec_test(bool f64, const void *vals, int C, CodecParams p, 
 
 uint64_t noalloc_scratch_words() { return kNoAllocScratchWords; }
 
-template <typename R>
-static cudaError_t launch_dual_t(const DualPassArgs &a, cudaStream_t s) {
+template <typename R, int kC, int kJ>
+static cudaError_t launch_dual_kc(const DualPassArgs &a, cudaStream_t s) {
     if (a.nslots > kMaxDualSlots) return cudaErrorInvalidValue;
     if (a.nsweeps > 0 && (a.rb != (sizeof(R) == 8 ? kDualRegBitsF64 : kDualRegBitsF32) || a.C + a.j < a.rb ||
                           a.nouter < 0 || a.nouter > kMaxOuterSel || !a.sweeps || !a.rops || !a.pool))
         return cudaErrorInvalidValue;
     const size_t smem = dual_pass_smem_bytes(sizeof(R) == 8, a.C, a.j);
-    cudaError_t e = ensure_dyn_smem(dual_pass_kernel<R>, smem);
+    cudaError_t e = ensure_dyn_smem(dual_pass_kernel<R, kC, kJ>, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     const int threads = dual_threads(a.C + a.j);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dual_pass_kernel<R>, threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dual_pass_kernel<R, kC, kJ>, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t grid = (uint64_t)per_sm * sm_count();
     if (grid > a.n_tiles) grid = a.n_tiles;
     if (grid == 0) grid = 1;
-    dual_pass_kernel<R><<<(unsigned)grid, threads, smem, s>>>(a);
+    dual_pass_kernel<R, kC, kJ><<<(unsigned)grid, threads, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t launch_dual_t(const DualPassArgs &a, cudaStream_t s) {
+    if (a.C == kMaxChunkLog2 && a.j == 4) return launch_dual_kc<R, kMaxChunkLog2, 4>(a, s);
+    return launch_dual_kc<R, 0, 0>(a, s);
 }
 
 cudaError_t launch_dual_pass(bool f64, const DualPassArgs &a, cudaStream_t s) {
