@@ -1105,7 +1105,8 @@ __device__ void tile_dense_k_f64(double2 *tile, int nb, int swm, int k, const in
 
 // kDense: the pass applies the dense k-qubit gate a.dense over every tile
 // (tile_dense_k_tc / tile_dense_k_f64) instead of the register sweeps.
-template <typename R, bool kCodes, bool kDense>
+// kC, kJ: compile-time chunk log2 and tile qubits (0: from the args).
+template <typename R, bool kCodes, bool kDense, int kC, int kJ>
 __global__ void __launch_bounds__(kStagedThreads, 1) staged_pass_kernel(const PassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(128) unsigned char staged_smem[];
@@ -1118,7 +1119,7 @@ __global__ void __launch_bounds__(kStagedThreads, 1) staged_pass_kernel(const Pa
     __shared__ int32_t s_tq[kMaxTileQubits];
     __shared__ int8_t s_oq[kMaxOuterSel];
 
-    const int C = a.C, j = a.j, nb = C + j;
+    const int C = kC ? kC : a.C, j = kJ ? kJ : a.j, nb = C + j;
     const int nchunks = 1 << j;
     const int ncomp = 2 << C;
     const int per_lane = ncomp >> 5;
@@ -2699,15 +2700,15 @@ static cudaError_t launch_pass_t(const PassArgs &a, cudaStream_t s) {
                                 : launch_pass_kc<R, RB, kCodes, kHB, 0, 0>(a, s);
 }
 
-template <typename R, bool kCodes, bool kDense = false>
-static cudaError_t launch_staged_t(const PassArgs &a, cudaStream_t s) {
+template <typename R, bool kCodes, bool kDense, int kC, int kJ>
+static cudaError_t launch_staged_kc(const PassArgs &a, cudaStream_t s) {
     const uint32_t nblk = 1u << (a.n - a.B);
     const uint32_t mask_words = nblk <= kMaxSmemBlocks ? (nblk + 31) / 32 : 0;
     const size_t smem = staged_layout(sizeof(R) == 8, a.C, a.j, mask_words, kDense ? a.dense.k : 0).total;
-    cudaError_t e = ensure_dyn_smem(staged_pass_kernel<R, kCodes, kDense>, smem);
+    cudaError_t e = ensure_dyn_smem(staged_pass_kernel<R, kCodes, kDense, kC, kJ>, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, staged_pass_kernel<R, kCodes, kDense>, kStagedThreads,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, staged_pass_kernel<R, kCodes, kDense, kC, kJ>, kStagedThreads,
                                                       smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
@@ -2718,12 +2719,19 @@ static cudaError_t launch_staged_t(const PassArgs &a, cudaStream_t s) {
     const char *env = std::getenv("QOMPSIM_SLAB_BYTES");
     const uint64_t slab = env ? (uint64_t)std::strtoull(env, nullptr, 10) : (uint64_t)kArenaSlabBytes;
     b.slab = (slab && a.capacity / grid >= 8 * slab) ? (slab + 127) / 128 * 128 : 0;
-    staged_pass_kernel<R, kCodes, kDense><<<(unsigned)grid, kStagedThreads, smem, s>>>(b);
+    staged_pass_kernel<R, kCodes, kDense, kC, kJ><<<(unsigned)grid, kStagedThreads, smem, s>>>(b);
     return cudaGetLastError();
 }
 
 size_t staged_pass_smem_bytes(bool f64, int C, int j, uint32_t nblocks) {
     return staged_layout(f64, C, j, nblocks <= kMaxSmemBlocks ? (nblocks + 31) / 32 : 0).total;
+}
+
+template <typename R, bool kCodes, bool kDense = false>
+static cudaError_t launch_staged_t(const PassArgs &a, cudaStream_t s) {
+    if (a.C == kMaxChunkLog2 && a.C + a.j == kDenseTileLog2)
+        return launch_staged_kc<R, kCodes, kDense, kMaxChunkLog2, kDenseTileLog2 - kMaxChunkLog2>(a, s);
+    return launch_staged_kc<R, kCodes, kDense, 0, 0>(a, s);
 }
 
 cudaError_t launch_pass(bool f64, const PassArgs &a, int, cudaStream_t s) {
