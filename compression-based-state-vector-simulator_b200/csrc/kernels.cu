@@ -1487,13 +1487,15 @@ __global__ void perm_pass_kernel(const PermPassArgs a) {
 }
 
 // ------------------------------------------------------------ dense pass
-template <typename R, int RB>
+// kC, kJ: the chunk and tile-qubit counts as compile-time constants (0 = read
+// them from the launch arguments).
+template <typename R, int RB, int kC, int kJ>
 __global__ void __launch_bounds__(kSweepThreads, 3) dense_pass_kernel(const DensePassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem[];
     T *tile = reinterpret_cast<T *>(smem);
     T *st = reinterpret_cast<T *>(a.state);
-    const int C = a.C, j = a.j, nb = C + j;
+    const int C = kC ? kC : a.C, j = kJ ? kJ : a.j, nb = C + j;
     const int size = 1 << nb;
     const int cmask = (1 << C) - 1;
     const int swm = swizzle_mask<R>(C);
@@ -2075,13 +2077,15 @@ __device__ void dual_tile_sweeps(typename Cplx<R>::T *tA, typename Cplx<R>::T *t
                                  int nsweeps, const ROp *__restrict__ ops, const typename Cplx<R>::T *__restrict__ pool,
                                  uint32_t ow, double *s_acc, int lane);
 
-template <typename R>
+// kC, kJ: the chunk and tile-qubit counts as compile-time constants (0 = read
+// them from the launch arguments).
+template <typename R, int kC, int kJ>
 __global__ void __launch_bounds__(kAdjThreads, 2) adjoint_pass_kernel(const AdjPassArgs a) {
     using T = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double s_acc[2 * kMaxAdjSlots];
     __shared__ int32_t s_tq[kMaxTileQubits];
-    const int C = a.C, j = a.j, nb = C + j, size = 1 << nb;
+    const int C = kC ? kC : a.C, j = kJ ? kJ : a.j, nb = C + j, size = 1 << nb;
     const int cmask = (1 << C) - 1;
     const int lane = threadIdx.x & 31;
     T *tp = reinterpret_cast<T *>(smem);
@@ -2766,21 +2770,31 @@ cudaError_t launch_perm_pass(const PermPassArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-template <typename R, int RB>
-static cudaError_t launch_dense_pass_t(const DensePassArgs &a, cudaStream_t s) {
+template <typename R, int RB, int kC, int kJ>
+static cudaError_t launch_dense_pass_kc(const DensePassArgs &a, cudaStream_t s) {
     const int nb = a.C + a.j;
     const size_t smem = (size_t)(2 * sizeof(R)) << nb;
-    cudaError_t e = ensure_dyn_smem(dense_pass_kernel<R, RB>, smem);
+    auto kern = dense_pass_kernel<R, RB, kC, kJ>;
+    cudaError_t e = ensure_dyn_smem(kern, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense_pass_kernel<R, RB>, kSweepThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSweepThreads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t grid = (uint64_t)per_sm * sm_count();
     if (grid > a.n_tiles) grid = a.n_tiles;
     if (grid == 0) grid = 1;
-    dense_pass_kernel<R, RB><<<(unsigned)grid, kSweepThreads, smem, s>>>(a);
+    kern<<<(unsigned)grid, kSweepThreads, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+// The uncompressed fused path's default geometry: 2^5-amplitude chunks and
+// tiles of 2^12 (complex128) or 2^13 (complex64) amplitudes.
+template <typename R, int RB>
+static cudaError_t launch_dense_pass_t(const DensePassArgs &a, cudaStream_t s) {
+    constexpr int kDC = 5, kDJ = sizeof(R) == 8 ? 7 : 8;
+    if (a.C == kDC && a.j == kDJ) return launch_dense_pass_kc<R, RB, kDC, kDJ>(a, s);
+    return launch_dense_pass_kc<R, RB, 0, 0>(a, s);
 }
 
 cudaError_t launch_dense_pass(bool f64, const DensePassArgs &a, int, cudaStream_t s) {
@@ -2991,25 +3005,35 @@ cudaError_t launch_block_bytes(const ChunkMeta *meta, const uint8_t *mask, uint3
     return cudaGetLastError();
 }
 
+template <typename R, int kC, int kJ>
+static cudaError_t launch_adjoint_pass_kc(const AdjPassArgs &a, cudaStream_t s) {
+    const int nb = a.C + a.j;
+    const size_t smem = (size_t)(4 * sizeof(R)) << nb;
+    auto kern = adjoint_pass_kernel<R, kC, kJ>;
+    cudaError_t e = ensure_dyn_smem(kern, smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kAdjThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    uint64_t grid = (uint64_t)per_sm * sm_count();
+    if (grid > a.n_tiles) grid = a.n_tiles;
+    if (grid == 0) grid = 1;
+    kern<<<(unsigned)grid, kAdjThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+// The uncompressed adjoint's default geometry: 2^5-amplitude chunks and
+// tiles of 2^11 (complex128) or 2^12 (complex64) amplitudes.
 template <typename R>
 static cudaError_t launch_adjoint_pass_t(const AdjPassArgs &a, cudaStream_t s) {
     if (a.nslots > kMaxAdjSlots) return cudaErrorInvalidValue;
     if (a.nsweeps > 0 && (a.rb != (sizeof(R) == 8 ? kDualRegBitsF64 : kDualRegBitsF32) || a.C + a.j < a.rb ||
                           a.nouter < 0 || a.nouter > kMaxOuterSel || !a.sweeps || !a.rops || !a.pool))
         return cudaErrorInvalidValue;
-    const int nb = a.C + a.j;
-    const size_t smem = (size_t)(4 * sizeof(R)) << nb;
-    cudaError_t e = ensure_dyn_smem(adjoint_pass_kernel<R>, smem);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_pass_kernel<R>, kAdjThreads, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    uint64_t grid = (uint64_t)per_sm * sm_count();
-    if (grid > a.n_tiles) grid = a.n_tiles;
-    if (grid == 0) grid = 1;
-    adjoint_pass_kernel<R><<<(unsigned)grid, kAdjThreads, smem, s>>>(a);
-    return cudaGetLastError();
+    constexpr int kAC = 5, kAJ = sizeof(R) == 8 ? 6 : 7;
+    if (a.C == kAC && a.j == kAJ) return launch_adjoint_pass_kc<R, kAC, kAJ>(a, s);
+    return launch_adjoint_pass_kc<R, 0, 0>(a, s);
 }
 
 cudaError_t launch_adjoint_pass(bool f64, const AdjPassArgs &a, cudaStream_t s) {
