@@ -1050,8 +1050,15 @@ struct qs_state {
     unsigned long long *tail_stats = nullptr;  // 3 counters per tail pass
     size_t tail_stats_cap = 0;
     std::vector<cudaEvent_t> tail_ev;
-    uint32_t *full_dev = nullptr;         // 1 when every block is stored (mask_full_kernel)
-    uint32_t *full_host = nullptr;        // pinned copy read after the stage
+    // 1 when every block is stored (mask_full_kernel): mapped pinned host
+    // memory and its device alias, written by the kernel itself
+    uint32_t *full_host = nullptr;
+    uint32_t *full_map = nullptr;
+    // end-of-apply error flag, counters, stage history and tail statistics,
+    // gathered by readback_kernel into mapped pinned host memory
+    unsigned long long *rb_host = nullptr;
+    unsigned long long *rb_map = nullptr;
+    size_t rb_cap = 0;
     int last_tail_from = -1;              // stage the last apply merged from (-1: none)
     void drop_tail() {
         if (tail_sweeps_dev) cudaFree(tail_sweeps_dev);
@@ -1127,8 +1134,8 @@ struct qs_state {
         if (pool_dev) cudaFree(pool_dev);
         drop_tail();
         if (tail_stats) cudaFree(tail_stats);
-        if (full_dev) cudaFree(full_dev);
         if (full_host) cudaFreeHost(full_host);
+        if (rb_host) cudaFreeHost(rb_host);
         if (history_dev) cudaFree(history_dev);
         for (auto e : pass_ev) cudaEventDestroy(e);
         if (error_dev) cudaFree(error_dev);
@@ -1302,9 +1309,10 @@ qs_status qs_create(qs_state **out, uint32_t n, uint32_t block_size, qs_dtype dt
     CREATE_TRY(cudaMalloc(&h->block_bytes, h->nb * sizeof(unsigned long long)));
     CREATE_TRY(cudaMalloc(&h->block_acc, h->nb * sizeof(unsigned long long)));
     CREATE_TRY(cudaMalloc(&h->group_active, h->nb));
-    CREATE_TRY(cudaMalloc(&h->error_dev, sizeof(int32_t)));
+    // 8 bytes: the end-of-apply readback copies it as one 64-bit word
+    CREATE_TRY(cudaMalloc(&h->error_dev, sizeof(unsigned long long)));
     CREATE_TRY(cudaMalloc(&h->dscratch, 4 * sizeof(double)));
-    CREATE_TRY(cudaMemset(h->error_dev, 0, sizeof(int32_t)));
+    CREATE_TRY(cudaMemset(h->error_dev, 0, sizeof(unsigned long long)));
 #undef CREATE_TRY
     qs_status s = h->init_basis(0);
     if (s != QS_OK) return cleanup(s);
@@ -1816,9 +1824,11 @@ qs_status qs_apply_circuit(qs_state *h) {
         printf("# of PUs per rank: 1\n# of streams per PU: 1\n");
         fflush(stdout);
     }
-    if (h->merge_tail && !h->full_dev) {
-        CUDA_TRY(h, cudaMalloc(&h->full_dev, sizeof(uint32_t)));
-        CUDA_TRY(h, cudaHostAlloc(&h->full_host, sizeof(uint32_t), cudaHostAllocDefault));
+    if (h->merge_tail && !h->full_host) {
+        void *dp = nullptr;
+        CUDA_TRY(h, cudaHostAlloc(&h->full_host, sizeof(uint32_t), cudaHostAllocMapped));
+        CUDA_TRY(h, cudaHostGetDevicePointer(&dp, h->full_host, 0));
+        h->full_map = static_cast<uint32_t *>(dp);
     }
     CUDA_TRY(h, cudaMemsetAsync(h->counters, 0, 8 * sizeof(unsigned long long), s));
     CUDA_TRY(h, cudaMemsetAsync(h->history_dev, 0, h->history_cap * sizeof(unsigned long long), s));
@@ -1907,10 +1917,12 @@ qs_status qs_apply_circuit(qs_state *h) {
 
     // whether every block is stored now (one synchronisation)
     auto mask_full_now = [&](bool *full) -> qs_status {
-        CUDA_TRY(h, qs::launch_mask_full(h->mask, h->nb, h->full_dev, s));
-        CUDA_TRY(h, cudaMemcpyAsync(h->full_host, h->full_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        // the previous flag test ended with a synchronisation, so no kernel
+        // writes the flag while the host sets it
+        *reinterpret_cast<volatile uint32_t *>(h->full_host) = 1u;
+        CUDA_TRY(h, qs::launch_mask_full(h->mask, h->nb, h->full_map, s));
         CUDA_TRY(h, cudaStreamSynchronize(s));
-        *full = *h->full_host != 0;
+        *full = *reinterpret_cast<volatile uint32_t *>(h->full_host) != 0;
         return QS_OK;
     };
 
@@ -1986,18 +1998,44 @@ qs_status qs_apply_circuit(qs_state *h) {
                                          h->block_bytes, h->history_dev + last + 1, s));
     }
     CUDA_TRY(h, cudaEventRecord(h->ev[1], s));
+    // error flag, counters, stage history and tail statistics reach the host
+    // through mapped memory written by one kernel: no copy-engine transfer
+    // that would queue behind another stream's store export
+    const size_t rb_words = 1 + 8 + h->history_cap + 3 * ntail;
+    if (h->rb_cap < rb_words) {
+        CUDA_TRY(h, cudaStreamSynchronize(s));
+        if (h->rb_host) cudaFreeHost(h->rb_host);
+        h->rb_host = h->rb_map = nullptr;
+        h->rb_cap = 0;
+        void *dp = nullptr;
+        CUDA_TRY(h, cudaHostAlloc(&h->rb_host, rb_words * sizeof(unsigned long long), cudaHostAllocMapped));
+        CUDA_TRY(h, cudaHostGetDevicePointer(&dp, h->rb_host, 0));
+        h->rb_map = static_cast<unsigned long long *>(dp);
+        h->rb_cap = rb_words;
+    }
+    qs::ReadbackList rl{};
+    rl.src[0] = reinterpret_cast<const unsigned long long *>(h->error_dev);
+    rl.words[0] = 1;
+    rl.src[1] = h->counters;
+    rl.words[1] = 8;
+    rl.src[2] = h->history_dev;
+    rl.words[2] = h->history_cap;
+    rl.n = 3;
+    if (ntail) {
+        rl.src[3] = h->tail_stats;
+        rl.words[3] = 3 * ntail;
+        rl.n = 4;
+    }
+    CUDA_TRY(h, qs::launch_readback(rl, h->rb_map, s));
     CUDA_TRY(h, cudaStreamSynchronize(s));
-    int32_t errflag = 0;
+    const volatile unsigned long long *rb = h->rb_host;
+    const int32_t errflag = (int32_t)(uint32_t)(rb[0] & 0xffffffffull);
     unsigned long long ctr[8];
-    CUDA_TRY(h, cudaMemcpy(&errflag, h->error_dev, sizeof(errflag), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(ctr, h->counters, sizeof(ctr), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < 8; ++i) ctr[i] = rb[1 + i];
     std::vector<unsigned long long> hist(h->history_cap);
-    CUDA_TRY(h, cudaMemcpy(hist.data(), h->history_dev, hist.size() * sizeof(unsigned long long),
-                           cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < hist.size(); ++i) hist[i] = rb[9 + i];
     std::vector<unsigned long long> tstats(3 * ntail);
-    if (ntail)
-        CUDA_TRY(h, cudaMemcpy(tstats.data(), h->tail_stats, tstats.size() * sizeof(unsigned long long),
-                               cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < tstats.size(); ++i) tstats[i] = rb[9 + h->history_cap + i];
     float ms = 0;
     CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
     if (errflag == 2)

@@ -415,7 +415,16 @@ cudaError_t launch_dense_norm(bool f64, const void *state, uint64_t dim, double 
 cudaError_t launch_dense_to_c128(bool f64, const void *state, uint64_t dim, double *out, cudaStream_t stream);
 cudaError_t launch_c128_to_dense(bool f64, const double *in, uint64_t dim, void *state, cudaStream_t stream);
 // *out = non-zero when every one of the nb blocks is stored, else 0.
+// *out (set to 1 by the caller beforehand) is cleared when a block of the
+// mask is not stored.
 cudaError_t launch_mask_full(const uint8_t *mask, uint32_t nb, uint32_t *out, cudaStream_t stream);
+// Up to four device arrays of 64-bit words gathered into one buffer.
+struct ReadbackList {
+    const unsigned long long *src[4];
+    size_t words[4];
+    int n;
+};
+cudaError_t launch_readback(const ReadbackList &l, unsigned long long *dst, cudaStream_t stream);
 cudaError_t launch_sum_mask_bytes(const uint8_t *mask, const unsigned long long *block_bytes, uint32_t nb,
                                   unsigned long long *out, cudaStream_t stream);
 

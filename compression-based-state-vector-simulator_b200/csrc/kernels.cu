@@ -1618,11 +1618,28 @@ __global__ void stage_end_kernel(const uint32_t *block_to_group, const uint8_t *
     if ((threadIdx.x & 31) == 0 && bytes) atomicAdd(history_slot, bytes);
 }
 
-// *out stays non-zero only when every block of the mask is stored (the
-// caller sets it non-zero first).
+// Clears *out when some block of the mask is not stored (the caller sets it
+// to 1 first); at most one store per CTA.  out may be the device alias of
+// mapped host memory, which the host reads once the stream has passed this
+// kernel: no copy-engine transfer, so the read does not queue behind
+// another stream's large copies.
 __global__ void mask_full_kernel(const uint8_t *mask, uint32_t nb, uint32_t *out) {
+    int all = 1;
     for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
-        if (!mask[b]) *out = 0u;
+        all &= mask[b] != 0;
+    all = __syncthreads_and(all);
+    if (threadIdx.x == 0 && !all) *reinterpret_cast<volatile uint32_t *>(out) = 0u;
+}
+
+// Copies up to four device word arrays into dst (back to back), the device
+// alias of mapped host memory: the end-of-apply counters reach the host
+// without a copy-engine transfer.
+__global__ void readback_kernel(ReadbackList l, unsigned long long *dst) {
+    size_t o = 0;
+    for (int k = 0; k < l.n; ++k) {
+        for (size_t i = threadIdx.x; i < l.words[k]; i += blockDim.x) dst[o + i] = l.src[k][i];
+        o += l.words[k];
+    }
 }
 
 __global__ void sum_mask_bytes_kernel(const uint8_t *mask, const unsigned long long *bb, uint32_t nb,
@@ -2829,9 +2846,15 @@ cudaError_t launch_stage_end(const uint32_t *b2g, const uint8_t *group_active, u
 }
 
 cudaError_t launch_mask_full(const uint8_t *mask, uint32_t nb, uint32_t *out, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(out, 0xff, sizeof(uint32_t), s);
-    if (e != cudaSuccess) return e;
-    mask_full_kernel<<<grid_for(nb, 256, 4), 256, 0, s>>>(mask, nb, out);
+    uint32_t grid = (nb + 1023u) / 1024u;
+    grid = grid > 148u ? 148u : (grid ? grid : 1u);
+    mask_full_kernel<<<grid, 1024, 0, s>>>(mask, nb, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_readback(const ReadbackList &l, unsigned long long *dst, cudaStream_t s) {
+    if (l.n < 0 || l.n > 4) return cudaErrorInvalidValue;
+    readback_kernel<<<1, 256, 0, s>>>(l, dst);
     return cudaGetLastError();
 }
 
