@@ -23,7 +23,10 @@
  * settings they share are only ever raised, under a lock).
  * All device work of a handle is ordered on one CUDA stream (qs_set_stream,
  * default: the legacy default stream).  Calls that return host data
- * synchronise that stream.
+ * synchronise that stream.  qs_apply_circuit reads its per-stage flags and
+ * final counters through mapped host memory written by its own kernels, not
+ * through copies, so on its own stream it never waits for another stream's
+ * host transfers (a store export on another handle, for example).
  */
 #ifndef QOMPSIM_H
 #define QOMPSIM_H
