@@ -14,6 +14,12 @@
 //   engine_host_check tail <gates file> <n> <B> <I> <f64>
 //       per start stage: passes of the per-stage plan from there, passes of
 //       the merged tail, and the tail pass that ends each stage
+//   engine_host_check selruns
+//       encode_selector_runs on random selector sets: where the selectors
+//       form at most two runs of consecutive bits, the variant computed from
+//       the runs picks, for every selector word, the matrix entries that the
+//       per-bit variant of the original selectors picked; other sets are
+//       left as they were
 #include "engine.cpp"
 
 #include <cstdio>
@@ -139,7 +145,82 @@ static int check_tail(const char *path, uint32_t n, uint32_t B, uint32_t I, bool
     return 0;
 }
 
+// The two device rules for an op's variant (rop_variant in kernels.cu):
+// selector bit j of the variant is bit sel[j] of the word W, or, with the
+// run encoding, runs [a, a + la) and [b, b + lb) of W side by side.
+static uint32_t variant_per_bit(const qs::ROp &o, uint32_t W) {
+    uint32_t v = 0;
+    for (int j = 0; j < o.nsel; ++j) v |= ((W >> o.sel[j]) & 1u) << j;
+    return v;
+}
+static uint32_t variant_from_runs(const qs::ROp &o, uint32_t W) {
+    const uint32_t a = o.sel[0] & 31u, la = o.sel[1], b = o.sel[2], lb = o.sel[3];
+    return ((W >> a) & ((1u << la) - 1u)) | (((W >> b) & ((1u << lb) - 1u)) << la);
+}
+
+static int check_selruns() {
+    std::mt19937 rng(7);
+    int bad = 0, encoded = 0, kept = 0;
+    for (int t = 0; t < 4000; ++t) {
+        const int ns = 1 + (int)(rng() % qs::kMaxSel);
+        std::vector<int> pos;
+        if (rng() % 2) {
+            // one or two runs of consecutive bits below bit 31
+            const int len1 = 1 + (int)(rng() % ns), len2 = ns - len1;
+            const int s1 = (int)(rng() % (31 - ns));
+            for (int k = 0; k < len1; ++k) pos.push_back(s1 + k);
+            if (len2) {
+                const int room = 31 - (s1 + len1 + 1) - len2;
+                const int s2 = s1 + len1 + 1 + (room > 0 ? (int)(rng() % (room + 1)) : 0);
+                for (int k = 0; k < len2; ++k) pos.push_back(s2 + k);
+            }
+        } else {
+            std::vector<int> all(31);
+            for (int k = 0; k < 31; ++k) all[k] = k;
+            std::shuffle(all.begin(), all.end(), rng);
+            pos.assign(all.begin(), all.begin() + ns);
+        }
+        std::shuffle(pos.begin(), pos.end(), rng);  // the variant's bit order is the selector order
+        std::vector<int> sorted(pos);
+        std::sort(sorted.begin(), sorted.end());
+        int runs = 1;
+        for (int k = 1; k < ns; ++k) runs += sorted[k] != sorted[k - 1] + 1;
+        const int stride = 1 + (int)(rng() % 4);
+        qs::ROp o{};
+        o.code = qs::OPC_M2;
+        o.nsel = (uint8_t)ns;
+        o.vstride = (uint8_t)stride;
+        for (int j = 0; j < ns; ++j) o.sel[j] = (uint8_t)pos[j];
+        o.mat = 3;
+        std::vector<cplx> pool(o.mat + ((size_t)1 << ns) * stride);
+        for (size_t k = 0; k < pool.size(); ++k) pool[k] = cplx((double)k, (double)t);
+        const std::vector<cplx> old(pool);
+        const qs::ROp orig = o;
+        encode_selector_runs(&o, stride, &pool);
+        if (runs <= 2) {
+            ++encoded;
+            bad += !(o.sel[0] & qs::kSelRuns) || o.mat != orig.mat || o.nsel != orig.nsel;
+            for (int w = 0; w < 256 && !bad; ++w) {
+                const uint32_t W = (uint32_t)rng() & 0x7fffffffu;
+                const uint32_t vr = variant_from_runs(o, W), vb = variant_per_bit(orig, W);
+                for (int e = 0; e < stride; ++e)
+                    bad += pool[o.mat + (size_t)vr * stride + e] != old[orig.mat + (size_t)vb * stride + e];
+            }
+        } else {
+            ++kept;
+            bad += std::memcmp(&o, &orig, sizeof(o)) != 0 || pool != old;
+        }
+        if (bad) {
+            printf("selruns: trial %d (%d selectors, %d runs) failed\n", t, ns, runs);
+            return 1;
+        }
+    }
+    printf("selruns ok %d encoded %d kept\n", encoded, kept);
+    return encoded > 0 && kept > 0 ? 0 : 1;
+}
+
 int main(int argc, char **argv) {
+    if (argc > 1 && !strcmp(argv[1], "selruns")) return check_selruns();
     if (argc > 1 && !strcmp(argv[1], "headers")) return check_headers();
     if (argc > 6 && !strcmp(argv[1], "plan"))
         return check_plan(argv[2], (uint32_t)atoi(argv[3]), (uint32_t)atoi(argv[4]), (uint32_t)atoi(argv[5]),

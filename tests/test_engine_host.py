@@ -43,6 +43,14 @@ def test_store_header_check(checker):
     assert r.returncode == 0 and "0 failures" in r.stdout, r.stdout + r.stderr
 
 
+def test_selector_run_encoding(checker):
+    """Ops whose selector bits form at most two runs are re-encoded with their
+    matrix variants permuted so that the two-shift rule of the device picks
+    what the per-bit rule picked; other ops are left as they were."""
+    r = subprocess.run([checker, "selruns"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "selruns ok" in r.stdout, r.stdout + r.stderr
+
+
 def _plan(checker, tmp_path, circuit, n, B, I, f64):
     import ctypes as ct
     from qulacs import _native
