@@ -20,6 +20,11 @@
 //       the runs picks, for every selector word, the matrix entries that the
 //       per-bit variant of the original selectors picked; other sets are
 //       left as they were
+//   engine_host_check halfchains
+//       fuse_half_chains on random op lists of two sweeps: runs of
+//       half-diagonals on one register bit become pending factors (ACC) and
+//       one application (D2HP) inside a sweep, never across sweeps, and the
+//       fused list gives every register group the unfused list's result
 #include "engine.cpp"
 
 #include <cstdio>
@@ -219,8 +224,106 @@ static int check_selruns() {
     return encoded > 0 && kept > 0 ? 0 : 1;
 }
 
+// The register ops of the check below, restated from apply_rop and the
+// r_* helpers in kernels.cu: D2 multiplies element s of the group by d0 or
+// d1 according to bit K of s, D2H by d1 where bit K is set, D2HP by zh d1
+// there and then resets zh to 1, ACC multiplies zh, M2 mixes every pair of
+// elements that differ in bit K, SCALAR multiplies z, which scales the whole
+// group once the sweep's ops are done.
+static void host_rop(std::vector<cplx> &v, cplx &z, cplx &zh, int code, const cplx *m) {
+    const int NS = (int)v.size();
+    auto in = [&](int base) { return code >= base && code < base + 8; };
+    if (code == qs::OPC_SCALAR) {
+        z *= m[0];
+    } else if (code == qs::OPC_ACC) {
+        zh *= m[0];
+    } else if (in(qs::OPC_D2)) {
+        const int K = code - qs::OPC_D2;
+        for (int t = 0; t < NS; ++t) v[t] *= ((t >> K) & 1) ? m[1] : m[0];
+    } else if (in(qs::OPC_D2H)) {
+        const int K = code - qs::OPC_D2H;
+        for (int t = 0; t < NS; ++t)
+            if ((t >> K) & 1) v[t] *= m[0];
+    } else if (in(qs::OPC_D2HP)) {
+        const int K = code - qs::OPC_D2HP;
+        const cplx d = zh * m[0];
+        for (int t = 0; t < NS; ++t)
+            if ((t >> K) & 1) v[t] *= d;
+        zh = cplx(1.0, 0.0);
+    } else if (in(qs::OPC_M2)) {
+        const int K = code - qs::OPC_M2;
+        for (int t = 0; t < NS; ++t) {
+            if ((t >> K) & 1) continue;
+            const cplx a = v[t], b = v[t | (1 << K)];
+            v[t] = m[0] * a + m[1] * b;
+            v[t | (1 << K)] = m[2] * a + m[3] * b;
+        }
+    }
+}
+
+static std::vector<cplx> host_sweeps(const std::vector<qs::ROp> &ops, const std::vector<qs::Sweep> &sw,
+                                     const std::vector<cplx> &pool, std::vector<cplx> v) {
+    for (const auto &w : sw) {
+        cplx z(1.0, 0.0), zh(1.0, 0.0);  // per group and sweep, as on the device
+        for (int k = w.g0; k < w.g1; ++k) host_rop(v, z, zh, ops[k].code, pool.data() + ops[k].mat);
+        for (auto &x : v) x *= z;
+    }
+    return v;
+}
+
+static int check_halfchains() {
+    std::mt19937 rng(11);
+    std::uniform_real_distribution<double> ang(-3.14159, 3.14159), amp(0.5, 1.5);
+    int fused = 0;
+    for (int t = 0; t < 3000; ++t) {
+        const int nops = 2 + (int)(rng() % 24), split = (int)(rng() % (nops + 1));
+        std::vector<qs::ROp> ops;
+        std::vector<cplx> pool;
+        for (int k = 0; k < nops; ++k) {
+            qs::ROp o{};
+            const int bit = (int)(rng() % 4), kind = (int)(rng() % 8);
+            // mostly half-diagonals on few bits, so that runs form
+            const int code = kind < 5 ? qs::OPC_D2H + (int)(rng() % 2) : kind == 5 ? qs::OPC_D2 + bit
+                           : kind == 6 ? qs::OPC_M2 + bit : qs::OPC_SCALAR;
+            const int nm = code >= qs::OPC_M2 ? 4 : (code >= qs::OPC_D2 && code < qs::OPC_D2H) ? 2 : 1;
+            o.code = (uint8_t)code;
+            o.vstride = (uint8_t)nm;
+            o.mat = (uint32_t)pool.size();
+            for (int e = 0; e < nm; ++e) pool.push_back(std::polar(amp(rng), ang(rng)));
+            ops.push_back(o);
+        }
+        std::vector<qs::Sweep> sw(2);
+        sw[0] = qs::Sweep{0, split, {0, 1, 2, 3, 0, 0}};
+        sw[1] = qs::Sweep{split, nops, {0, 1, 2, 3, 0, 0}};
+        std::vector<qs::ROp> f(ops);
+        fuse_half_chains(&f, 0, sw);
+        for (int k = 0; k < nops; ++k) {
+            fused += f[k].code == qs::OPC_ACC;
+            // an ACC hands its factor to the next op of its own sweep
+            const bool last = k + 1 == split || k + 1 == nops;
+            if (f[k].code == qs::OPC_ACC && last) {
+                printf("halfchains: trial %d: pending factor at the end of a sweep\n", t);
+                return 1;
+            }
+        }
+        for (int g = 0; g < 4; ++g) {
+            std::vector<cplx> v(16);
+            for (auto &x : v) x = std::polar(amp(rng), ang(rng));
+            const auto a = host_sweeps(ops, sw, pool, v), b = host_sweeps(f, sw, pool, v);
+            for (int e = 0; e < 16; ++e)
+                if (std::abs(a[e] - b[e]) > 1e-12 * (1.0 + std::abs(a[e]))) {
+                    printf("halfchains: trial %d: element %d differs (%g)\n", t, e, std::abs(a[e] - b[e]));
+                    return 1;
+                }
+        }
+    }
+    printf("halfchains ok %d fused\n", fused);
+    return fused > 0 ? 0 : 1;
+}
+
 int main(int argc, char **argv) {
     if (argc > 1 && !strcmp(argv[1], "selruns")) return check_selruns();
+    if (argc > 1 && !strcmp(argv[1], "halfchains")) return check_halfchains();
     if (argc > 1 && !strcmp(argv[1], "headers")) return check_headers();
     if (argc > 6 && !strcmp(argv[1], "plan"))
         return check_plan(argv[2], (uint32_t)atoi(argv[3]), (uint32_t)atoi(argv[4]), (uint32_t)atoi(argv[5]),

@@ -51,6 +51,14 @@ def test_selector_run_encoding(checker):
     assert r.returncode == 0 and "selruns ok" in r.stdout, r.stdout + r.stderr
 
 
+def test_half_diagonal_chain_fusion(checker):
+    """Runs of half-diagonals on one register bit fused into pending factors
+    and one application give every register group the unfused result, and
+    no pending factor outlives its sweep."""
+    r = subprocess.run([checker, "halfchains"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "halfchains ok" in r.stdout, r.stdout + r.stderr
+
+
 def _plan(checker, tmp_path, circuit, n, B, I, f64):
     import ctypes as ct
     from qulacs import _native
