@@ -20,6 +20,13 @@
 //       the runs picks, for every selector word, the matrix entries that the
 //       per-bit variant of the original selectors picked; other sets are
 //       left as they were
+//   engine_host_check dagplan
+//       plan_passes_dag and plan_passes on random gate lists: every gate is
+//       placed once; a pass's tile holds every qubit >= C on which one of its
+//       gates mixes amplitudes and at most jmax of them (padded to jmin);
+//       its other qubits >= C fit the outer selectors; and the passes' gates
+//       in order keep every two gates that do not commute (they share a qubit
+//       on which one of them mixes) in their original order
 //   engine_host_check halfchains
 //       fuse_half_chains on random op lists of two sweeps: runs of
 //       half-diagonals on one register bit become pending factors (ACC) and
@@ -321,8 +328,83 @@ static int check_halfchains() {
     return fused > 0 ? 0 : 1;
 }
 
+static int check_dagplan() {
+    std::mt19937 rng(5);
+    long pairs = 0, moved = 0;
+    for (int t = 0; t < 2000; ++t) {
+        const int C = 4 + (int)(rng() % 5), n = C + 2 + (int)(rng() % 24);
+        const int jmax = 3 + (int)(rng() % 3), jmin = jmax;
+        const int G = 1 + (int)(rng() % 160);
+        std::vector<CGate> cg(G);
+        for (auto &g : cg) {
+            g.nq = 1 + (int)(rng() % 2);
+            g.q[0] = (int)(rng() % n);
+            do g.q[1] = (int)(rng() % n); while (g.nq == 2 && g.q[1] == g.q[0]);
+            for (int b = 0; b < g.nq; ++b) g.mix[b] = rng() % 2;
+        }
+        std::vector<uint32_t> ids(G);
+        for (int i = 0; i < G; ++i) ids[i] = (uint32_t)i;
+        for (int dag = 0; dag < 2; ++dag) {
+            const auto pl = dag ? plan_passes_dag(ids, cg, C, jmax, jmin, C, n) : plan_passes(ids, cg, C, jmax, jmin, C, n);
+            std::vector<int> pos(G, -1);
+            int k = 0;
+            for (const auto &p : pl) {
+                std::set<int> tile(p.tile.begin(), p.tile.end()), outer;
+                if (tile.size() != p.tile.size() || (int)tile.size() > std::max(jmax, jmin)) {
+                    printf("dagplan: trial %d: tile of %zu qubits\n", t, p.tile.size());
+                    return 1;
+                }
+                for (uint32_t gi : p.gates) {
+                    if (gi >= (uint32_t)G || pos[gi] >= 0) {
+                        printf("dagplan: trial %d: gate %u placed twice or unknown\n", t, gi);
+                        return 1;
+                    }
+                    pos[gi] = k++;
+                    for (int b = 0; b < cg[gi].nq; ++b) {
+                        const int q = cg[gi].q[b];
+                        if (q < C) continue;
+                        if (cg[gi].mix[b] && !tile.count(q)) {
+                            printf("dagplan: trial %d: gate %u mixes qubit %d outside its tile\n", t, gi, q);
+                            return 1;
+                        }
+                        if (!cg[gi].mix[b] && !tile.count(q)) outer.insert(q);
+                    }
+                }
+                if ((int)outer.size() > qs::kMaxOuterSel) {
+                    printf("dagplan: trial %d: %zu outer selector qubits\n", t, outer.size());
+                    return 1;
+                }
+            }
+            if (k != G) {
+                printf("dagplan: trial %d: %d of %d gates placed\n", t, k, G);
+                return 1;
+            }
+            for (int i = 0; i < G; ++i)
+                for (int j = i + 1; j < G; ++j) {
+                    bool conflict = false;
+                    for (int a = 0; a < cg[i].nq; ++a)
+                        for (int b = 0; b < cg[j].nq; ++b)
+                            conflict |= cg[i].q[a] == cg[j].q[b] && (cg[i].mix[a] || cg[j].mix[b]);
+                    if (!conflict) {
+                        moved += dag && pos[i] > pos[j];
+                        continue;
+                    }
+                    ++pairs;
+                    if (pos[i] > pos[j]) {
+                        printf("dagplan: trial %d (%s): gates %d and %d do not commute but changed order\n", t,
+                               dag ? "dag" : "linear", i, j);
+                        return 1;
+                    }
+                }
+        }
+    }
+    printf("dagplan ok %ld ordered pairs, %ld commuting pairs reordered\n", pairs, moved);
+    return moved > 0 ? 0 : 1;
+}
+
 int main(int argc, char **argv) {
     if (argc > 1 && !strcmp(argv[1], "selruns")) return check_selruns();
+    if (argc > 1 && !strcmp(argv[1], "dagplan")) return check_dagplan();
     if (argc > 1 && !strcmp(argv[1], "halfchains")) return check_halfchains();
     if (argc > 1 && !strcmp(argv[1], "headers")) return check_headers();
     if (argc > 6 && !strcmp(argv[1], "plan"))

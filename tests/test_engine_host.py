@@ -51,6 +51,15 @@ def test_selector_run_encoding(checker):
     assert r.returncode == 0 and "selruns ok" in r.stdout, r.stdout + r.stderr
 
 
+def test_pass_planner_order_and_tiles(checker):
+    """Both pass planners place every gate once, give each pass a tile that
+    holds the qubits its gates mix (at most jmax, padded to jmin) and at most
+    the allowed outer selectors, and keep every non-commuting pair of gates
+    in order; the reordering planner does move commuting gates."""
+    r = subprocess.run([checker, "dagplan"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "dagplan ok" in r.stdout, r.stdout + r.stderr
+
+
 def test_half_diagonal_chain_fusion(checker):
     """Runs of half-diagonals on one register bit fused into pending factors
     and one application give every register group the unfused result, and
