@@ -27,6 +27,11 @@
 //       its other qubits >= C fit the outer selectors; and the passes' gates
 //       in order keep every two gates that do not commute (they share a qubit
 //       on which one of them mixes) in their original order
+//   engine_host_check chunkperm
+//       stage_relabel on random gate lists: SWAP and X gates on qubits >= C
+//       fold into a chunk permutation and the other gates are relabelled
+//       through it; the relabelled gates followed by the permutation's chunk
+//       moves give the original list's state on a dense vector
 //   engine_host_check halfchains
 //       fuse_half_chains on random op lists of two sweeps: runs of
 //       half-diagonals on one register bit become pending factors (ACC) and
@@ -402,8 +407,102 @@ static int check_dagplan() {
     return moved > 0 ? 0 : 1;
 }
 
+// A gate on a dense vector: index bit i of the matrix (row-major) is qubit q[i].
+static void host_apply(std::vector<cplx> &v, const CGate &g) {
+    const int dim = 1 << g.nq;
+    uint64_t mask = 0;
+    for (int i = 0; i < g.nq; ++i) mask |= 1ull << g.q[i];
+    for (uint64_t base = 0; base < v.size(); ++base) {
+        if (base & mask) continue;
+        uint64_t idx[4];
+        cplx x[4], y[4];
+        for (int c = 0; c < dim; ++c) {
+            idx[c] = base;
+            for (int i = 0; i < g.nq; ++i)
+                if ((c >> i) & 1) idx[c] |= 1ull << g.q[i];
+            x[c] = v[idx[c]];
+        }
+        for (int r = 0; r < dim; ++r) {
+            y[r] = 0;
+            for (int c = 0; c < dim; ++c) y[r] += g.m[r * dim + c] * x[c];
+        }
+        for (int r = 0; r < dim; ++r) v[idx[r]] = y[r];
+    }
+}
+
+// The chunk moves of a pass's output permutation (apply_perm in kernels.cu):
+// chunk c goes to c with bit dst[k] taken from bit src[k], the kept bits
+// unchanged, then the flip bits flipped.
+static uint64_t host_apply_perm(const qs::ChunkPerm &p, uint64_t c) {
+    uint64_t o = c & p.keep;
+    for (int k = 0; k < p.nmove; ++k) o |= ((c >> p.src[k]) & 1ull) << p.dst[k];
+    return o ^ p.flip;
+}
+
+static int check_chunkperm() {
+    std::mt19937 rng(13);
+    std::uniform_real_distribution<double> u(-1.0, 1.0);
+    const cplx one(1.0, 0.0), zero(0.0, 0.0);
+    int folded = 0;
+    for (int t = 0; t < 2000; ++t) {
+        const int n = 6 + (int)(rng() % 5), C = 2 + (int)(rng() % 3), G = 1 + (int)(rng() % 40);
+        std::vector<CGate> cg;
+        for (int k = 0; k < G; ++k) {
+            CGate g;
+            const int kind = (int)(rng() % 6);
+            g.nq = kind == 1 || kind == 3 ? 1 : 2;
+            const bool high = kind <= 1 || kind == 5;  // SWAP / X / X x X on qubits >= C
+            const int lo = high ? C : 0;
+            g.q[0] = lo + (int)(rng() % (n - lo));
+            do g.q[1] = lo + (int)(rng() % (n - lo)); while (g.nq == 2 && g.q[1] == g.q[0]);
+            if (g.nq == 2 && g.q[0] > g.q[1]) std::swap(g.q[0], g.q[1]);
+            const int dim = 1 << g.nq;
+            for (int e = 0; e < 16; ++e) g.m[e] = zero;
+            if (kind == 0) {         // SWAP
+                g.m[0] = g.m[1 * 4 + 2] = g.m[2 * 4 + 1] = g.m[15] = one;
+            } else if (kind == 1) {  // X
+                g.m[1] = g.m[2] = one;
+            } else if (kind == 5) {  // X on both qubits
+                for (int r = 0; r < 4; ++r) g.m[r * 4 + (r ^ 3)] = one;
+            } else if (kind == 4 && rng() % 2) {  // CNOT: a permutation that is not folded
+                g.m[0] = g.m[1 * 4 + 3] = g.m[2 * 4 + 2] = g.m[3 * 4 + 1] = one;
+            } else if (rng() % 3 == 0) {          // diagonal
+                for (int r = 0; r < dim; ++r) g.m[r * dim + r] = cplx(u(rng), u(rng));
+            } else {                              // dense
+                for (int e = 0; e < dim * dim; ++e) g.m[e] = cplx(u(rng), u(rng));
+            }
+            compute_mixing(&g);
+            cg.push_back(g);
+        }
+        std::vector<uint32_t> ids(G);
+        for (int k = 0; k < G; ++k) ids[k] = (uint32_t)k;
+        std::vector<CGate> out;
+        HostPerm P(n - C);
+        stage_relabel(cg, ids, C, true, &out, &P);
+        folded += G - (int)out.size();
+        std::vector<cplx> v(1ull << n);
+        for (auto &x : v) x = cplx(u(rng), u(rng));
+        std::vector<cplx> want(v), got(v);
+        for (const auto &g : cg) host_apply(want, g);
+        for (const auto &g : out) host_apply(got, g);
+        const qs::ChunkPerm dp = P.device();
+        std::vector<cplx> moved(got.size());
+        const uint64_t cm = (1ull << C) - 1;
+        for (uint64_t k = 0; k < got.size(); ++k) moved[(host_apply_perm(dp, k >> C) << C) | (k & cm)] = got[k];
+        for (uint64_t k = 0; k < want.size(); ++k)
+            if (std::abs(moved[k] - want[k]) > 1e-9 * (1.0 + std::abs(want[k]))) {
+                printf("chunkperm: trial %d (n %d, C %d, %d gates): amplitude %llu differs\n", t, n, C, G,
+                       (unsigned long long)k);
+                return 1;
+            }
+    }
+    printf("chunkperm ok %d gates folded\n", folded);
+    return folded > 0 ? 0 : 1;
+}
+
 int main(int argc, char **argv) {
     if (argc > 1 && !strcmp(argv[1], "selruns")) return check_selruns();
+    if (argc > 1 && !strcmp(argv[1], "chunkperm")) return check_chunkperm();
     if (argc > 1 && !strcmp(argv[1], "dagplan")) return check_dagplan();
     if (argc > 1 && !strcmp(argv[1], "halfchains")) return check_halfchains();
     if (argc > 1 && !strcmp(argv[1], "headers")) return check_headers();

@@ -60,6 +60,15 @@ def test_pass_planner_order_and_tiles(checker):
     assert r.returncode == 0 and "dagplan ok" in r.stdout, r.stdout + r.stderr
 
 
+def test_chunk_permutation_folding(checker):
+    """SWAP and X gates on qubits above the chunk bits folded into one chunk
+    permutation, the other gates relabelled through it: the relabelled gates
+    and then the permutation's chunk moves give the original circuit's state
+    (dense vectors of up to 10 qubits, random gates, CNOTs left unfolded)."""
+    r = subprocess.run([checker, "chunkperm"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "chunkperm ok" in r.stdout, r.stdout + r.stderr
+
+
 def test_half_diagonal_chain_fusion(checker):
     """Runs of half-diagonals on one register bit fused into pending factors
     and one application give every register group the unfused result, and
