@@ -32,6 +32,11 @@
 //       fold into a chunk permutation and the other gates are relabelled
 //       through it; the relabelled gates followed by the permutation's chunk
 //       moves give the original list's state on a dense vector
+//   engine_host_check opcompile
+//       the fused path's op compiler (planner, sweeps, register ops,
+//       diagonal merging, selector variants, chain fusion) on random
+//       circuits: its ops, interpreted over every tile of a dense vector by a
+//       host restatement of the tile pass, give the gates applied one by one
 //   engine_host_check halfchains
 //       fuse_half_chains on random op lists of two sweeps: runs of
 //       half-diagonals on one register bit become pending factors (ACC) and
@@ -439,6 +444,212 @@ static uint64_t host_apply_perm(const qs::ChunkPerm &p, uint64_t c) {
     return o ^ p.flip;
 }
 
+// Every register op of a single-store pass on a group of 16 elements,
+// restated from apply_rop and the r_* helpers in kernels.cu.  Codes of one
+// register bit are BASE + K; codes of two bits are BASE + 8 A + B.
+static void host_rop_any(cplx *v, cplx &z, cplx &zh, int code, const cplx *m) {
+    const int NS = 1 << qs::kRegBits;
+    auto in = [&](int base, int span) { return code >= base && code < base + span; };
+    if (code == qs::OPC_SCALAR) {
+        z *= m[0];
+    } else if (code == qs::OPC_ACC) {
+        zh *= m[0];
+    } else if (in(qs::OPC_D2, 8) || in(qs::OPC_D2H, 8) || in(qs::OPC_D2HP, 8) || in(qs::OPC_M2, 8) ||
+               in(qs::OPC_X, 8)) {
+        const int base = code & ~7, K = code & 7;
+        cplx d1 = 0;  // X ops carry no matrix entries: m is read only by the others
+        if (base == qs::OPC_D2H) d1 = m[0];
+        if (base == qs::OPC_D2HP) {
+            d1 = zh * m[0];
+            zh = cplx(1.0, 0.0);
+        }
+        for (int t = 0; t < NS; ++t) {
+            const bool hi = (t >> K) & 1;
+            if (base == qs::OPC_D2) v[t] *= hi ? m[1] : m[0];
+            else if ((base == qs::OPC_D2H || base == qs::OPC_D2HP) && hi) v[t] *= d1;
+            else if ((base == qs::OPC_M2 || base == qs::OPC_X) && !hi) {
+                const cplx a = v[t], b = v[t | (1 << K)];
+                v[t] = base == qs::OPC_X ? b : m[0] * a + m[1] * b;
+                v[t | (1 << K)] = base == qs::OPC_X ? a : m[2] * a + m[3] * b;
+            }
+        }
+    } else {
+        const int base = code >= qs::OPC_SWAP ? qs::OPC_SWAP : code >= qs::OPC_M4 ? qs::OPC_M4
+                       : code >= qs::OPC_D4H ? qs::OPC_D4H : qs::OPC_D4;
+        const int A = (code - base) >> 3, B = (code - base) & 7;
+        for (int t = 0; t < NS; ++t) {
+            const int k = ((t >> A) & 1) | (((t >> B) & 1) << 1);
+            if (base == qs::OPC_D4) v[t] *= m[k];
+            else if (base == qs::OPC_D4H && k) v[t] *= m[k - 1];
+        }
+        if (base == qs::OPC_M4 || base == qs::OPC_SWAP)
+            for (int t = 0; t < NS; ++t) {
+                if (((t >> A) & 1) || ((t >> B) & 1)) continue;
+                const int i[4] = {t, t | (1 << A), t | (1 << B), t | (1 << A) | (1 << B)};
+                const cplx x[4] = {v[i[0]], v[i[1]], v[i[2]], v[i[3]]};
+                for (int r = 0; r < 4; ++r) {
+                    if (base == qs::OPC_SWAP) {
+                        v[i[r]] = x[r == 1 ? 2 : r == 2 ? 1 : r];
+                        continue;
+                    }
+                    cplx acc = 0;
+                    for (int c = 0; c < 4; ++c) acc += m[4 * r + c] * x[c];
+                    v[i[r]] = acc;
+                }
+            }
+    }
+}
+
+// rop_variant in kernels.cu: the op's matrix variant for selector word W.
+static uint32_t host_variant(const qs::ROp &o, uint32_t W) {
+    if (o.sel[0] & qs::kSelRuns) return variant_from_runs(o, W);
+    uint32_t var = 0;
+    for (int j = 0; j < o.nsel; ++j) var |= ((W >> o.sel[j]) & 1u) << j;
+    return var;
+}
+
+static uint64_t host_insert_zero_bits(uint64_t x, const std::vector<int> &pos) {
+    for (int t : pos) x = ((x >> t) << (t + 1)) | (x & ((1ull << t) - 1));
+    return x;
+}
+
+// One fused tile pass over a dense vector, restated from dense_pass_kernel
+// and tile_sweeps: tile element e holds chunk element e mod 2^C of the
+// chunk whose tile-qubit bits are e >> C; a sweep walks the groups of 16
+// elements that differ in its register bits; the selector word is the
+// group's first element index with the tile's outer-qubit bits above it.
+static void host_tile_pass(std::vector<cplx> &st, int n, int C, const std::vector<int> &tile,
+                           const std::vector<qs::Sweep> &sw, const std::vector<qs::ROp> &ops,
+                           const std::vector<cplx> &pool, const std::vector<int> &outer) {
+    const int j = (int)tile.size(), nb = C + j, RB = qs::kRegBits;
+    std::vector<int> tq(j);
+    for (int k = 0; k < j; ++k) tq[k] = tile[k] - C;
+    std::vector<cplx> t(1ull << nb);
+    for (uint64_t tid = 0; tid < (1ull << (n - nb)); ++tid) {
+        const uint64_t cb = host_insert_zero_bits(tid, tq);
+        auto amp = [&](uint64_t e) {
+            uint64_t c = cb;
+            for (int k = 0; k < j; ++k) c |= ((e >> (C + k)) & 1ull) << tq[k];
+            return (c << C) | (e & ((1ull << C) - 1));
+        };
+        for (uint64_t e = 0; e < t.size(); ++e) t[e] = st[amp(e)];
+        uint32_t ow = 0;
+        for (size_t i = 0; i < outer.size(); ++i) ow |= (uint32_t)(((cb << C) >> outer[i]) & 1ull) << i;
+        for (const auto &w : sw) {
+            std::vector<int> sb(w.sbits, w.sbits + RB);
+            for (uint64_t g = 0; g < (1ull << (nb - RB)); ++g) {
+                const uint64_t base = host_insert_zero_bits(g, sb);
+                const uint32_t W = (uint32_t)base | (ow << nb);
+                cplx v[16];
+                auto off = [&](int s2) {
+                    uint64_t o = 0;
+                    for (int k = 0; k < RB; ++k)
+                        if ((s2 >> k) & 1) o |= 1ull << sb[k];
+                    return o;
+                };
+                for (int s2 = 0; s2 < 16; ++s2) v[s2] = t[base | off(s2)];
+                cplx z(1.0, 0.0), zh(1.0, 0.0);
+                for (int k = w.g0; k < w.g1; ++k)
+                    host_rop_any(v, z, zh, ops[k].code, pool.data() + ops[k].mat + host_variant(ops[k], W) * ops[k].vstride);
+                for (int s2 = 0; s2 < 16; ++s2) t[base | off(s2)] = z * v[s2];
+            }
+        }
+        for (uint64_t e = 0; e < t.size(); ++e) st[amp(e)] = t[e];
+    }
+}
+
+// Random circuits through the fused path's host steps (plan_passes_dag,
+// tiles padded to the register bits, to_kgate, plan_sweeps, build_ops,
+// merge_diagonal_ops, finalize_ops, fuse_half_chains, as in
+// qs_dense_apply_gates) and then through host_tile_pass, against the gates
+// applied one by one.
+static int check_opcompile() {
+    std::mt19937 rng(17);
+    std::uniform_real_distribution<double> u(-1.0, 1.0);
+    const cplx one(1.0, 0.0), zero(0.0, 0.0);
+    const int RB = qs::kRegBits;
+    long nops = 0, nsel = 0;
+    for (int t = 0; t < 400; ++t) {
+        const int n = 7 + (int)(rng() % 5), C = 2 + (int)(rng() % 4), jmax = 3 + (int)(rng() % 3);
+        const int G = 1 + (int)(rng() % 60);
+        std::vector<CGate> cg;
+        for (int k = 0; k < G; ++k) {
+            CGate g;
+            g.nq = 1 + (int)(rng() % 2);
+            g.q[0] = (int)(rng() % n);
+            do g.q[1] = (int)(rng() % n); while (g.nq == 2 && g.q[1] == g.q[0]);
+            if (g.nq == 2 && g.q[0] > g.q[1]) std::swap(g.q[0], g.q[1]);
+            const int dim = 1 << g.nq, kind = (int)(rng() % 6);
+            for (int e = 0; e < 16; ++e) g.m[e] = zero;
+            if (kind == 0) {  // diagonal (phases, controlled phases when one entry differs)
+                for (int r = 0; r < dim; ++r) g.m[r * dim + r] = rng() % 2 ? one : std::polar(1.0, u(rng) * 3);
+            } else if (kind == 1) {  // permutation: X, SWAP, CNOT
+                const int pk = (int)(rng() % 3);
+                for (int r = 0; r < dim; ++r) {
+                    const int c = dim == 2 ? r ^ 1 : pk == 0 ? (r == 1 ? 2 : r == 2 ? 1 : r) : pk == 1 ? r ^ 3 : (r & 1 ? r ^ 2 : r);
+                    g.m[r * dim + c] = one;
+                }
+            } else if (kind == 2 && dim == 4) {  // block-diagonal: mixes one qubit, selects by the other
+                const int sel = (int)(rng() % 2);
+                for (int b = 0; b < 2; ++b)
+                    for (int r = 0; r < 2; ++r)
+                        for (int c = 0; c < 2; ++c) {
+                            const int R = sel ? (r | (b << 1)) : (b | (r << 1)), Cc = sel ? (c | (b << 1)) : (b | (c << 1));
+                            g.m[R * 4 + Cc] = cplx(u(rng), u(rng));
+                        }
+            } else {  // dense
+                for (int e = 0; e < dim * dim; ++e) g.m[e] = cplx(u(rng), u(rng));
+            }
+            compute_mixing(&g);
+            cg.push_back(g);
+        }
+        std::vector<cplx> v(1ull << n);
+        for (auto &x : v) x = cplx(u(rng), u(rng));
+        std::vector<cplx> want(v), got(v);
+        for (const auto &g : cg) host_apply(want, g);
+        std::vector<uint32_t> ids(G);
+        for (int k = 0; k < G; ++k) ids[k] = (uint32_t)k;
+        auto pl = plan_passes_dag(ids, cg, C, jmax, std::min(jmax, 3), C, n);
+        for (auto &pp : pl) {
+            std::set<int> ts(pp.tile.begin(), pp.tile.end());
+            for (int q = C; q < n && C + (int)ts.size() < RB; ++q) ts.insert(q);
+            pp.tile.assign(ts.begin(), ts.end());
+            const int nb = C + (int)pp.tile.size();
+            if (nb < RB || nb > n) {
+                printf("opcompile: trial %d: tile of %d bits\n", t, nb);
+                return 1;
+            }
+            std::vector<qs::KGate> kg;
+            for (uint32_t gi : pp.gates) kg.push_back(to_kgate(cg[gi], pp.tile, C));
+            auto swp = plan_sweeps(kg, 0, kg.size(), nb, RB);
+            std::vector<RawOp> raw;
+            std::vector<cplx> rpool, pool;
+            build_ops(kg, 0, swp, RB, &raw, &rpool);
+            std::vector<qs::Sweep> merged;
+            merge_diagonal_ops(swp, 0, &raw, &rpool, &merged);
+            std::vector<int> outer;
+            std::vector<qs::ROp> ops;
+            if (!finalize_ops(raw, rpool, nb, &outer, &ops, &pool)) {
+                printf("opcompile: trial %d: too many outer selectors\n", t);
+                return 1;
+            }
+            fuse_half_chains(&ops, 0, merged);
+            nops += (long)ops.size();
+            for (const auto &o : ops) nsel += o.nsel;
+            host_tile_pass(got, n, C, pp.tile, merged, ops, pool, outer);
+        }
+        for (uint64_t k = 0; k < want.size(); ++k)
+            if (std::abs(got[k] - want[k]) > 1e-9 * (1.0 + std::abs(want[k]))) {
+                printf("opcompile: trial %d (n %d, C %d, jmax %d, %d gates, %zu passes): amplitude %llu differs "
+                       "(%g vs %g)\n", t, n, C, jmax, G, pl.size(), (unsigned long long)k, std::abs(got[k]),
+                       std::abs(want[k]));
+                return 1;
+            }
+    }
+    printf("opcompile ok %ld ops, %ld selector bits\n", nops, nsel);
+    return 0;
+}
+
 static int check_chunkperm() {
     std::mt19937 rng(13);
     std::uniform_real_distribution<double> u(-1.0, 1.0);
@@ -503,6 +714,7 @@ static int check_chunkperm() {
 int main(int argc, char **argv) {
     if (argc > 1 && !strcmp(argv[1], "selruns")) return check_selruns();
     if (argc > 1 && !strcmp(argv[1], "chunkperm")) return check_chunkperm();
+    if (argc > 1 && !strcmp(argv[1], "opcompile")) return check_opcompile();
     if (argc > 1 && !strcmp(argv[1], "dagplan")) return check_dagplan();
     if (argc > 1 && !strcmp(argv[1], "halfchains")) return check_halfchains();
     if (argc > 1 && !strcmp(argv[1], "headers")) return check_headers();

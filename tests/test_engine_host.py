@@ -69,6 +69,15 @@ def test_chunk_permutation_folding(checker):
     assert r.returncode == 0 and "chunkperm ok" in r.stdout, r.stdout + r.stderr
 
 
+def test_op_compiler_against_direct_application(checker):
+    """Random circuits of dense, diagonal, block-diagonal and permutation
+    gates compiled to register ops by the fused path's host steps; the ops,
+    interpreted tile by tile by a host restatement of the tile pass, give
+    the state of the gates applied one by one (within 1e-9)."""
+    r = subprocess.run([checker, "opcompile"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "opcompile ok" in r.stdout, r.stdout + r.stderr
+
+
 def test_half_diagonal_chain_fusion(checker):
     """Runs of half-diagonals on one register bit fused into pending factors
     and one application give every register group the unfused result, and
