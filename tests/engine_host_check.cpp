@@ -37,6 +37,12 @@
 //       diagonal merging, selector variants, chain fusion) on random
 //       circuits: its ops, interpreted over every tile of a dense vector by a
 //       host restatement of the tile pass, give the gates applied one by one
+//   engine_host_check dualcompile
+//       the two-store (adjoint) op compiler, plan_dual_sweeps, on random
+//       unitary circuits with Pauli-generated parametric gates at 3 and 4
+//       register bits: its ops, interpreted by a host restatement of the
+//       two-store tile pass, give every derivative sum and both final states
+//       of the gates applied one by one
 //   engine_host_check halfchains
 //       fuse_half_chains on random op lists of two sweeps: runs of
 //       half-diagonals on one register bit become pending factors (ACC) and
@@ -650,6 +656,211 @@ static int check_opcompile() {
     return 0;
 }
 
+// A two-store pass, restated from dual_tile_sweeps: every gate op acts on
+// the groups of both stores (each with its own pending scalars), and an
+// OPC_SUM op adds f conj(zb) za sum_s conj(w[s ^ xs]) (-1)^{|s & zs|} v[s]
+// to its slot (f: the op's +-1 variant for the Z bits outside the group).
+static void host_dual_pass(std::vector<cplx> &A, std::vector<cplx> &B, int n, int C, int RB,
+                           const std::vector<int> &tile, const qs::Sweep *sw, size_t nsw, const qs::ROp *ops,
+                           const std::vector<cplx> &pool, const std::vector<int> &outer, std::vector<cplx> *sums) {
+    const int j = (int)tile.size(), nb = C + j, NS = 1 << RB;
+    std::vector<int> tq(j);
+    for (int k = 0; k < j; ++k) tq[k] = tile[k] - C;
+    std::vector<cplx> ta(1ull << nb), tb(1ull << nb);
+    for (uint64_t tid = 0; tid < (1ull << (n - nb)); ++tid) {
+        const uint64_t cb = host_insert_zero_bits(tid, tq);
+        auto amp = [&](uint64_t e) {
+            uint64_t c = cb;
+            for (int k = 0; k < j; ++k) c |= ((e >> (C + k)) & 1ull) << tq[k];
+            return (c << C) | (e & ((1ull << C) - 1));
+        };
+        for (uint64_t e = 0; e < ta.size(); ++e) {
+            ta[e] = A[amp(e)];
+            tb[e] = B[amp(e)];
+        }
+        uint32_t ow = 0;
+        for (size_t i = 0; i < outer.size(); ++i) ow |= (uint32_t)(((cb << C) >> outer[i]) & 1ull) << i;
+        for (size_t si = 0; si < nsw; ++si) {
+            const qs::Sweep &w = sw[si];
+            std::vector<int> sb(w.sbits, w.sbits + RB);
+            auto off = [&](int s2) {
+                uint64_t o = 0;
+                for (int k = 0; k < RB; ++k)
+                    if ((s2 >> k) & 1) o |= 1ull << sb[k];
+                return o;
+            };
+            for (uint64_t g = 0; g < (1ull << (nb - RB)); ++g) {
+                const uint64_t base = host_insert_zero_bits(g, sb);
+                const uint32_t W = (uint32_t)base | (ow << nb);
+                // the interpreter works on 16-element groups; with RB = 3 the
+                // upper half stays zero and no op of the sweep touches bit 3
+                cplx v[16] = {}, u[16] = {};
+                for (int s2 = 0; s2 < NS; ++s2) {
+                    v[s2] = ta[base | off(s2)];
+                    u[s2] = tb[base | off(s2)];
+                }
+                cplx za(1.0, 0.0), zb(1.0, 0.0), zha(1.0, 0.0), zhb(1.0, 0.0);
+                for (int k = w.g0; k < w.g1; ++k) {
+                    const qs::ROp &o = ops[k];
+                    if (o.code == qs::OPC_SUM) {
+                        const int xs = o.pad >> 4, zs = o.pad & 15;
+                        cplx acc = 0;
+                        for (int s2 = 0; s2 < NS; ++s2)
+                            acc += std::conj(u[s2 ^ xs]) * v[s2] * ((__builtin_popcount(s2 & zs) & 1) ? -1.0 : 1.0);
+                        (*sums)[o.vstride] += pool[o.mat + host_variant(o, W)] * std::conj(zb) * za * acc;
+                    } else {
+                        const cplx *m = pool.data() + o.mat + host_variant(o, W) * o.vstride;
+                        host_rop_any(v, za, zha, o.code, m);
+                        host_rop_any(u, zb, zhb, o.code, m);
+                    }
+                }
+                for (int s2 = 0; s2 < NS; ++s2) {
+                    ta[base | off(s2)] = za * v[s2];
+                    tb[base | off(s2)] = zb * u[s2];
+                }
+            }
+        }
+        for (uint64_t e = 0; e < ta.size(); ++e) {
+            A[amp(e)] = ta[e];
+            B[amp(e)] = tb[e];
+        }
+    }
+}
+
+// A random unitary of size dim (Gram-Schmidt on random complex columns):
+// the adjoint's sums are invariant under gates that commute with a
+// parametric gate only when those gates are unitary.
+static void random_unitary(int dim, cplx *m, std::mt19937 &rng) {
+    std::uniform_real_distribution<double> u(-1.0, 1.0);
+    for (int c = 0; c < dim; ++c) {
+        cplx col[4];
+        for (int r = 0; r < dim; ++r) col[r] = cplx(u(rng), u(rng));
+        for (int p = 0; p < c; ++p) {
+            cplx d = 0;
+            for (int r = 0; r < dim; ++r) d += std::conj(m[r * dim + p]) * col[r];
+            for (int r = 0; r < dim; ++r) col[r] -= d * m[r * dim + p];
+        }
+        double nrm = 0;
+        for (int r = 0; r < dim; ++r) nrm += std::norm(col[r]);
+        nrm = std::sqrt(nrm);
+        for (int r = 0; r < dim; ++r) m[r * dim + c] = col[r] / nrm;
+    }
+}
+
+// plan_dual_sweeps on random circuits with parametric gates: the two-store
+// ops, interpreted by host_dual_pass, give for each parametric gate
+// sum_x conj(B[x ^ gx]) (-1)^{|x & gz|} A[x] taken just before the gate,
+// and the states of every gate applied to both stores one by one.
+static int check_dualcompile() {
+    std::mt19937 rng(19);
+    std::uniform_real_distribution<double> u(-1.0, 1.0);
+    const cplx one(1.0, 0.0), zero(0.0, 0.0);
+    long nsum = 0, fused_passes = 0, passes = 0;
+    for (int t = 0; t < 300; ++t) {
+        const int RB = t % 2 ? qs::kDualRegBitsF32 : qs::kDualRegBitsF64;
+        const int n = 7 + (int)(rng() % 4), C = 2 + (int)(rng() % 4), jmax = 3 + (int)(rng() % 3);
+        const int G = 1 + (int)(rng() % 40);
+        std::vector<CGate> cg;
+        std::vector<int32_t> slots(G, -1);
+        std::vector<uint64_t> gx(G, 0), gz(G, 0);
+        int nslot = 0;
+        for (int k = 0; k < G; ++k) {
+            CGate g;
+            g.nq = 1 + (int)(rng() % 2);
+            g.q[0] = (int)(rng() % n);
+            do g.q[1] = (int)(rng() % n); while (g.nq == 2 && g.q[1] == g.q[0]);
+            if (g.nq == 2 && g.q[0] > g.q[1]) std::swap(g.q[0], g.q[1]);
+            const int dim = 1 << g.nq;
+            for (int e = 0; e < 16; ++e) g.m[e] = zero;
+            if (rng() % 3 == 0)
+                for (int r = 0; r < dim; ++r) g.m[r * dim + r] = std::polar(1.0, u(rng) * 3);
+            else
+                random_unitary(dim, g.m, rng);
+            compute_mixing(&g);
+            if (rng() % 2) {  // parametric: a Pauli generator on the gate's own qubits
+                slots[k] = nslot++;
+                for (int b = 0; b < g.nq; ++b) {
+                    const int pk = (int)(rng() % 4);  // I, X, Y, Z
+                    if (pk == 1 || pk == 2) gx[k] |= 1ull << g.q[b];
+                    if (pk == 2 || pk == 3) gz[k] |= 1ull << g.q[b];
+                    if (pk == 1 || pk == 2) g.mix[b] = true;  // as qs_dense_adjoint: flipped qubits mix
+                }
+            }
+            cg.push_back(g);
+        }
+        // reference: every gate on both stores in order, each sum just before its gate
+        std::vector<cplx> a0(1ull << n), b0(1ull << n);
+        for (auto &x : a0) x = cplx(u(rng), u(rng));
+        for (auto &x : b0) x = cplx(u(rng), u(rng));
+        std::vector<cplx> wa(a0), wb(b0), want(nslot, 0.0);
+        for (int k = 0; k < G; ++k) {
+            if (slots[k] >= 0)
+                for (uint64_t x = 0; x < wa.size(); ++x)
+                    want[slots[k]] += std::conj(wb[x ^ gx[k]]) * wa[x] * ((__builtin_popcountll(x & gz[k]) & 1) ? -1.0 : 1.0);
+            host_apply(wa, cg[k]);
+            host_apply(wb, cg[k]);
+        }
+        std::vector<cplx> ga(a0), gb(b0), got(nslot, 0.0);
+        std::vector<uint32_t> ids(G);
+        for (int k = 0; k < G; ++k) ids[k] = (uint32_t)k;
+        auto pl = plan_passes_dag(ids, cg, C, jmax, std::min(jmax, 3), C, n);
+        for (auto &pp : pl) {
+            std::set<int> ts(pp.tile.begin(), pp.tile.end());
+            for (int q = C; q < n && C + (int)ts.size() < RB; ++q) ts.insert(q);
+            pp.tile.assign(ts.begin(), ts.end());
+            std::vector<qs::Sweep> asw;
+            std::vector<qs::ROp> arops;
+            std::vector<cplx> apool;
+            DualSweepPlan dp;
+            ++passes;
+            if (!plan_dual_sweeps(cg, pp.gates, slots.data(), gx.data(), gz.data(), pp.tile, C, RB, &asw, &arops,
+                                  &apool, &dp)) {
+                // not fusable: the engine runs such a pass op by op; here the reference steps stand in
+                for (uint32_t gi : pp.gates) {
+                    if (slots[gi] >= 0)
+                        for (uint64_t x = 0; x < ga.size(); ++x)
+                            got[slots[gi]] += std::conj(gb[x ^ gx[gi]]) * ga[x] *
+                                              ((__builtin_popcountll(x & gz[gi]) & 1) ? -1.0 : 1.0);
+                    host_apply(ga, cg[gi]);
+                    host_apply(gb, cg[gi]);
+                }
+                continue;
+            }
+            ++fused_passes;
+            std::vector<cplx> local(std::max(1, nslot), 0.0);
+            host_dual_pass(ga, gb, n, C, RB, pp.tile, asw.data() + dp.sw_off, dp.nsw, arops.data() + dp.rop_off, apool,
+                           dp.outer, &local);
+            int ls = 0;
+            for (uint32_t gi : pp.gates)
+                if (slots[gi] >= 0) {
+                    got[slots[gi]] += local[ls++];
+                    ++nsum;
+                }
+        }
+        double scale = 1.0;
+        for (const auto &x : wa) scale = std::max(scale, std::abs(x));
+        for (const auto &x : wb) scale = std::max(scale, std::abs(x));
+        // |sum| <= |A| |B|, both norms kept by the unitary gates
+        double na = 0, nb2 = 0;
+        for (const auto &x : a0) na += std::norm(x);
+        for (const auto &x : b0) nb2 += std::norm(x);
+        const double tol = 1e-12 * std::sqrt(na * nb2) * (1 + G);
+        for (int k = 0; k < nslot; ++k)
+            if (std::abs(got[k] - want[k]) > tol) {
+                printf("dualcompile: trial %d (RB %d, n %d, C %d): sum %d differs (%g vs %g)\n", t, RB, n, C, k,
+                       std::abs(got[k]), std::abs(want[k]));
+                return 1;
+            }
+        for (uint64_t x = 0; x < wa.size(); ++x)
+            if (std::abs(ga[x] - wa[x]) > 1e-9 * scale || std::abs(gb[x] - wb[x]) > 1e-9 * scale) {
+                printf("dualcompile: trial %d (RB %d): amplitude %llu differs\n", t, RB, (unsigned long long)x);
+                return 1;
+            }
+    }
+    printf("dualcompile ok %ld of %ld passes fused, %ld sums\n", fused_passes, passes, nsum);
+    return fused_passes > passes / 2 && nsum > 0 ? 0 : 1;
+}
+
 static int check_chunkperm() {
     std::mt19937 rng(13);
     std::uniform_real_distribution<double> u(-1.0, 1.0);
@@ -715,6 +926,7 @@ int main(int argc, char **argv) {
     if (argc > 1 && !strcmp(argv[1], "selruns")) return check_selruns();
     if (argc > 1 && !strcmp(argv[1], "chunkperm")) return check_chunkperm();
     if (argc > 1 && !strcmp(argv[1], "opcompile")) return check_opcompile();
+    if (argc > 1 && !strcmp(argv[1], "dualcompile")) return check_dualcompile();
     if (argc > 1 && !strcmp(argv[1], "dagplan")) return check_dagplan();
     if (argc > 1 && !strcmp(argv[1], "halfchains")) return check_halfchains();
     if (argc > 1 && !strcmp(argv[1], "headers")) return check_headers();

@@ -78,6 +78,16 @@ def test_op_compiler_against_direct_application(checker):
     assert r.returncode == 0 and "opcompile ok" in r.stdout, r.stdout + r.stderr
 
 
+def test_two_store_op_compiler_sums_and_states(checker):
+    """The adjoint's two-store passes compiled by plan_dual_sweeps: on random
+    unitary circuits with parametric gates (X, Y, Z generators on their own
+    qubits), the interpreted ops give every derivative sum
+    sum_x conj(lambda[x ^ gx]) (-1)^{|x & gz|} psi[x] just before its gate and
+    both final states, at 3 (complex128) and 4 (complex64) register bits."""
+    r = subprocess.run([checker, "dualcompile"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "dualcompile ok" in r.stdout, r.stdout + r.stderr
+
+
 def test_half_diagonal_chain_fusion(checker):
     """Runs of half-diagonals on one register bit fused into pending factors
     and one application give every register group the unfused result, and
